@@ -1,0 +1,1105 @@
+// libgpucvt: C ABI (include/gpu_cvt.h) over the sm_100a kernels.
+// Unity translation unit: the device code lives in the included headers.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gpu_cvt.h"
+#include "cvt_eval.cuh"
+#include "cvt_stage.cuh"
+
+using namespace cvt;
+
+// ---------------------------------------------------------------------------
+// errors, launch accounting
+// ---------------------------------------------------------------------------
+static thread_local std::string g_last_error;
+static std::atomic<unsigned long long> g_launches{0};
+
+static cvt_status_t fail(cvt_status_t s, const std::string& msg) {
+  g_last_error = msg;
+  return s;
+}
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      return fail(e_ == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,                  \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                           \
+    }                                                                                            \
+  } while (0)
+
+#define LAUNCHED(n) g_launches.fetch_add((n), std::memory_order_relaxed)
+#define CKLAUNCH()                                                                               \
+  do {                                                                                           \
+    LAUNCHED(1);                                                                                 \
+    cudaError_t e_ = cudaGetLastError();                                                         \
+    if (e_ != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+  } while (0)
+
+static inline cudaStream_t S_(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+static inline int cdiv(long a, long b) { return (int)((a + b - 1) / b); }
+
+extern "C" const char* cvt_status_string(cvt_status_t s) {
+  switch (s) {
+    case CVT_OK: return "ok";
+    case CVT_ERR_INVALID: return "invalid argument";
+    case CVT_ERR_CUDA: return "CUDA error";
+    case CVT_ERR_OOM: return "out of device memory";
+    case CVT_ERR_UNSUPPORTED: return "unsupported";
+    case CVT_ERR_CAPACITY: return "capacity exceeded";
+  }
+  return "unknown";
+}
+extern "C" const char* cvt_last_error(void) { return g_last_error.c_str(); }
+extern "C" int cvt_version(void) { return 1; }
+extern "C" unsigned long long cvt_launch_count(void) { return g_launches.load(); }
+
+// stream-ordered scratch
+struct Scratch {
+  cudaStream_t st;
+  std::vector<void*> ptrs;
+  explicit Scratch(cudaStream_t s) : st(s) {}
+  template <class X> cudaError_t get(X** p, size_t count) {
+    void* q = nullptr;
+    cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(count * sizeof(X), 16), st);
+    if (e == cudaSuccess) { ptrs.push_back(q); *p = reinterpret_cast<X*>(q); }
+    return e;
+  }
+  ~Scratch() { for (void* q : ptrs) cudaFreeAsync(q, st); }
+};
+
+// ---------------------------------------------------------------------------
+// grid build over one device point set (stage API + mesh vertex grid)
+// ---------------------------------------------------------------------------
+struct PointGrid {
+  GridGeom* geom = nullptr;
+  int* cell_count = nullptr;
+  int* cell_start = nullptr;
+  int* part = nullptr;
+  int2* cellrank = nullptr;
+  Pt4<float>* sorted = nullptr;
+  int total_cells = 0;  // scan length (spatial capacity + NaN bucket)
+};
+
+// geometry supplied by the host (hgeom != nullptr) or derived on the device
+// from the bbox with ~per_cell points per cell
+static cvt_status_t build_point_grid(Scratch& sc, const float* P, int n, float per_cell, const GridGeom* hgeom,
+                                     PointGrid& pg) {
+  cudaStream_t st = sc.st;
+  int cap = hgeom ? hgeom->ncell : std::max(64, 2 * n);
+  pg.total_cells = cap + 1;
+  CK(sc.get(&pg.geom, 1));
+  CK(sc.get(&pg.cell_count, (size_t)pg.total_cells));
+  CK(sc.get(&pg.cell_start, (size_t)pg.total_cells + 1));
+  CK(sc.get(&pg.part, (size_t)scan_blocks(pg.total_cells) + 2));
+  CK(sc.get(&pg.cellrank, (size_t)std::max(n, 1)));
+  CK(sc.get(&pg.sorted, (size_t)std::max(n, 1)));
+  if (hgeom) {
+    CK(cudaMemcpyAsync(pg.geom, hgeom, sizeof(GridGeom), cudaMemcpyHostToDevice, st));
+  } else {
+    int* bb;
+    CK(sc.get(&bb, 6));
+    k_bbox_init<<<1, 32, 0, st>>>(bb);
+    CKLAUNCH();
+    if (n > 0) { k_bbox<<<cdiv(n, 256), 256, 0, st>>>(n, P, bb); CKLAUNCH(); }
+    k_grid_geom<<<1, 32, 0, st>>>(bb, n, per_cell, cap, pg.geom);
+    CKLAUNCH();
+  }
+  CK(cudaMemsetAsync(pg.cell_count, 0, sizeof(int) * pg.total_cells, st));
+  if (n > 0) {
+    k_grid_count<float><<<cdiv(n, 256), 256, 0, st>>>(n, P, SegGrid{pg.geom, nullptr, nullptr}, pg.cell_count, pg.cellrank);
+    CKLAUNCH();
+  }
+  launch_exclusive_scan(pg.total_cells, pg.cell_count, pg.part, pg.cell_start, st);
+  LAUNCHED(3);
+  CK(cudaGetLastError());
+  if (n > 0) {
+    k_grid_scatter<float><<<cdiv(n, 256), 256, 0, st>>>(n, P, pg.cellrank, pg.cell_start, pg.sorted);
+    CKLAUNCH();
+  }
+  return CVT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// stage API
+// ---------------------------------------------------------------------------
+template <int KK>
+static void launch_knn_points(const PointGrid& pg, int n, const uint8_t* frozen, int kk, uint32_t* knn, float* dist,
+                              cudaStream_t st) {
+  k_stage_knn_points<KK><<<cdiv(n, 128), 128, 0, st>>>(pg.geom, pg.cell_start, pg.sorted, pg.total_cells, frozen, kk,
+                                                       knn, dist);
+}
+template <int KK>
+static void launch_knn_query(const PointGrid& pg, const float* Q, int nQ, const uint8_t* frozen, int kk, int ex,
+                             uint32_t* knn, float* dist, cudaStream_t st) {
+  k_stage_knn_query<KK><<<cdiv(nQ, 128), 128, 0, st>>>(pg.geom, pg.cell_start, pg.sorted, Q, nQ, frozen, kk, ex, knn,
+                                                       dist);
+}
+
+#define KK_DISPATCH(kk, FN, ...)                                 \
+  do {                                                           \
+    if ((kk) <= 1) FN<1>(__VA_ARGS__);                           \
+    else if ((kk) <= 5) FN<5>(__VA_ARGS__);                      \
+    else if ((kk) <= 9) FN<9>(__VA_ARGS__);                      \
+    else if ((kk) <= 17) FN<17>(__VA_ARGS__);                    \
+    else if ((kk) <= 21) FN<21>(__VA_ARGS__);                    \
+    else if ((kk) <= 25) FN<25>(__VA_ARGS__);                    \
+    else if ((kk) <= 33) FN<33>(__VA_ARGS__);                    \
+    else FN<64>(__VA_ARGS__);                                    \
+  } while (0)
+
+extern "C" cvt_status_t cvt_knn_sites(const float* pts, int n, int kk, const uint8_t* frozen, uint32_t* knn,
+                                      float* dist, void* stream) {
+  if (n < 0 || kk < 1 || kk > 64 || (n > 0 && (!pts || !knn))) return fail(CVT_ERR_INVALID, "cvt_knn_sites: bad arguments");
+  if (n == 0) return CVT_OK;
+  cudaStream_t st = S_(stream);
+  Scratch sc(st);
+  PointGrid pg;
+  cvt_status_t s = build_point_grid(sc, pts, n, 0.2f * kk, nullptr, pg);
+  if (s != CVT_OK) return s;
+  KK_DISPATCH(kk, launch_knn_points, pg, n, frozen, kk, knn, dist, st);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_knn_query_to_points(const float* cand, int n_cand, const float* query, int n_query, int kk,
+                                                const uint8_t* frozen, uint32_t* knn, float* dist, void* stream) {
+  if (n_cand < 0 || n_query < 0 || kk < 1 || kk > 64 || (n_query > 0 && (!query || !knn)) || (n_cand > 0 && !cand))
+    return fail(CVT_ERR_INVALID, "cvt_knn_query_to_points: bad arguments");
+  if (n_query == 0) return CVT_OK;
+  cudaStream_t st = S_(stream);
+  Scratch sc(st);
+  PointGrid pg;
+  cvt_status_t s = build_point_grid(sc, cand, n_cand, 0.2f * kk + 1.f, nullptr, pg);
+  if (s != CVT_OK) return s;
+  KK_DISPATCH(kk, launch_knn_query, pg, query, n_query, frozen, kk, 0, knn, dist, st);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_knn_vertices(const float* V, int nV, const float* Q, int nQ, int k, int exclude_self,
+                                         const uint8_t* frozen, int* out, void* stream) {
+  if (nV < 0 || nQ < 0 || k < 1 || k > 64 || (nQ > 0 && (!Q || !out)) || (nV > 0 && !V))
+    return fail(CVT_ERR_INVALID, "cvt_knn_vertices: bad arguments");
+  if (nQ == 0) return CVT_OK;
+  cudaStream_t st = S_(stream);
+  Scratch sc(st);
+  PointGrid pg;
+  cvt_status_t s = build_point_grid(sc, V, nV, 0.2f * k + 1.f, nullptr, pg);
+  if (s != CVT_OK) return s;
+  // int output: the uint32 sentinel 0xFFFFFFFF reads as -1
+  KK_DISPATCH(k, launch_knn_query, pg, Q, nQ, frozen, k, exclude_self ? 1 : 0, reinterpret_cast<uint32_t*>(out),
+              (float*)nullptr, st);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_knn_drop_self(const uint32_t* in, int n, int kin, int kout, uint32_t* out, void* stream) {
+  if (n < 0 || kin < 1 || kout < 1 || (n > 0 && (!in || !out))) return fail(CVT_ERR_INVALID, "cvt_knn_drop_self: bad arguments");
+  if (n == 0) return CVT_OK;
+  k_stage_drop_self<<<cdiv(n, 256), 256, 0, S_(stream)>>>(in, n, kin, kout, out);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_restore_frozen_rows(const uint8_t* frozen, const uint32_t* prev, uint32_t* cur, int n, int k,
+                                                void* stream) {
+  if (n < 0 || k < 1 || (n > 0 && (!frozen || !prev || !cur))) return fail(CVT_ERR_INVALID, "cvt_restore_frozen_rows: bad arguments");
+  if (n == 0) return CVT_OK;
+  k_stage_restore_rows<<<cdiv(n, 256), 256, 0, S_(stream)>>>(frozen, prev, cur, n, k);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_vertex_normals(const float* V, int nV, const int* F, int nF, const int* vf_off,
+                                           const int* vf_faces, float* N, void* stream) {
+  if (nV < 0 || nF < 0 || (nV > 0 && (!V || !vf_off || !N)) || (nF > 0 && (!F || !vf_faces)))
+    return fail(CVT_ERR_INVALID, "cvt_vertex_normals: bad arguments");
+  if (nV == 0) return CVT_OK;
+  k_stage_normals<<<cdiv(nV, 256), 256, 0, S_(stream)>>>(V, nV, F, vf_off, vf_faces, N);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_frames(const float* N0, const int* knnV, int kproj, int n, float* U, float* V, void* stream) {
+  if (n < 0 || kproj < 1 || (n > 0 && (!N0 || !knnV || !U || !V))) return fail(CVT_ERR_INVALID, "cvt_frames: bad arguments");
+  if (n == 0) return CVT_OK;
+  k_stage_frames<<<cdiv(n, 256), 256, 0, S_(stream)>>>(N0, knnV, kproj, n, U, V);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+constexpr int kClipBlock = 128;
+constexpr int kClipCap = 32;
+
+template <int PROF>
+static cvt_status_t clip_dispatch(const float* S, const float* U, const float* V, const uint32_t* knn, int n, int K, float R,
+                                  float* cent, int* nverts, cudaStream_t st) {
+  Scratch sc(st);
+  int* ovf;
+  CK(sc.get(&ovf, (size_t)n + 1));
+  CK(cudaMemsetAsync(ovf, 0, sizeof(int), st));
+  const size_t smem = 2 * kClipCap * kClipBlock * sizeof(V2<float>);
+  static bool attr = false;
+  if (!attr) {
+    CK(cudaFuncSetAttribute(k_stage_clip<PROF, kClipBlock, kClipCap>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr = true;
+  }
+  k_stage_clip<PROF, kClipBlock, kClipCap><<<cdiv(n, kClipBlock), kClipBlock, smem, st>>>(S, U, V, knn, n, K, R, cent, nverts, ovf);
+  CKLAUNCH();
+  k_stage_clip_fallback<PROF><<<148, 64, 0, st>>>(S, U, V, knn, n, K, R, cent, nverts, ovf);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_clip_centroids(const float* S, const float* U, const float* V, const uint32_t* knn, int n,
+                                           int K, float R, int profile, float* cent, int* nverts, void* stream) {
+  if (n < 0 || K < 1 || (n > 0 && (!S || !U || !V || !knn || !cent))) return fail(CVT_ERR_INVALID, "cvt_clip_centroids: bad arguments");
+  if (profile != CVT_PROFILE_REF && profile != CVT_PROFILE_MIXED)
+    return fail(CVT_ERR_UNSUPPORTED, "cvt_clip_centroids: profile must be REF or MIXED (FP64 runs in the engine)");
+  if (n == 0) return CVT_OK;
+  if (profile == CVT_PROFILE_REF) return clip_dispatch<PROF_REF>(S, U, V, knn, n, K, R, cent, nverts, S_(stream));
+  return clip_dispatch<PROF_MIXED>(S, U, V, knn, n, K, R, cent, nverts, S_(stream));
+}
+
+extern "C" cvt_status_t cvt_project(const float* cent, const float* V, const int* F, const int* vf_off, const int* vf_faces,
+                                    const int* knnV, int kproj, int nV, int nF, int nQ, int profile, const float* Sold,
+                                    float* Snew, void* stream) {
+  if (nQ < 0 || kproj < 1 || kproj > 16 || (nQ > 0 && (!cent || !V || !F || !vf_off || !vf_faces || !knnV || !Snew)))
+    return fail(CVT_ERR_INVALID, "cvt_project: bad arguments");
+  if (profile == CVT_PROFILE_MIXED && nQ > 0 && !Sold) return fail(CVT_ERR_INVALID, "cvt_project: MIXED needs Sold");
+  if (profile != CVT_PROFILE_REF && profile != CVT_PROFILE_MIXED) return fail(CVT_ERR_UNSUPPORTED, "cvt_project: profile");
+  if (nQ == 0) return CVT_OK;
+  if (profile == CVT_PROFILE_REF)
+    k_stage_project<PROF_REF><<<cdiv(nQ, 128), 128, 0, S_(stream)>>>(cent, V, F, vf_off, vf_faces, knnV, kproj, nV, nF, nQ, Sold, Snew);
+  else
+    k_stage_project<PROF_MIXED><<<cdiv(nQ, 128), 128, 0, S_(stream)>>>(cent, V, F, vf_off, vf_faces, knnV, kproj, nV, nF, nQ, Sold, Snew);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_freeze(const float* S, const float* Snew, const uint32_t* knn, const uint32_t* prev_knn, int n,
+                                   int K, int has_prev, const uint8_t* tier, const float* thr2_tier, const int* need_tier,
+                                   uint8_t* streak, uint8_t* cand, uint8_t* frozen, int* counts, void* stream) {
+  if (n < 0 || K < 1 || !thr2_tier || !need_tier ||
+      (n > 0 && (!S || !Snew || !knn || !prev_knn || !streak || !cand || !frozen || !counts)))
+    return fail(CVT_ERR_INVALID, "cvt_freeze: bad arguments");
+  if (n == 0) return CVT_OK;
+  FreezeTable tab;
+  for (int t = 0; t < 6; ++t) { tab.thr2[t] = thr2_tier[t]; tab.need[t] = need_tier[t]; }
+  k_stage_freeze<<<cdiv(n, 256), 256, 0, S_(stream)>>>(S, Snew, knn, prev_knn, n, K, has_prev, tier, tab, streak, cand, frozen, counts);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_count_frozen(const uint8_t* frozen, int n, int* out_sum, void* stream) {
+  if (n < 0 || !out_sum || (n > 0 && !frozen)) return fail(CVT_ERR_INVALID, "cvt_count_frozen: bad arguments");
+  if (n == 0) return CVT_OK;
+  k_stage_count_frozen<<<cdiv(n, 256), 256, 0, S_(stream)>>>(frozen, n, out_sum);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_tiers(int mode, int n, int K, const float* site_normal, const uint32_t* knn, uint8_t* tier,
+                                  void* stream) {
+  if ((mode != 1 && mode != 2) || n < 0 || K < 1 || (n > 0 && (!site_normal || !knn || !tier)))
+    return fail(CVT_ERR_INVALID, "cvt_tiers: bad arguments");
+  if (n == 0) return CVT_OK;
+  k_stage_tiers<<<cdiv(n, 128), 128, 0, S_(stream)>>>(mode, n, K, site_normal, knn, tier);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// resident meshes
+// ---------------------------------------------------------------------------
+struct cvt_mesh {
+  int nV = 0, nF = 0;
+  float R = 0.f, area = 0.f, lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0}, diag = 0.f;
+  float* dV = nullptr;
+  int* dF = nullptr;
+  int* doff = nullptr;
+  int* dfcs = nullptr;
+  float* dN = nullptr;
+  GridGeom vg{};
+  int* dvcell_start = nullptr;
+  Pt4<float>* dvsorted = nullptr;
+  BVHNode* dnodes = nullptr;
+  int* dtri = nullptr;
+  int nnodes = 0;
+  size_t bytes = 0;
+  std::vector<float> hV;
+  std::vector<int> hF;
+  MeshDev dev() const {
+    MeshDev m;
+    m.V = dV; m.F = dF; m.vf_off = doff; m.vf_faces = dfcs; m.N = dN;
+    m.vcell_start = dvcell_start; m.vsorted = dvsorted; m.vg = vg;
+    m.nV = nV; m.nF = nF; m.R = R;
+    m.thr2 = ((0.01f * R) * 0.01f) * R;
+    return m;
+  }
+};
+
+static void mesh_free(cvt_mesh* m) {
+  if (!m) return;
+  cudaFree(m->dV); cudaFree(m->dF); cudaFree(m->doff); cudaFree(m->dfcs); cudaFree(m->dN);
+  cudaFree(m->dvcell_start); cudaFree(m->dvsorted); cudaFree(m->dnodes); cudaFree(m->dtri);
+  delete m;
+}
+
+template <class X> static cudaError_t dmalloc(X** p, size_t count, size_t* acc) {
+  *acc += std::max<size_t>(count * sizeof(X), 16);
+  return cudaMalloc((void**)p, std::max<size_t>(count * sizeof(X), 16));
+}
+
+// Uniform grid for surface points: cell edge = factor * radius expected to
+// hold k points at the surface density n/area; at most max_cells cells.
+static GridGeom surface_grid(const float lo[3], const float hi[3], double area, long n, double k, double factor,
+                             long max_cells) {
+  GridGeom g{};
+  double ext[3] = {(double)hi[0] - lo[0], (double)hi[1] - lo[1], (double)hi[2] - lo[2]};
+  double emax = std::max({ext[0], ext[1], ext[2], 1e-20});
+  double dens = (double)std::max<long>(n, 1) / std::max(area, 1e-30);
+  double h = factor * std::sqrt(k / (M_PI * dens));
+  h = std::max(h, emax / 2048.0);
+  if (!(h > 0) || !std::isfinite(h)) h = emax;
+  double pad = 1e-4 * emax;
+  for (int it = 0; it < 200; ++it) {
+    long prod = 1;
+    for (int a = 0; a < 3; ++a) {
+      g.dim[a] = std::max(1, (int)std::ceil((ext[a] + 2 * pad) / h));
+      prod *= g.dim[a];
+    }
+    if (prod <= max_cells) break;
+    h *= 1.05;
+  }
+  for (int a = 0; a < 3; ++a) g.lo[a] = (float)(lo[a] - pad);
+  g.h = (float)h;
+  g.inv_h = (float)(1.0 / h);
+  g.cell_base = 0;
+  g.ncell = g.dim[0] * g.dim[1] * g.dim[2];
+  return g;
+}
+
+static float g_vcell_factor = 1.5f;
+
+extern "C" void cvt_set_vertex_cell_factor(float f) { if (f > 0.f) g_vcell_factor = f; }
+
+extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, int nF, cvt_mesh_t* out) {
+  if (!out || !V || !F || nV <= 0 || nF <= 0) return fail(CVT_ERR_INVALID, "cvt_mesh_create: empty mesh or null pointer");
+  for (long k = 0; k < 3L * nF; ++k)
+    if (F[k] < 0 || F[k] >= nV) return fail(CVT_ERR_INVALID, "cvt_mesh_create: face index out of range");
+  cvt_mesh* m = new cvt_mesh();
+  // R over every input vertex (main.cu:169-227)
+  float bmin[3] = {1e30f, 1e30f, 1e30f}, bmax[3] = {-1e30f, -1e30f, -1e30f};
+  for (int i = 0; i < nV; ++i)
+    for (int a = 0; a < 3; ++a) {
+      bmin[a] = std::fmin(bmin[a], V[3 * i + a]);
+      bmax[a] = std::fmax(bmax[a], V[3 * i + a]);
+    }
+  m->R = std::fmax(bmax[0] - bmin[0], std::fmax(bmax[1] - bmin[1], bmax[2] - bmin[2]));
+  // compaction (main.cu:230-257)
+  std::vector<int> remap(nV, -1);
+  std::vector<unsigned char> used(nV, 0);
+  for (long k = 0; k < 3L * nF; ++k) used[F[k]] = 1;
+  int nn = 0;
+  for (int i = 0; i < nV; ++i) if (used[i]) remap[i] = nn++;
+  m->nV = nn;
+  m->nF = nF;
+  m->hV.resize(3 * (size_t)nn);
+  for (int i = 0; i < nV; ++i)
+    if (remap[i] >= 0) for (int a = 0; a < 3; ++a) m->hV[3 * (size_t)remap[i] + a] = V[3 * i + a];
+  m->hF.resize(3 * (size_t)nF);
+  for (long k = 0; k < 3L * nF; ++k) m->hF[k] = remap[F[k]];
+  double area = 0.0;
+  for (int a = 0; a < 3; ++a) { m->lo[a] = 1e30f; m->hi[a] = -1e30f; }
+  for (int i = 0; i < nn; ++i)
+    for (int a = 0; a < 3; ++a) {
+      m->lo[a] = std::fmin(m->lo[a], m->hV[3 * i + a]);
+      m->hi[a] = std::fmax(m->hi[a], m->hV[3 * i + a]);
+    }
+  for (int f = 0; f < nF; ++f) {
+    const float* a = &m->hV[3 * (size_t)m->hF[3 * f]];
+    const float* b = &m->hV[3 * (size_t)m->hF[3 * f + 1]];
+    const float* c = &m->hV[3 * (size_t)m->hF[3 * f + 2]];
+    double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
+    double e2[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
+    double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+    area += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+  }
+  m->area = (float)area;
+  double dx = (double)m->hi[0] - m->lo[0], dy = (double)m->hi[1] - m->lo[1], dz = (double)m->hi[2] - m->lo[2];
+  m->diag = (float)std::sqrt(dx * dx + dy * dy + dz * dz);
+  // vertex -> face CSR in face order (main.cu:259-285)
+  std::vector<int> off(nn + 1, 0), fcs(3 * (size_t)nF);
+  for (long k = 0; k < 3L * nF; ++k) off[m->hF[k] + 1]++;
+  for (int v = 0; v < nn; ++v) off[v + 1] += off[v];
+  {
+    std::vector<int> cur(off.begin(), off.end() - 1);
+    for (int f = 0; f < nF; ++f)
+      for (int k = 0; k < 3; ++k) fcs[cur[m->hF[3 * f + k]]++] = f;
+  }
+  std::vector<BVHNode> nodes;
+  std::vector<int> tri;
+  build_bvh_host(m->hV.data(), m->hF.data(), nF, 8, nodes, tri);
+  m->nnodes = (int)nodes.size();
+  m->vg = surface_grid(m->lo, m->hi, area, nn, 6.0, g_vcell_factor, 4L * nn + 64);
+  cudaError_t e = cudaSuccess;
+  size_t acc = 0;
+#define MCK(x)                                                                              \
+  do {                                                                                      \
+    e = (x);                                                                                \
+    if (e != cudaSuccess) {                                                                 \
+      mesh_free(m);                                                                         \
+      return fail(e == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,              \
+                  std::string("cvt_mesh_create: ") + cudaGetErrorString(e));                \
+    }                                                                                       \
+  } while (0)
+  MCK(dmalloc(&m->dV, 3 * (size_t)nn, &acc));
+  MCK(dmalloc(&m->dF, 3 * (size_t)nF, &acc));
+  MCK(dmalloc(&m->doff, (size_t)nn + 1, &acc));
+  MCK(dmalloc(&m->dfcs, 3 * (size_t)nF, &acc));
+  MCK(dmalloc(&m->dN, 3 * (size_t)nn, &acc));
+  MCK(dmalloc(&m->dvcell_start, (size_t)m->vg.ncell + 2, &acc));
+  MCK(dmalloc(&m->dvsorted, (size_t)nn, &acc));
+  MCK(dmalloc(&m->dnodes, nodes.size(), &acc));
+  MCK(dmalloc(&m->dtri, tri.size(), &acc));
+  m->bytes = acc;
+  cudaStream_t st = 0;
+  MCK(cudaMemcpyAsync(m->dV, m->hV.data(), sizeof(float) * 3 * nn, cudaMemcpyHostToDevice, st));
+  MCK(cudaMemcpyAsync(m->dF, m->hF.data(), sizeof(int) * 3 * (size_t)nF, cudaMemcpyHostToDevice, st));
+  MCK(cudaMemcpyAsync(m->doff, off.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice, st));
+  MCK(cudaMemcpyAsync(m->dfcs, fcs.data(), sizeof(int) * 3 * (size_t)nF, cudaMemcpyHostToDevice, st));
+  MCK(cudaMemcpyAsync(m->dnodes, nodes.data(), sizeof(BVHNode) * nodes.size(), cudaMemcpyHostToDevice, st));
+  MCK(cudaMemcpyAsync(m->dtri, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice, st));
+  k_stage_normals<<<cdiv(nn, 256), 256, 0, st>>>(m->dV, nn, m->dF, m->doff, m->dfcs, m->dN);
+  LAUNCHED(1);
+  MCK(cudaGetLastError());
+  {
+    Scratch sc(st);
+    PointGrid pg;
+    cvt_status_t s = build_point_grid(sc, m->dV, nn, 0.f, &m->vg, pg);
+    if (s != CVT_OK) { mesh_free(m); return s; }
+    MCK(cudaMemcpyAsync(m->dvcell_start, pg.cell_start, sizeof(int) * (m->vg.ncell + 2), cudaMemcpyDeviceToDevice, st));
+    MCK(cudaMemcpyAsync(m->dvsorted, pg.sorted, sizeof(Pt4<float>) * nn, cudaMemcpyDeviceToDevice, st));
+  }
+  MCK(cudaStreamSynchronize(st));
+#undef MCK
+  *out = m;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_mesh_info(cvt_mesh_t m, cvt_mesh_info_t* info) {
+  if (!m || !info) return fail(CVT_ERR_INVALID, "cvt_mesh_info: null");
+  info->nV = m->nV; info->nF = m->nF; info->R = m->R; info->area = m->area;
+  for (int a = 0; a < 3; ++a) { info->bbox_lo[a] = m->lo[a]; info->bbox_hi[a] = m->hi[a]; }
+  info->diag = m->diag;
+  info->device_bytes = m->bytes;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_mesh_device_arrays(cvt_mesh_t m, const float** V, const int** F, const float** N,
+                                               const int** vf_off, const int** vf_faces) {
+  if (!m) return fail(CVT_ERR_INVALID, "cvt_mesh_device_arrays: null");
+  if (V) *V = m->dV;
+  if (F) *F = m->dF;
+  if (N) *N = m->dN;
+  if (vf_off) *vf_off = m->doff;
+  if (vf_faces) *vf_faces = m->dfcs;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_mesh_destroy(cvt_mesh_t m) {
+  if (!m) return CVT_OK;
+  cudaDeviceSynchronize();
+  mesh_free(m);
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_hausdorff_to_mesh(cvt_mesh_t ref, const float* Vc, int nVc, const int* Fc, int nFc, float* out,
+                                              void* stream) {
+  if (!ref || !out || nVc < 0 || nFc < 0 || (nVc > 0 && !Vc) || (nFc > 0 && !Fc))
+    return fail(CVT_ERR_INVALID, "cvt_hausdorff_to_mesh: bad arguments");
+  cudaStream_t st = S_(stream);
+  long nP = (long)nVc + 4L * nFc;
+  if (nP == 0) { *out = 0.f; return CVT_OK; }
+  Scratch sc(st);
+  unsigned* bits;
+  int* ovf;
+  CK(sc.get(&bits, 1));
+  CK(sc.get(&ovf, 1));
+  CK(cudaMemsetAsync(bits, 0, sizeof(unsigned), st));
+  CK(cudaMemsetAsync(ovf, 0, sizeof(int), st));
+  k_hausdorff<<<cdiv(nP, 128), 128, 0, st>>>(Vc, nVc, Fc, nP, ref->dnodes, ref->dtri, ref->dV, ref->dF, bits, ovf);
+  CKLAUNCH();
+  unsigned hb = 0;
+  int ho = 0;
+  CK(cudaMemcpyAsync(&hb, bits, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&ho, ovf, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (ho) return fail(CVT_ERR_CAPACITY, "cvt_hausdorff_to_mesh: BVH deeper than the traversal stack");
+  float d2;
+  std::memcpy(&d2, &hb, sizeof(float));
+  *out = std::sqrt(d2);
+  return CVT_OK;
+}
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+extern "C" void cvt_params_default(cvt_params_t* p) {
+  if (!p) return;
+  p->k = 24;
+  p->mode = 0;
+  p->profile = CVT_PROFILE_REF;
+  p->kproj = 5;
+  p->ex_quirk = 1;
+  p->cell_factor = 1.1f;
+  p->use_graph = 1;
+}
+
+// first-fit interval allocator over [0, cap)
+struct RangeAlloc {
+  std::vector<std::pair<int, int>> free_;  // (start, len), sorted by start
+  void init(int cap) { free_.assign(1, {0, cap}); }
+  int take(int len) {
+    if (len <= 0) return -1;
+    for (size_t k = 0; k < free_.size(); ++k)
+      if (free_[k].second >= len) {
+        int s = free_[k].first;
+        free_[k].first += len;
+        free_[k].second -= len;
+        if (free_[k].second == 0) free_.erase(free_.begin() + k);
+        return s;
+      }
+    return -1;
+  }
+  void give(int s, int len) {
+    if (len <= 0) return;
+    free_.push_back({s, len});
+    std::sort(free_.begin(), free_.end());
+    std::vector<std::pair<int, int>> m;
+    for (auto& r : free_) {
+      if (!m.empty() && m.back().first + m.back().second == r.first) m.back().second += r.second;
+      else m.push_back(r);
+    }
+    free_.swap(m);
+  }
+};
+
+__global__ void k_fill_int(int* p, int n, int v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+__global__ void k_f32_to_f64(const float* a, double* b, long n) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (double)a[i];
+}
+__global__ void k_f64_to_f32(const double* a, float* b, long n) {
+  long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) b[i] = (float)a[i];
+}
+
+struct cvt_engine {
+  cvt_params_t p{};
+  int K = 24, max_seg = 0, max_sites = 0, max_cells = 0;
+  bool f64 = false;
+  // host mirrors
+  std::vector<SegDev> segs;
+  std::vector<GridGeom> geom;
+  std::vector<int> active;
+  std::vector<cvt_mesh_t> seg_mesh;
+  std::vector<int> seg_cells;  // cells reserved (spatial + NaN bucket)
+  std::vector<int> host_iters;
+  RangeAlloc site_alloc, cell_alloc;
+  int parity = 0;
+  // device
+  SegDev* d_segs = nullptr;
+  GridGeom* d_geom = nullptr;
+  int* d_active = nullptr;
+  MeshDev* d_meshes = nullptr;
+  int* d_site_seg = nullptr;
+  void* d_S[2] = {nullptr, nullptr};
+  uint32_t* d_knn[2] = {nullptr, nullptr};
+  int* d_knnv = nullptr;
+  int* d_nnv = nullptr;
+  uint8_t* d_frozen = nullptr;
+  uint8_t* d_streak = nullptr;
+  uint8_t* d_tier = nullptr;
+  int2* d_cellrank = nullptr;
+  void* d_sorted = nullptr;
+  int* d_cell_count = nullptr;
+  int* d_cell_start = nullptr;
+  int* d_part = nullptr;
+  int* d_stats = nullptr;
+  int* d_ovf = nullptr;
+  // graphs
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int graph_nodes = 0;
+  long long last_launches = 0;
+};
+
+static void engine_free(cvt_engine* e) {
+  if (!e) return;
+  for (int k = 0; k < 2; ++k) {
+    if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
+    cudaFree(e->d_S[k]);
+    cudaFree(e->d_knn[k]);
+  }
+  cudaFree(e->d_segs); cudaFree(e->d_geom); cudaFree(e->d_active); cudaFree(e->d_meshes); cudaFree(e->d_site_seg);
+  cudaFree(e->d_knnv); cudaFree(e->d_nnv); cudaFree(e->d_frozen); cudaFree(e->d_streak); cudaFree(e->d_tier);
+  cudaFree(e->d_cellrank); cudaFree(e->d_sorted); cudaFree(e->d_cell_count); cudaFree(e->d_cell_start);
+  cudaFree(e->d_part); cudaFree(e->d_stats); cudaFree(e->d_ovf);
+  delete e;
+}
+
+static bool k_supported(int k) { return k == 8 || k == 12 || k == 16 || k == 20 || k == 24 || k == 32; }
+
+extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segments, int max_sites, int max_cells,
+                                          cvt_engine_t* out) {
+  if (!p || !out || max_segments < 1 || max_sites < 1 || max_cells < 2)
+    return fail(CVT_ERR_INVALID, "cvt_engine_create: bad arguments");
+  if (!k_supported(p->k)) return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: k must be one of 8,12,16,20,24,32");
+  if (p->kproj != kKProj) return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: kproj must be 5");
+  if (p->mode < 0 || p->mode > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: mode must be 0, 1 or 2");
+  if (p->profile < 0 || p->profile > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: profile");
+  cvt_engine* e = new cvt_engine();
+  e->p = *p;
+  e->K = p->k;
+  e->f64 = p->profile == CVT_PROFILE_FP64;
+  e->max_seg = max_segments;
+  e->max_sites = max_sites;
+  e->max_cells = max_cells;
+  e->segs.assign(max_segments, SegDev{});
+  e->geom.assign(max_segments, GridGeom{});
+  e->active.assign(max_segments, 0);
+  e->seg_mesh.assign(max_segments, nullptr);
+  e->seg_cells.assign(max_segments, 0);
+  e->host_iters.assign(max_segments, 0);
+  e->site_alloc.init(max_sites);
+  e->cell_alloc.init(max_cells);
+  const size_t tsz = e->f64 ? sizeof(double) : sizeof(float);
+  const size_t psz = e->f64 ? sizeof(Pt4<double>) : sizeof(Pt4<float>);
+  cudaError_t err = cudaSuccess;
+#define ECK(x)                                                                               \
+  do {                                                                                       \
+    err = (x);                                                                               \
+    if (err != cudaSuccess) {                                                                \
+      engine_free(e);                                                                        \
+      return fail(err == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,             \
+                  std::string("cvt_engine_create: ") + cudaGetErrorString(err));             \
+    }                                                                                        \
+  } while (0)
+  const size_t ns = (size_t)max_sites;
+  ECK(cudaMalloc(&e->d_segs, sizeof(SegDev) * max_segments));
+  ECK(cudaMalloc(&e->d_geom, sizeof(GridGeom) * max_segments));
+  ECK(cudaMalloc(&e->d_active, sizeof(int) * max_segments));
+  ECK(cudaMalloc(&e->d_meshes, sizeof(MeshDev) * max_segments));
+  ECK(cudaMalloc(&e->d_site_seg, sizeof(int) * ns));
+  for (int k = 0; k < 2; ++k) {
+    ECK(cudaMalloc(&e->d_S[k], tsz * 3 * ns));
+    ECK(cudaMalloc(&e->d_knn[k], sizeof(uint32_t) * e->K * ns));
+  }
+  ECK(cudaMalloc(&e->d_knnv, sizeof(int) * kKProj * ns));
+  ECK(cudaMalloc(&e->d_nnv, sizeof(int) * ns));
+  ECK(cudaMalloc(&e->d_frozen, ns));
+  ECK(cudaMalloc(&e->d_streak, ns));
+  ECK(cudaMalloc(&e->d_tier, ns));
+  ECK(cudaMalloc(&e->d_cellrank, sizeof(int2) * ns));
+  ECK(cudaMalloc(&e->d_sorted, psz * ns));
+  ECK(cudaMalloc(&e->d_cell_count, sizeof(int) * (size_t)max_cells));
+  ECK(cudaMalloc(&e->d_cell_start, sizeof(int) * ((size_t)max_cells + 1)));
+  ECK(cudaMalloc(&e->d_part, sizeof(int) * ((size_t)scan_blocks(max_cells) + 2)));
+  ECK(cudaMalloc(&e->d_stats, sizeof(int) * (size_t)max_segments * kStatsRing * kStatsWords));
+  ECK(cudaMalloc(&e->d_ovf, sizeof(int) * (ns + 1)));
+  ECK(cudaMemset(e->d_active, 0, sizeof(int) * max_segments));
+  ECK(cudaMemset(e->d_segs, 0, sizeof(SegDev) * max_segments));
+  ECK(cudaMemset(e->d_geom, 0, sizeof(GridGeom) * max_segments));
+  ECK(cudaMemset(e->d_meshes, 0, sizeof(MeshDev) * max_segments));
+  ECK(cudaMemset(e->d_stats, 0, sizeof(int) * (size_t)max_segments * kStatsRing * kStatsWords));
+  ECK(cudaMemset(e->d_ovf, 0, sizeof(int)));
+  for (int k = 0; k < 2; ++k) {
+    ECK(cudaMemset(e->d_S[k], 0, tsz * 3 * ns));
+    ECK(cudaMemset(e->d_knn[k], 0, sizeof(uint32_t) * e->K * ns));
+  }
+  k_fill_int<<<cdiv((long)ns, 256), 256>>>(e->d_site_seg, (int)ns, -1);
+  LAUNCHED(1);
+  ECK(cudaGetLastError());
+  ECK(cudaDeviceSynchronize());
+#undef ECK
+  *out = e;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_destroy(cvt_engine_t e) {
+  if (!e) return CVT_OK;
+  cudaDeviceSynchronize();
+  engine_free(e);
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, const float* sites, int n,
+                                               int sites_on_device, int* seg_id, void* stream) {
+  if (!e || !mesh || !sites || n < 1 || !seg_id) return fail(CVT_ERR_INVALID, "cvt_engine_add_segment: bad arguments");
+  cudaStream_t st = S_(stream);
+  int s = -1;
+  for (int k = 0; k < e->max_seg; ++k) if (!e->active[k] && !e->seg_mesh[k]) { s = k; break; }
+  if (s < 0) return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: no free segment slot");
+  GridGeom g = surface_grid(mesh->lo, mesh->hi, mesh->area, n, (double)(e->K + 1), e->p.cell_factor, 8L * n + 64);
+  int cells = g.ncell + 1;
+  int base = e->site_alloc.take(n);
+  if (base < 0) return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: site capacity exhausted");
+  int cbase = e->cell_alloc.take(cells);
+  if (cbase < 0) { e->site_alloc.give(base, n); return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: cell capacity exhausted"); }
+  g.cell_base = cbase;
+  SegDev sd{};
+  sd.mesh = s;
+  sd.site_base = base;
+  sd.n_sites = n;
+  sd.mode = e->p.mode;
+  sd.ex_quirk = e->p.ex_quirk;
+  sd.iter = 0;
+  MeshDev md = mesh->dev();
+  static const int kStreak1[6] = {5, 10, 15, 20, 25, 25};  // main.cu:22, 543-553
+  static const int kStreak2[6] = {5, 10, 15, 20, 25, 10};  // main.cu:39, 554-563
+  for (int t = 0; t < 6; ++t) {
+    sd.thr2_tier[t] = md.thr2;
+    int stv = e->p.mode == 0 ? 5 : (e->p.mode == 1 ? kStreak1[t] : kStreak2[t]);
+    sd.need_tier[t] = std::max(1, stv - 1);
+  }
+  e->segs[s] = sd;
+  e->geom[s] = g;
+  e->active[s] = 1;
+  e->seg_mesh[s] = mesh;
+  e->seg_cells[s] = cells;
+  e->host_iters[s] = 0;
+  const size_t tsz = e->f64 ? sizeof(double) : sizeof(float);
+  CK(cudaMemcpyAsync(e->d_segs + s, &e->segs[s], sizeof(SegDev), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(e->d_geom + s, &e->geom[s], sizeof(GridGeom), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(e->d_meshes + s, &md, sizeof(MeshDev), cudaMemcpyHostToDevice, st));
+  char* Sdst = (char*)e->d_S[e->parity] + tsz * 3 * (size_t)base;
+  if (!e->f64) {
+    CK(cudaMemcpyAsync(Sdst, sites, sizeof(float) * 3 * (size_t)n,
+                       sites_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+  } else {
+    const float* src = sites;
+    Scratch sc(st);
+    if (!sites_on_device) {
+      float* tmp;
+      CK(sc.get(&tmp, 3 * (size_t)n));
+      CK(cudaMemcpyAsync(tmp, sites, sizeof(float) * 3 * (size_t)n, cudaMemcpyHostToDevice, st));
+      src = tmp;
+    }
+    k_f32_to_f64<<<cdiv(3L * n, 256), 256, 0, st>>>(src, (double*)Sdst, 3L * n);
+    CKLAUNCH();
+  }
+  k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(e->d_site_seg + base, n, s);
+  CKLAUNCH();
+  k_fill_int<<<cdiv(5L * n, 256), 256, 0, st>>>(e->d_knnv + 5L * base, 5 * n, -1);
+  CKLAUNCH();
+  CK(cudaMemsetAsync(e->d_frozen + base, 0, n, st));
+  CK(cudaMemsetAsync(e->d_streak + base, 0, n, st));
+  CK(cudaMemsetAsync(e->d_tier + base, 0, n, st));
+  for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(e->d_knn[k] + (size_t)e->K * base, 0, sizeof(uint32_t) * e->K * (size_t)n, st));
+  CK(cudaMemsetAsync(e->d_stats + (size_t)s * kStatsRing * kStatsWords, 0, sizeof(int) * kStatsRing * kStatsWords, st));
+  CK(cudaMemcpyAsync(e->d_active + s, &e->active[s], sizeof(int), cudaMemcpyHostToDevice, st));
+  // the host mirrors above are read by the async copies; keep them stable
+  CK(cudaStreamSynchronize(st));
+  *seg_id = s;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_remove_segment(cvt_engine_t e, int s) {
+  if (!e || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_remove_segment: bad segment");
+  CK(cudaDeviceSynchronize());
+  e->active[s] = 0;
+  CK(cudaMemcpy(e->d_active + s, &e->active[s], sizeof(int), cudaMemcpyHostToDevice));
+  k_fill_int<<<cdiv(e->segs[s].n_sites, 256), 256>>>(e->d_site_seg + e->segs[s].site_base, e->segs[s].n_sites, -1);
+  CKLAUNCH();
+  CK(cudaDeviceSynchronize());
+  e->site_alloc.give(e->segs[s].site_base, e->segs[s].n_sites);
+  e->cell_alloc.give(e->geom[s].cell_base, e->seg_cells[s]);
+  e->seg_mesh[s] = nullptr;
+  return CVT_OK;
+}
+
+constexpr int kCellBlockF = 128;
+constexpr int kCellBlockD = 64;
+constexpr int kCellCap = 32;
+
+template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
+  EngineArgs<T> a;
+  a.segs = e->d_segs; a.geom = e->d_geom; a.active = e->d_active; a.meshes = e->d_meshes; a.site_seg = e->d_site_seg;
+  a.S[0] = (T*)e->d_S[0]; a.S[1] = (T*)e->d_S[1];
+  a.knn[0] = e->d_knn[0]; a.knn[1] = e->d_knn[1];
+  a.knnv = e->d_knnv; a.nnv = e->d_nnv;
+  a.frozen = e->d_frozen; a.streak = e->d_streak; a.tier = e->d_tier;
+  a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
+  a.stats = e->d_stats; a.ovf = e->d_ovf; a.cent_dbg = nullptr; a.K = e->K;
+  return a;
+}
+
+template <class T, int KK>
+static void launch_site_knn(const EngineArgs<T>& a, int nsites, int parity, cudaStream_t st) {
+  k_site_knn<T, KK><<<cdiv(nsites, 128), 128, 0, st>>>(a, parity);
+}
+
+// ev (optional, 5 events): recorded before the grid build, after it, after
+// the KNN kernel, after the cell kernel and after the bookkeeping kernels
+template <int PROF>
+static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t st, int* nlaunch, cudaEvent_t* ev) {
+  using T = typename PT<PROF>::T;
+  using PP = typename PT<PROF>::PP;
+  EngineArgs<T> a = engine_args<T>(e);
+  const int ns = e->max_sites;
+  int L = 0;
+  if (ev) CK(cudaEventRecord(ev[0], st));
+  CK(cudaMemsetAsync(e->d_cell_count, 0, sizeof(int) * e->max_cells, st));
+  k_grid_count<T><<<cdiv(ns, 256), 256, 0, st>>>(ns, (const T*)e->d_S[parity], SegGrid{e->d_geom, e->d_site_seg, e->d_active},
+                                                 e->d_cell_count, e->d_cellrank);
+  L++;
+  launch_exclusive_scan(e->max_cells, e->d_cell_count, e->d_part, e->d_cell_start, st);
+  L += 3;
+  k_grid_scatter<T><<<cdiv(ns, 256), 256, 0, st>>>(ns, (const T*)e->d_S[parity], e->d_cellrank, e->d_cell_start,
+                                                   (Pt4<T>*)e->d_sorted);
+  L++;
+  if (ev) CK(cudaEventRecord(ev[1], st));
+  // cell_start[max_cells] is the number of gridded sites (read on the device)
+  a.total_cells = e->max_cells;
+  switch (e->K) {
+    case 8: launch_site_knn<T, 9>(a, ns, parity, st); break;
+    case 12: launch_site_knn<T, 13>(a, ns, parity, st); break;
+    case 16: launch_site_knn<T, 17>(a, ns, parity, st); break;
+    case 20: launch_site_knn<T, 21>(a, ns, parity, st); break;
+    case 24: launch_site_knn<T, 25>(a, ns, parity, st); break;
+    default: launch_site_knn<T, 33>(a, ns, parity, st); break;
+  }
+  L++;
+  if (ev) CK(cudaEventRecord(ev[2], st));
+  constexpr int BLK = sizeof(PP) == 8 ? kCellBlockD : kCellBlockF;
+  const size_t smem = 2 * kCellCap * BLK * sizeof(V2<PP>);
+  k_site_cell<PROF, BLK, kCellCap><<<cdiv(ns, BLK), BLK, smem, st>>>(a, parity);
+  L++;
+  if (ev) CK(cudaEventRecord(ev[3], st));
+  k_site_cell_fallback<PROF><<<148, 64, 0, st>>>(a, parity);
+  L++;
+  k_seg_advance<<<1, 256, 0, st>>>(e->d_segs, e->d_active, e->max_seg, e->d_stats, e->d_ovf);
+  L++;
+  if (ev) CK(cudaEventRecord(ev[4], st));
+  CK(cudaGetLastError());
+  *nlaunch = L;
+  return CVT_OK;
+}
+
+static cvt_status_t enqueue_iteration(cvt_engine* e, int parity, cudaStream_t st, int* nlaunch,
+                                      cudaEvent_t* ev = nullptr) {
+  switch (e->p.profile) {
+    case CVT_PROFILE_REF: return enqueue_iteration_t<PROF_REF>(e, parity, st, nlaunch, ev);
+    case CVT_PROFILE_MIXED: return enqueue_iteration_t<PROF_MIXED>(e, parity, st, nlaunch, ev);
+    default: return enqueue_iteration_t<PROF_FP64>(e, parity, st, nlaunch, ev);
+  }
+}
+
+static cvt_status_t set_smem_attrs(cvt_engine* e) {
+  static bool done[3] = {false, false, false};
+  int pr = e->p.profile;
+  if (done[pr]) return CVT_OK;
+  const int smemF = 2 * kCellCap * kCellBlockF * (int)sizeof(V2<float>);
+  const int smemD = 2 * kCellCap * kCellBlockD * (int)sizeof(V2<double>);
+  if (pr == CVT_PROFILE_REF)
+    CK(cudaFuncSetAttribute(k_site_cell<PROF_REF, kCellBlockF, kCellCap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemF));
+  else if (pr == CVT_PROFILE_MIXED)
+    CK(cudaFuncSetAttribute(k_site_cell<PROF_MIXED, kCellBlockF, kCellCap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemF));
+  else
+    CK(cudaFuncSetAttribute(k_site_cell<PROF_FP64, kCellBlockD, kCellCap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemD));
+  done[pr] = true;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream) {
+  if (!e || iters < 0) return fail(CVT_ERR_INVALID, "cvt_engine_run: bad arguments");
+  cudaStream_t st = S_(stream);
+  cvt_status_t s = set_smem_attrs(e);
+  if (s != CVT_OK) return s;
+  long long launches = 0;
+  for (int it = 0; it < iters; ++it) {
+    int par = e->parity;
+    int nl = 0;
+    if (e->p.use_graph) {
+      if (!e->gexec[par]) {
+        cudaStream_t cs;
+        CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+        cvt_status_t q = enqueue_iteration(e, par, cs, &nl);
+        cudaGraph_t gr = nullptr;
+        cudaError_t ce = cudaStreamEndCapture(cs, &gr);
+        cudaStreamDestroy(cs);
+        if (q != CVT_OK) { if (gr) cudaGraphDestroy(gr); return q; }
+        if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+        ce = cudaGraphInstantiate(&e->gexec[par], gr, 0);
+        cudaGraphDestroy(gr);
+        if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+        e->graph_nodes = nl;
+      }
+      CK(cudaGraphLaunch(e->gexec[par], st));
+      nl = e->graph_nodes;
+      LAUNCHED(nl);
+    } else {
+      s = enqueue_iteration(e, par, st, &nl);
+      if (s != CVT_OK) return s;
+      LAUNCHED(nl);
+    }
+    launches += nl;
+    e->parity ^= 1;
+    for (int k = 0; k < e->max_seg; ++k) if (e->active[k]) e->host_iters[k]++;
+  }
+  e->last_launches = launches;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms, void* stream) {
+  if (!e || !ms || iters < 1) return fail(CVT_ERR_INVALID, "cvt_engine_profile: bad arguments");
+  cudaStream_t st = S_(stream);
+  cvt_status_t s = set_smem_attrs(e);
+  if (s != CVT_OK) return s;
+  cudaEvent_t ev[5];
+  for (int k = 0; k < 5; ++k) CK(cudaEventCreate(&ev[k]));
+  double acc[4] = {0, 0, 0, 0};
+  for (int it = 0; it < iters; ++it) {
+    int nl = 0;
+    s = enqueue_iteration(e, e->parity, st, &nl, ev);
+    if (s != CVT_OK) break;
+    LAUNCHED(nl);
+    e->parity ^= 1;
+    for (int k = 0; k < e->max_seg; ++k) if (e->active[k]) e->host_iters[k]++;
+    CK(cudaEventSynchronize(ev[4]));
+    for (int k = 0; k < 4; ++k) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
+      acc[k] += t;
+    }
+  }
+  for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < 4; ++k) ms[k] = (float)(acc[k] / iters);
+  return s;
+}
+
+extern "C" cvt_status_t cvt_engine_get_sites(cvt_engine_t e, int s, float* out, int out_on_device, void* stream) {
+  if (!e || !out || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_get_sites: bad arguments");
+  cudaStream_t st = S_(stream);
+  const SegDev& sd = e->segs[s];
+  size_t cnt = 3 * (size_t)sd.n_sites;
+  if (!e->f64) {
+    const float* src = (const float*)e->d_S[e->parity] + 3 * (size_t)sd.site_base;
+    CK(cudaMemcpyAsync(out, src, sizeof(float) * cnt, out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+  } else {
+    const double* src = (const double*)e->d_S[e->parity] + 3 * (size_t)sd.site_base;
+    Scratch sc(st);
+    float* tmp = out;
+    if (!out_on_device) CK(sc.get(&tmp, cnt));
+    k_f64_to_f32<<<cdiv((long)cnt, 256), 256, 0, st>>>(src, tmp, (long)cnt);
+    CKLAUNCH();
+    if (!out_on_device) CK(cudaMemcpyAsync(out, tmp, sizeof(float) * cnt, cudaMemcpyDeviceToHost, st));
+  }
+  if (!out_on_device) CK(cudaStreamSynchronize(st));
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_get_sites_f64(cvt_engine_t e, int s, double* out, void* stream) {
+  if (!e || !out || s < 0 || s >= e->max_seg || !e->seg_mesh[s] || !e->f64)
+    return fail(CVT_ERR_INVALID, "cvt_engine_get_sites_f64: bad arguments (FP64 engines only)");
+  cudaStream_t st = S_(stream);
+  const SegDev& sd = e->segs[s];
+  const double* src = (const double*)e->d_S[e->parity] + 3 * (size_t)sd.site_base;
+  CK(cudaMemcpyAsync(out, src, sizeof(double) * 3 * (size_t)sd.n_sites, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_get_state(cvt_engine_t e, int s, uint32_t* knn, int* knnv, uint8_t* frozen,
+                                             uint8_t* tier, void* stream) {
+  if (!e || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_get_state: bad segment");
+  cudaStream_t st = S_(stream);
+  const SegDev& sd = e->segs[s];
+  const size_t n = sd.n_sites, b = sd.site_base;
+  // the list of the last completed iteration sits in the buffer it wrote
+  const uint32_t* kl = e->d_knn[e->parity ^ 1];
+  if (knn) CK(cudaMemcpyAsync(knn, kl + (size_t)e->K * b, sizeof(uint32_t) * e->K * n, cudaMemcpyDeviceToHost, st));
+  if (knnv) CK(cudaMemcpyAsync(knnv, e->d_knnv + 5 * b, sizeof(int) * 5 * n, cudaMemcpyDeviceToHost, st));
+  if (frozen) CK(cudaMemcpyAsync(frozen, e->d_frozen + b, n, cudaMemcpyDeviceToHost, st));
+  if (tier) CK(cudaMemcpyAsync(tier, e->d_tier + b, n, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_get_stats(cvt_engine_t e, int s, int iter, cvt_iter_stats_t* out, void* stream) {
+  if (!e || !out || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_get_stats: bad segment");
+  if (iter < 0 || iter >= e->host_iters[s] || iter < e->host_iters[s] - kStatsRing)
+    return fail(CVT_ERR_INVALID, "cvt_engine_get_stats: iteration not held");
+  cudaStream_t st = S_(stream);
+  int w[kStatsWords];
+  CK(cudaMemcpyAsync(w, e->d_stats + ((size_t)s * kStatsRing + (iter % kStatsRing)) * kStatsWords, sizeof(w),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  out->same = w[0]; out->low = w[1]; out->both = w[2]; out->newly_frozen = w[3];
+  float d2;
+  std::memcpy(&d2, &w[4], sizeof(float));
+  out->max_motion = std::sqrt(d2);
+  out->iter = w[5];
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_segment_iters(cvt_engine_t e, int s, int* iters) {
+  if (!e || !iters || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_segment_iters: bad segment");
+  *iters = e->host_iters[s];
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n) {
+  if (!e || !n) return fail(CVT_ERR_INVALID, "cvt_engine_last_launches: null");
+  *n = e->last_launches;
+  return CVT_OK;
+}
+
+// capacity for one mesh + site set
+static void engine_caps(const cvt_mesh* m, int n, const cvt_params_t* p, int* cells) {
+  GridGeom g = surface_grid(m->lo, m->hi, m->area, n, (double)(p->k + 1), p->cell_factor, 8L * n + 64);
+  *cells = g.ncell + 1;
+}
+
+extern "C" cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF, const float* sites_in, int n_sites,
+                                   const cvt_params_t* p, int iters, float* sites_out, int* counts) {
+  if (!V || !F || !sites_in || !sites_out || !p || n_sites < 1 || iters < 0)
+    return fail(CVT_ERR_INVALID, "cvt_remesh: bad arguments");
+  cvt_mesh_t m = nullptr;
+  cvt_status_t s = cvt_mesh_create(V, nV, F, nF, &m);
+  if (s != CVT_OK) return s;
+  int cells = 0;
+  engine_caps(m, n_sites, p, &cells);
+  cvt_engine_t e = nullptr;
+  s = cvt_engine_create(p, 1, n_sites, cells, &e);
+  if (s != CVT_OK) { cvt_mesh_destroy(m); return s; }
+  int seg = -1;
+  s = cvt_engine_add_segment(e, m, sites_in, n_sites, 0, &seg, nullptr);
+  if (s == CVT_OK) s = cvt_engine_run(e, iters, nullptr);
+  if (s == CVT_OK) s = cvt_engine_get_sites(e, seg, sites_out, 0, nullptr);
+  if (s == CVT_OK && counts) {
+    int lo = std::max(0, iters - kStatsRing);
+    for (int it = 0; it < iters && s == CVT_OK; ++it) {
+      if (it < lo) { for (int a = 0; a < 4; ++a) counts[4 * it + a] = -1; continue; }
+      cvt_iter_stats_t t;
+      s = cvt_engine_get_stats(e, seg, it, &t, nullptr);
+      counts[4 * it + 0] = t.same; counts[4 * it + 1] = t.low; counts[4 * it + 2] = t.both; counts[4 * it + 3] = t.newly_frozen;
+    }
+  }
+  cvt_engine_destroy(e);
+  cvt_mesh_destroy(m);
+  return s;
+}

@@ -1,0 +1,502 @@
+// Fused Lloyd-iteration kernels over many (mesh, site set) segments.
+//
+// One iteration (main.cu:669-881 per segment) is:
+//   grid build over all active sites   (count -> scan -> scatter)
+//   k_site_knn   per site: exact (K+1)-NN in its segment, drop self
+//                (site_knn.cuh:79), restore the previous list for frozen
+//                sites (main.cu:678), nearest mesh vertex for the frame
+//                (main.cu:685-700)
+//   k_site_cell  per site: frame (site_normals.cuh:69), tangent-plane clip
+//                and centroid (2dClip.cuh:82), centroid -> 5 nearest
+//                vertices (main.cu:719-735, frozen sites keep theirs),
+//                one-ring projection (near_project.cuh:149), freeze test
+//                and apply (freezetest.cuh:155-212, 270-327, 451-466),
+//                tier assignment on the segment's first iteration
+//                (main.cu:640-667)
+//   k_site_cell_fallback  the same for the rare cells whose polygon
+//                outgrows the shared-memory buffer (exact 64-vertex cap)
+//   k_seg_advance  per-segment iteration counters / statistics slots
+// All sizes come from device memory, so the whole iteration is captured once
+// in a CUDA graph and relaunched while segments come and go.
+#pragma once
+#include "cvt_grid.cuh"
+
+namespace cvt {
+
+constexpr int kStatsRing = 256;   // iterations of per-segment statistics kept
+constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter, -, -
+constexpr int kKProj = 5;         // KPROJ (main.cu:394)
+constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
+
+struct MeshDev {
+  const float* V;
+  const int* F;
+  const int* vf_off;
+  const int* vf_faces;
+  const float* N;
+  const int* vcell_start;
+  const Pt4<float>* vsorted;
+  GridGeom vg;
+  int nV, nF;
+  float R;     // clip square half-size: longest input bbox edge (main.cu:421)
+  float thr2;  // freeze displacement threshold, squared (main.cu:431)
+};
+
+struct SegDev {
+  int mesh;       // index into the mesh table
+  int site_base;  // first global site index
+  int n_sites;
+  int mode;       // 0 / 1 / 2
+  int ex_quirk;
+  int iter;       // iterations completed (device-side count)
+  float thr2_tier[6];
+  int need_tier[6];
+};
+
+template <int PROF> struct PT;
+template <> struct PT<PROF_REF> { using T = float; using Q = float; using PP = float; };
+template <> struct PT<PROF_MIXED> { using T = float; using Q = double; using PP = float; };
+template <> struct PT<PROF_FP64> { using T = double; using Q = double; using PP = double; };
+
+template <class T> struct EngineArgs {
+  const SegDev* segs;
+  const GridGeom* geom;
+  const int* active;
+  const MeshDev* meshes;
+  const int* site_seg;
+  T* S[2];
+  uint32_t* knn[2];
+  int* knnv;
+  int* nnv;
+  uint8_t* frozen;
+  uint8_t* streak;
+  uint8_t* tier;
+  const int* cell_start;
+  const Pt4<T>* sorted;
+  int total_cells;
+  int* stats;
+  int* ovf;  // [0] = count, [1 + k] = overflowed site
+  T* cent_dbg;
+  int K;
+};
+
+// polygon storage: vertex k at p[k * stride] (shared memory: thread-
+// interleaved; local memory: stride 1)
+template <class PP> struct PolyRef {
+  V2<PP>* p;
+  int stride;
+  __device__ __forceinline__ V2<PP> get(int k) const { return p[k * stride]; }
+  __device__ __forceinline__ void set(int k, V2<PP> v) const { p[k * stride] = v; }
+};
+
+// Sutherland-Hodgman clip by a*x + b*y - c <= eps (2dClip.cuh:11-53).  Stops
+// with ovf = true before writing vertex `cap` (buffer full); keeps the
+// reference's 64-vertex cap (2dClip.cuh:47-50) for larger buffers.
+template <class PP, class Q>
+__device__ __forceinline__ int clip_poly(const PolyRef<PP>& in, int n, const PolyRef<PP>& out, Q a, Q b, Q c,
+                                         Q eps, int cap, bool& ovf) {
+  if (n <= 0) return 0;
+  auto f = [&](V2<PP> p) -> Q { return fmaT(a, (Q)p.x, fmaT(b, (Q)p.y, -c)); };
+  auto isect = [&](V2<PP> s, V2<PP> e, Q fs, Q fe) -> V2<PP> {
+    Q t = divT(fs, (fs - fe) + (Q)1e-30);
+    return {(PP)fmaT(t, (Q)e.x - (Q)s.x, (Q)s.x), (PP)fmaT(t, (Q)e.y - (Q)s.y, (Q)s.y)};
+  };
+  V2<PP> s = in.get(n - 1);
+  Q fs = f(s);
+  bool ins_s = fs <= eps;
+  int m = 0;
+  for (int i = 0; i < n; ++i) {
+    V2<PP> e = in.get(i);
+    Q fe = f(e);
+    bool ins_e = fe <= eps;
+    if (ins_e) {
+      if (!ins_s) {
+        if (m >= cap) { ovf = true; return m; }
+        out.set(m++, isect(s, e, fs, fe));
+      }
+      if (m >= cap) { ovf = true; return m; }
+      out.set(m++, e);
+    } else if (ins_s) {
+      if (m >= cap) { ovf = true; return m; }
+      out.set(m++, isect(s, e, fs, fe));
+    }
+    s = e; fs = fe; ins_s = ins_e;
+    if (m >= 64) { m = 64; break; }
+  }
+  return m;
+}
+
+// Clip the square [-R,R]^2 by the bisectors of the listed neighbours; returns
+// the vertex count (polygon in `cur` on return) or -1 on buffer overflow.
+template <int PROF>
+__device__ __forceinline__ int clip_cell(const typename PT<PROF>::T* __restrict__ S, int site_base, int n_sites,
+                                         V3<typename PT<PROF>::T> si, const uint32_t* __restrict__ row, int K,
+                                         const Frame<typename PT<PROF>::T>& fr, float R,
+                                         PolyRef<typename PT<PROF>::PP>& cur, PolyRef<typename PT<PROF>::PP>& nxt,
+                                         int cap) {
+  using T = typename PT<PROF>::T;
+  using Q = typename PT<PROF>::Q;
+  using PP = typename PT<PROF>::PP;
+  const PP r = (PP)R;
+  cur.set(0, {-r, -r}); cur.set(1, {r, -r}); cur.set(2, {r, r}); cur.set(3, {-r, r});
+  int n = 4;
+  bool ovf = false;
+  for (int t = 0; t < K; ++t) {
+    uint32_t j = __ldg(row + t);
+    if (j >= (uint32_t)n_sites) continue;
+    V3<T> sj = ld3(S, (long)site_base + j);
+    Q a, b, c;
+    if (PROF == PROF_MIXED) {
+      V3<double> d{(double)sj.x - (double)si.x, (double)sj.y - (double)si.y, (double)sj.z - (double)si.z};
+      V3<double> u = cvt3<double>(fr.u), v = cvt3<double>(fr.v);
+      a = (Q)dot3(d, u); b = (Q)dot3(d, v); c = (Q)(0.5 * dot3(d, d));
+    } else {
+      V3<T> d = sub3(sj, si);
+      a = (Q)dot3(d, fr.u); b = (Q)dot3(d, fr.v); c = (Q)((T)0.5 * dot3(d, d));
+    }
+    n = clip_poly<PP, Q>(cur, n, nxt, a, b, c, (Q)1e-12, cap, ovf);
+    if (ovf) return -1;
+    PolyRef<PP> tmp = cur; cur = nxt; nxt = tmp;
+    if (n == 0) break;
+  }
+  return n;
+}
+
+// ---------------------------------------------------------------------------
+// tiers (main.cu:18-150) in FP64, identical operation order to the host code
+// ---------------------------------------------------------------------------
+__device__ inline void sym3_eigenvalues_d(const double C[9], double lam[3]) {
+  double v[3] = {1.0, 0.0, 0.0};
+  for (int it = 0; it < 20; ++it) {
+    double w[3] = {C[0] * v[0] + C[1] * v[1] + C[2] * v[2], C[3] * v[0] + C[4] * v[1] + C[5] * v[2],
+                   C[6] * v[0] + C[7] * v[1] + C[8] * v[2]};
+    double n = __dsqrt_rn(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    if (n < 1e-30) break;
+    v[0] = __ddiv_rn(w[0], n); v[1] = __ddiv_rn(w[1], n); v[2] = __ddiv_rn(w[2], n);
+  }
+  lam[0] = v[0] * (C[0] * v[0] + C[1] * v[1] + C[2] * v[2]) + v[1] * (C[3] * v[0] + C[4] * v[1] + C[5] * v[2]) +
+           v[2] * (C[6] * v[0] + C[7] * v[1] + C[8] * v[2]);
+  double C2[9];
+  for (int i = 0; i < 9; ++i) C2[i] = C[i];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) C2[3 * r + c] -= lam[0] * v[r] * v[c];
+  double v2[3] = {0.0, 1.0, 0.0};
+  for (int it = 0; it < 20; ++it) {
+    double w[3] = {C2[0] * v2[0] + C2[1] * v2[1] + C2[2] * v2[2], C2[3] * v2[0] + C2[4] * v2[1] + C2[5] * v2[2],
+                   C2[6] * v2[0] + C2[7] * v2[1] + C2[8] * v2[2]};
+    double n = __dsqrt_rn(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+    if (n < 1e-30) break;
+    v2[0] = __ddiv_rn(w[0], n); v2[1] = __ddiv_rn(w[1], n); v2[2] = __ddiv_rn(w[2], n);
+  }
+  lam[1] = v2[0] * (C2[0] * v2[0] + C2[1] * v2[1] + C2[2] * v2[2]) + v2[1] * (C2[3] * v2[0] + C2[4] * v2[1] + C2[5] * v2[2]) +
+           v2[2] * (C2[6] * v2[0] + C2[7] * v2[1] + C2[8] * v2[2]);
+  lam[2] = C[0] + C[4] + C[8] - lam[0] - lam[1];
+}
+
+// normal(i) gives the unit normal of local site i as float[3]
+template <class NormalOf>
+__device__ inline int tier_of(int mode, int i, int n, int K, const uint32_t* row, NormalOf normal) {
+  const double TH[4] = {0.15, 0.35, 0.55, 0.80};
+  float ni[3];
+  normal(i, ni);
+  double sum = 0.0;
+  int cnt = 0;
+  for (int j = 0; j < K; ++j) {
+    int jj = (int)row[j];
+    if (jj < 0 || jj >= n) continue;
+    float nj[3];
+    normal(jj, nj);
+    double c = (double)ni[0] * (double)nj[0] + (double)ni[1] * (double)nj[1] + (double)ni[2] * (double)nj[2];
+    if (c > 1.0) c = 1.0;
+    if (c < -1.0) c = -1.0;
+    sum += c;
+    cnt++;
+  }
+  double nv = cnt > 0 ? (1.0 - __ddiv_rn(sum, (double)cnt)) : 0.0;
+  double L = 0.0;
+  if (mode == 2) {
+    double mean[3] = {0, 0, 0};
+    int c2 = 0;
+    for (int j = 0; j < K; ++j) {
+      int jj = (int)row[j];
+      if (jj < 0 || jj >= n) continue;
+      float nj[3];
+      normal(jj, nj);
+      for (int a = 0; a < 3; ++a) mean[a] += (double)nj[a];
+      c2++;
+    }
+    if (c2 >= 2) {
+      for (int a = 0; a < 3; ++a) mean[a] = __ddiv_rn(mean[a], (double)c2);
+      double C[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int j = 0; j < K; ++j) {
+        int jj = (int)row[j];
+        if (jj < 0 || jj >= n) continue;
+        float nj[3];
+        normal(jj, nj);
+        double d[3] = {(double)nj[0] - mean[0], (double)nj[1] - mean[1], (double)nj[2] - mean[2]};
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) C[3 * r + c] += d[r] * d[c];
+      }
+      double lam[3];
+      sym3_eigenvalues_d(C, lam);
+      double tmp;
+      if (lam[0] > lam[1]) { tmp = lam[0]; lam[0] = lam[1]; lam[1] = tmp; }
+      if (lam[1] > lam[2]) { tmp = lam[1]; lam[1] = lam[2]; lam[2] = tmp; }
+      if (lam[0] > lam[1]) { tmp = lam[0]; lam[0] = lam[1]; lam[1] = tmp; }
+      if (lam[2] > 1e-30) L = __ddiv_rn(lam[2] - lam[1], lam[2]);
+    }
+  }
+  int t = 0;
+  while (t < 4 && nv >= TH[t]) t++;
+  if (mode == 2 && t == 4 && L > 0.80) t = 5;
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// k_site_knn
+// ---------------------------------------------------------------------------
+template <class T, int KK>
+__global__ void __launch_bounds__(128) k_site_knn(EngineArgs<T> a, int parity) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n_grid = __ldg(a.cell_start + a.total_cells);
+  if (t >= n_grid) return;
+  const Pt4<T> me = a.sorted[t];
+  const int g = (int)me.id;
+  const int s = __ldg(a.site_seg + g);
+  const SegDev& sd = a.segs[s];
+  const MeshDev& md = a.meshes[sd.mesh];
+  constexpr int K = KK - 1;
+  uint32_t* row = a.knn[parity] + (size_t)g * K;
+  if (sd.mode != 0 && a.frozen[g]) {
+    const uint32_t* prow = a.knn[parity ^ 1] + (size_t)g * K;
+#pragma unroll
+    for (int k = 0; k < K; k += 4)
+      *reinterpret_cast<uint4*>(row + k) = *reinterpret_cast<const uint4*>(prow + k);
+    a.nnv[g] = a.knnv[(size_t)g * kKProj];
+    return;
+  }
+  const V3<T> q{me.x, me.y, me.z};
+  const GridGeom G = a.geom[s];
+  TopK<T, KK> top;
+  grid_knn<T, T, KK>(G, a.cell_start, a.sorted, q, top, [](uint32_t) { return true; });
+  // drop self (site_knn.cuh:79-103); local indices.  A point occurs at most
+  // once in the list, so dropping it is a shift of the entries after it and
+  // the K kept entries never need the reference's pad-with-last fallback.
+  const uint32_t base = (uint32_t)sd.site_base;
+  const uint32_t i = (uint32_t)g - base;
+  uint32_t loc[KK];
+  int p = K;
+#pragma unroll
+  for (int k = KK - 1; k >= 0; --k) {
+    uint32_t gid = KeyOps<T>::idx(top.k[k]);
+    loc[k] = gid == 0xffffffffu ? 0xffffffffu : gid - base;
+    if (loc[k] == i) p = k;
+  }
+#pragma unroll
+  for (int k = 0; k < K; k += 4) {
+    uint4 v;
+    v.x = (k + 0 < p) ? loc[k + 0] : loc[k + 1];
+    v.y = (k + 1 < p) ? loc[k + 1] : loc[k + 2];
+    v.z = (k + 2 < p) ? loc[k + 2] : loc[k + 3];
+    v.w = (k + 3 < p) ? loc[k + 3] : loc[k + 4];
+    *reinterpret_cast<uint4*>(row + k) = v;
+  }
+  // nearest mesh vertex of the site (frame vertex)
+  TopK<T, 1> v1;
+  grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, v1, [](uint32_t) { return true; });
+  a.nnv[g] = (int)KeyOps<T>::idx(v1.k[0]);
+}
+
+// ---------------------------------------------------------------------------
+// per-site step after the KNN
+// ---------------------------------------------------------------------------
+struct SiteOut {
+  int seg;
+  int same, low, both, newly;
+  float disp2;
+};
+
+template <int PROF>
+__device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g,
+                                          PolyRef<typename PT<PROF>::PP> A, PolyRef<typename PT<PROF>::PP> B,
+                                          int cap, SiteOut& o) {
+  using T = typename PT<PROF>::T;
+  using PP = typename PT<PROF>::PP;
+  const int s = __ldg(a.site_seg + g);
+  const SegDev& sd = a.segs[s];
+  const MeshDev& md = a.meshes[sd.mesh];
+  const int K = a.K;
+  const T* __restrict__ S = a.S[parity];
+  const uint32_t* row = a.knn[parity] + (size_t)g * K;
+  const int i = g - sd.site_base;
+  const bool fz = sd.mode != 0 && a.frozen[g];
+  const V3<T> si = ld3(S, g);
+
+  // frame from the nearest vertex normal
+  const int nn = a.nnv[g];
+  Frame<T> fr;
+  if (nn < 0) fr = {{(T)1, (T)0, (T)0}, {(T)0, (T)1, (T)0}};
+  else fr = frame_from_normal(V3<T>{(T)__ldg(md.N + 3 * nn), (T)__ldg(md.N + 3 * nn + 1), (T)__ldg(md.N + 3 * nn + 2)});
+
+  // clip + centroid
+  PolyRef<PP> cur = A, nxt = B;
+  const int np = clip_cell<PROF>(S, sd.site_base, sd.n_sites, si, row, K, fr, md.R, cur, nxt, cap);
+  if (np < 0) return false;
+  const V2<PP> c2 = poly_centroid<PP>(cur, np, PROF == PROF_MIXED);
+  V3<T> cent;
+  if (!(finiteT(c2.x) && finiteT(c2.y))) {
+    cent = {(T)NAN, (T)NAN, (T)NAN};
+  } else {
+    const T cx = (T)c2.x, cy = (T)c2.y;
+    cent = {si.x + fmaT(fr.u.x, cx, fr.v.x * cy), si.y + fmaT(fr.u.y, cx, fr.v.y * cy),
+            si.z + fmaT(fr.u.z, cx, fr.v.z * cy)};
+  }
+  if (a.cent_dbg) st3(a.cent_dbg, g, cent);
+
+  // centroid -> nearest mesh vertices (frozen sites keep theirs)
+  int* kv = a.knnv + (size_t)g * kKProj;
+  int knnv[kKProj];
+  if (!fz) {
+    TopK<T, kKProj> top;
+    const int skip = (sd.mode == 0 && sd.ex_quirk) ? i : -1;
+    grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, cent, top,
+                               [skip](uint32_t id) { return (int)id != skip; });
+#pragma unroll
+    for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];
+  }
+
+  // projection
+  V3<T> sn;
+  if (PROF == PROF_MIXED && !finite3(cent)) {
+    sn = si;
+  } else if (PROF == PROF_REF) {
+    sn = project_onering<T, float>(cent, md.V, md.nV, md.F, md.nF, md.vf_off, md.vf_faces, knnv, kKProj);
+  } else {
+    sn = project_onering<T, double>(cent, md.V, md.nV, md.F, md.nF, md.vf_off, md.vf_faces, knnv, kKProj);
+  }
+  st3(a.S[parity ^ 1], g, sn);
+
+  // tiers on the segment's first iteration (modes 1/2)
+  const int it = sd.iter;
+  if (it == 0 && sd.mode != 0) {
+    const int base = sd.site_base;
+    auto normal = [&](int j, float out[3]) {
+      int v = a.nnv[base + j];
+      if (v < 0) { out[0] = out[1] = out[2] = 0.f; return; }
+      out[0] = __ldg(md.N + 3 * v); out[1] = __ldg(md.N + 3 * v + 1); out[2] = __ldg(md.N + 3 * v + 2);
+    };
+    a.tier[g] = (uint8_t)tier_of(sd.mode, i, sd.n_sites, K, row, normal);
+  }
+
+  // freeze test + apply
+  o.seg = s;
+  o.same = o.low = o.both = o.newly = 0;
+  const T d2 = dist2(sn, si);
+  o.disp2 = (float)d2;
+  if (it == 0) {
+    a.streak[g] = 0;
+  } else {
+    const int tt = min((int)a.tier[g], 5);
+    const uint32_t* prow = a.knn[parity ^ 1] + (size_t)g * K;
+    bool same = true;
+    for (int k = 0; k < K; k += 4) {
+      uint4 x = *reinterpret_cast<const uint4*>(row + k);
+      uint4 y = *reinterpret_cast<const uint4*>(prow + k);
+      same = same && x.x == y.x && x.y == y.y && x.z == y.z && x.w == y.w;
+    }
+    const bool low = d2 <= (T)sd.thr2_tier[tt];
+    const bool both = same && low;
+    int st = a.streak[g];
+    st = both ? (st < 255 ? st + 1 : st) : 0;
+    const bool cand = st >= sd.need_tier[tt];
+    o.same = same; o.low = low; o.both = both;
+    if (sd.mode == 0) {
+      a.streak[g] = 0;   // mode 0 clears streak and frozen every iteration (main.cu:837-846)
+    } else {
+      a.streak[g] = (uint8_t)st;
+      if (cand && !a.frozen[g]) { a.frozen[g] = 1; o.newly = 1; }
+    }
+  }
+  return true;
+}
+
+__device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, const SiteOut& o) {
+  // warp-aggregated per-segment counters; every lane of the warp takes part
+  const unsigned full = 0xffffffffu;
+  const int key = o.seg;
+  const unsigned peers = __match_any_sync(full, key);
+  const int leader = __ffs(peers) - 1;
+  const int lane = threadIdx.x & 31;
+  const int same = __popc(__ballot_sync(full, o.same) & peers);
+  const int low = __popc(__ballot_sync(full, o.low) & peers);
+  const int both = __popc(__ballot_sync(full, o.both) & peers);
+  const int newly = __popc(__ballot_sync(full, o.newly) & peers);
+  const unsigned dbits = __reduce_max_sync(peers, __float_as_uint(o.seg >= 0 ? o.disp2 : 0.f));
+  if (lane == leader && key >= 0) {
+    int* sl = stats + ((size_t)key * kStatsRing + (segs[key].iter % kStatsRing)) * kStatsWords;
+    if (same) atomicAdd(sl + 0, same);
+    if (low) atomicAdd(sl + 1, low);
+    if (both) atomicAdd(sl + 2, both);
+    if (newly) atomicAdd(sl + 3, newly);
+    atomicMax(reinterpret_cast<unsigned*>(sl + 4), dbits);
+  }
+}
+
+template <int PROF, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK) k_site_cell(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  using PP = typename PT<PROF>::PP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V2<PP>* sm = reinterpret_cast<V2<PP>*>(smem_raw);
+  PolyRef<PP> A{sm + threadIdx.x, BLOCK}, B{sm + CAP * BLOCK + threadIdx.x, BLOCK};
+  const int t = blockIdx.x * BLOCK + threadIdx.x;
+  const int n_grid = __ldg(a.cell_start + a.total_cells);
+  SiteOut o{-1, 0, 0, 0, 0, 0.f};
+  if (t < n_grid) {
+    const int g = (int)a.sorted[t].id;
+    if (!site_step<PROF>(a, parity, g, A, B, CAP, o)) {
+      o = SiteOut{-1, 0, 0, 0, 0, 0.f};
+      int k = atomicAdd(a.ovf, 1);
+      a.ovf[1 + k] = g;
+    }
+  }
+  stats_flush(a.stats, a.segs, o);
+}
+
+template <int PROF>
+__global__ void __launch_bounds__(64) k_site_cell_fallback(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  using PP = typename PT<PROF>::PP;
+  V2<PP> buf[2][kFallbackCap];
+  const int n = *(volatile int*)a.ovf;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int g = a.ovf[1 + k];
+    SiteOut o{-1, 0, 0, 0, 0, 0.f};
+    site_step<PROF>(a, parity, g, PolyRef<PP>{buf[0], 1}, PolyRef<PP>{buf[1], 1}, kFallbackCap, o);
+    int* sl = a.stats + ((size_t)o.seg * kStatsRing + (a.segs[o.seg].iter % kStatsRing)) * kStatsWords;
+    if (o.same) atomicAdd(sl + 0, 1);
+    if (o.low) atomicAdd(sl + 1, 1);
+    if (o.both) atomicAdd(sl + 2, 1);
+    if (o.newly) atomicAdd(sl + 3, 1);
+    atomicMax(reinterpret_cast<unsigned*>(sl + 4), __float_as_uint(o.disp2));
+  }
+}
+
+// iteration bookkeeping: advance active segments, clear their next stats
+// slot, reset the overflow list
+__global__ void k_seg_advance(SegDev* segs, const int* active, int nseg, int* stats, int* ovf) {
+  for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
+    if (!active[s]) continue;
+    int it = segs[s].iter;
+    int* cur = stats + ((size_t)s * kStatsRing + (it % kStatsRing)) * kStatsWords;
+    cur[5] = it;
+    int nx = it + 1;
+    int* sl = stats + ((size_t)s * kStatsRing + (nx % kStatsRing)) * kStatsWords;
+    for (int w = 0; w < kStatsWords; ++w) sl[w] = 0;
+    segs[s].iter = nx;
+  }
+  if (threadIdx.x == 0) ovf[0] = 0;
+}
+
+}  // namespace cvt

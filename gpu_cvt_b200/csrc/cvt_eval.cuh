@@ -1,0 +1,242 @@
+// Evaluation: BVH over the reference surface and the one-sided Hausdorff
+// distance of a candidate mesh (evaluate.cuh:15-383), plus the dual-triangle
+// extraction that produces the candidate mesh from the sites
+// (near_project.cuh:201-352, buildmesh.cuh:11-241, main.cu:928-974).
+#pragma once
+#include <algorithm>
+#include <vector>
+#include "cvt_engine.cuh"
+
+namespace cvt {
+
+// 40-byte node, layout of evaluate.cuh:15-22
+struct BVHNode {
+  float bmin[3], bmax[3];
+  int left, right, triStart, triCount;
+};
+
+// Host build with the reference's rule: bounds from the triangle boxes,
+// leaf <= leaf_size triangles, otherwise split the centroid-sorted list
+// (stable sort along the longest centroid-extent axis) at its middle;
+// nodes numbered in pre-order (evaluate.cuh:114-201).
+struct BvhBuilder {
+  const std::vector<float>& info;  // per triangle: bmin(3) bmax(3) ctr(3)
+  std::vector<BVHNode>& nodes;
+  std::vector<int>& tri;
+  int leaf;
+  int rec(std::vector<int>& tids) {
+    BVHNode nd{};
+    for (int a = 0; a < 3; ++a) { nd.bmin[a] = 1e30f; nd.bmax[a] = -1e30f; }
+    for (int t : tids)
+      for (int a = 0; a < 3; ++a) {
+        nd.bmin[a] = std::min(nd.bmin[a], info[9 * t + a]);
+        nd.bmax[a] = std::max(nd.bmax[a], info[9 * t + 3 + a]);
+      }
+    nd.left = nd.right = -1;
+    nd.triStart = -1;
+    nd.triCount = 0;
+    int me = (int)nodes.size();
+    nodes.push_back(nd);
+    if ((int)tids.size() <= leaf) {
+      nodes[me].triStart = (int)tri.size();
+      nodes[me].triCount = (int)tids.size();
+      tri.insert(tri.end(), tids.begin(), tids.end());
+      return me;
+    }
+    float cmin[3] = {1e30f, 1e30f, 1e30f}, cmax[3] = {-1e30f, -1e30f, -1e30f};
+    for (int t : tids)
+      for (int a = 0; a < 3; ++a) {
+        cmin[a] = std::min(cmin[a], info[9 * t + 6 + a]);
+        cmax[a] = std::max(cmax[a], info[9 * t + 6 + a]);
+      }
+    float ex = cmax[0] - cmin[0], ey = cmax[1] - cmin[1], ez = cmax[2] - cmin[2];
+    int axis = (ex >= ey && ex >= ez) ? 0 : (ey >= ez ? 1 : 2);
+    std::stable_sort(tids.begin(), tids.end(),
+                     [&](int a, int b) { return info[9 * a + 6 + axis] < info[9 * b + 6 + axis]; });
+    size_t mid = tids.size() / 2;
+    std::vector<int> L(tids.begin(), tids.begin() + mid), R(tids.begin() + mid, tids.end());
+    std::vector<int>().swap(tids);
+    int l = rec(L);
+    int r = rec(R);
+    nodes[me].left = l;
+    nodes[me].right = r;
+    return me;
+  }
+};
+
+inline void build_bvh_host(const float* V, const int* F, int nF, int leaf, std::vector<BVHNode>& nodes,
+                           std::vector<int>& tri) {
+  std::vector<float> info((size_t)9 * nF);
+  const float third = 1.0f / 3.0f;
+  for (int i = 0; i < nF; ++i) {
+    const float* a = V + 3 * F[3 * i];
+    const float* b = V + 3 * F[3 * i + 1];
+    const float* c = V + 3 * F[3 * i + 2];
+    float* o = &info[(size_t)9 * i];
+    for (int k = 0; k < 3; ++k) {
+      o[k] = std::min(a[k], std::min(b[k], c[k]));
+      o[3 + k] = std::max(a[k], std::max(b[k], c[k]));
+      o[6 + k] = (a[k] + (b[k] + c[k])) * third;
+    }
+  }
+  nodes.clear();
+  tri.clear();
+  nodes.reserve(2 * (size_t)nF / 4 + 16);
+  tri.reserve(nF);
+  if (nF == 0) return;
+  std::vector<int> tids(nF);
+  for (int i = 0; i < nF; ++i) tids[i] = i;
+  BvhBuilder b{info, nodes, tri, leaf};
+  b.rec(tids);
+}
+
+// Per-probe closest squared distance to the BVH surface.  Near-first
+// traversal: of two children the nearer box is visited first, which only
+// changes the order, not the minimum.  The stack holds at most one pending
+// sibling per level (depth <= 2*log2(nF) for the median split).
+constexpr int kBvhStack = 96;
+
+__device__ __forceinline__ float bvh_closest_d2(V3<float> p, const BVHNode* __restrict__ nodes,
+                                                const int* __restrict__ tri, const float* __restrict__ V,
+                                                const int* __restrict__ F, int* overflow) {
+  float best = 1e30f;
+  int stack[kBvhStack];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp) {
+    const BVHNode nd = nodes[stack[--sp]];
+    if (aabb_d2(p, nd.bmin, nd.bmax) >= best) continue;
+    if (nd.triCount > 0) {
+      for (int k = 0; k < nd.triCount; ++k) {
+        int t = __ldg(tri + nd.triStart + k);
+        V3<float> a = ld3(V, __ldg(F + 3 * t)), b = ld3(V, __ldg(F + 3 * t + 1)), c = ld3(V, __ldg(F + 3 * t + 2));
+        float d2 = point_tri_d2(p, a, b, c);
+        if (d2 < best) best = d2;
+      }
+    } else {
+      const BVHNode L = nodes[nd.left], R = nodes[nd.right];
+      float dl = aabb_d2(p, L.bmin, L.bmax), dr = aabb_d2(p, R.bmin, R.bmax);
+      if (sp + 2 > kBvhStack) { atomicAdd(overflow, 1); continue; }
+      if (dl < dr) {
+        if (dr < best) stack[sp++] = nd.right;
+        if (dl < best) stack[sp++] = nd.left;
+      } else {
+        if (dl < best) stack[sp++] = nd.left;
+        if (dr < best) stack[sp++] = nd.right;
+      }
+    }
+  }
+  return best;
+}
+
+// probe k of the candidate mesh: vertices, then per face the centroid and
+// the three edge midpoints (evaluate.cuh:253-283)
+__device__ __forceinline__ V3<float> probe_point(const float* __restrict__ V, int nV, const int* __restrict__ F, long k) {
+  if (k < nV) return ld3(V, k);
+  long f = (k - nV) >> 2;
+  int w = (int)((k - nV) & 3);
+  V3<float> a = ld3(V, F[3 * f]), b = ld3(V, F[3 * f + 1]), c = ld3(V, F[3 * f + 2]);
+  const float third = 1.0f / 3.0f;
+  if (w == 0) return {(a.x + (b.x + c.x)) * third, (a.y + (b.y + c.y)) * third, (a.z + (b.z + c.z)) * third};
+  if (w == 1) return {(a.x + b.x) * 0.5f, (a.y + b.y) * 0.5f, (a.z + b.z) * 0.5f};
+  if (w == 2) return {(b.x + c.x) * 0.5f, (b.y + c.y) * 0.5f, (b.z + c.z) * 0.5f};
+  return {(c.x + a.x) * 0.5f, (c.y + a.y) * 0.5f, (c.z + a.z) * 0.5f};
+}
+
+// max over probes of the closest squared distance, reduced in-kernel:
+// warp max, then one atomicMax on the float bits (non-negative floats
+// order as unsigned ints) -- replaces the CUB max of evaluate.cuh:335-343.
+__global__ void __launch_bounds__(128) k_hausdorff(const float* __restrict__ Vc, int nVc, const int* __restrict__ Fc,
+                                                   long nP, const BVHNode* __restrict__ nodes, const int* __restrict__ tri,
+                                                   const float* __restrict__ Vr, const int* __restrict__ Fr,
+                                                   unsigned* out_bits, int* overflow) {
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  float d = 0.f;
+  if (k < nP) d = bvh_closest_d2(probe_point(Vc, nVc, Fc, k), nodes, tri, Vr, Fr, overflow);
+  unsigned b = __float_as_uint(d);
+  b = __reduce_max_sync(0xffffffffu, b);
+  if ((threadIdx.x & 31) == 0) atomicMax(out_bits, b);
+}
+
+// ---------------------------------------------------------------------------
+// dual-triangle extraction
+// ---------------------------------------------------------------------------
+constexpr int kFaceMaxPoly = 256;   // MAX_POLY (main.cu:393)
+
+// Labelled clip (near_project.cuh:201-244) + active-bisector pairs
+// (near_project.cuh:318-351) + key emission (buildmesh.cuh:170-201) per site.
+// Buffers: per thread 2 x kFaceMaxPoly float2 + labels in local memory.
+__global__ void __launch_bounds__(64) k_face_keys(const float* __restrict__ S, const float* __restrict__ U,
+                                                  const float* __restrict__ Vv, const uint32_t* __restrict__ knn,
+                                                  int n, int K, float R2, float eps_clip, float tol_active,
+                                                  unsigned long long* keys, int* key_count, int max_keys) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float2 bufA[kFaceMaxPoly], bufB[kFaceMaxPoly];
+  int labA[kFaceMaxPoly], labB[kFaceMaxPoly];
+  float2* cp = bufA; float2* np = bufB;
+  int* cl = labA; int* nl = labB;
+  int na = 4;
+  cp[0] = make_float2(-R2, -R2); cp[1] = make_float2(R2, -R2); cp[2] = make_float2(R2, R2); cp[3] = make_float2(-R2, R2);
+  cl[0] = cl[1] = cl[2] = cl[3] = -1;
+  const V3<float> si = ld3(S, i), ui = ld3(U, i), vi = ld3(Vv, i);
+  const uint32_t* nb = knn + (size_t)i * K;
+  for (int t = 0; t < K; ++t) {
+    int j = (int)nb[t];
+    if ((unsigned)j >= (unsigned)n || j == i) continue;
+    V3<float> d = sub3(ld3(S, j), si);
+    float a = dot3(d, ui), b = dot3(d, vi), c = 0.5f * dot3(d, d);
+    int m = 0;
+    if (na > 0) {
+      float2 s = cp[na - 1];
+      float fs = fmaT(a, s.x, fmaT(b, s.y, -c));
+      for (int k = 0; k < na; ++k) {
+        float2 e = cp[k];
+        int le = cl[k];
+        float fe = fmaT(a, e.x, fmaT(b, e.y, -c));
+        bool ins_e = fe <= eps_clip, ins_s = fs <= eps_clip;
+        if (ins_e) {
+          if (!ins_s && m < kFaceMaxPoly) {
+            float tt = divT(fs, (fs - fe) + 1e-30f);
+            np[m] = make_float2(fmaT(tt, e.x - s.x, s.x), fmaT(tt, e.y - s.y, s.y)); nl[m] = j; m++;
+          }
+          if (m < kFaceMaxPoly) { np[m] = e; nl[m] = le; m++; }
+        } else if (ins_s && m < kFaceMaxPoly) {
+          float tt = divT(fs, (fs - fe) + 1e-30f);
+          np[m] = make_float2(fmaT(tt, e.x - s.x, s.x), fmaT(tt, e.y - s.y, s.y)); nl[m] = j; m++;
+        }
+        s = e; fs = fe;
+      }
+    }
+    na = m;
+    float2* tp = cp; cp = np; np = tp;
+    int* tl = cl; cl = nl; nl = tl;
+    if (na == 0) break;
+  }
+  if (na < 3) return;
+  for (int k = 0; k < na; ++k) {
+    float2 p = cp[k];
+    float b1 = 1e30f, b2 = 1e30f;
+    int j1 = -1, j2 = -1;
+    for (int t = 0; t < K; ++t) {
+      int j = (int)nb[t];
+      if ((unsigned)j >= (unsigned)n || j == i) continue;
+      V3<float> d = sub3(ld3(S, j), si);
+      float a = dot3(d, ui), b = dot3(d, vi), c = 0.5f * dot3(d, d);
+      float s = fabsf(fmaT(a, p.x, fmaT(b, p.y, -c)));
+      if (s < b1) { b2 = b1; j2 = j1; b1 = s; j1 = j; }
+      else if (s < b2) { b2 = s; j2 = j; }
+    }
+    if (!(j1 >= 0 && j2 >= 0 && j1 != j2 && b1 <= tol_active && b2 <= tol_active)) continue;
+    int x = i, y = j1, z = j2, tmp;
+    if (x > y) { tmp = x; x = y; y = tmp; }
+    if (y > z) { tmp = y; y = z; z = tmp; }
+    if (x > y) { tmp = x; x = y; y = tmp; }
+    int pos = atomicAdd(key_count, 1);
+    if (pos < max_keys)
+      keys[pos] = (unsigned long long)(uint32_t)x | ((unsigned long long)(uint32_t)y << 21) |
+                  ((unsigned long long)(uint32_t)z << 42);
+  }
+}
+
+}  // namespace cvt

@@ -1,0 +1,273 @@
+// Uniform-grid spatial hash and exact K-nearest-neighbour search.
+//
+// Replaces the reference's random-hub index (bitonic-hubs-grid.cuh:1142-1656,
+// rebuilt with ~20 cudaMalloc per call, host shuffles and H x H bound
+// matrices) with a per-segment uniform grid rebuilt by a counting sort every
+// iteration.  The answer is the exact K nearest points in (squared distance,
+// index) order; the search widens ring by ring until the K-th candidate is
+// provably closer than every unvisited cell, so the result does not depend
+// on the cell size (only the time does).
+#pragma once
+#include "cvt_math.cuh"
+
+namespace cvt {
+
+// Grid over one segment's points.  Cells [cell_base, cell_base + ncell) are
+// spatial (x fastest); cell_base + ncell is the bucket of non-finite points,
+// which is never searched.
+struct GridGeom {
+  float lo[3];
+  float h, inv_h;
+  int dim[3];
+  int cell_base;
+  int ncell;
+};
+
+// Cell-ordered copy of a point: coordinates plus the point's global index.
+template <class T> struct alignas(16) Pt4 { T x, y, z; uint32_t id; };
+
+template <class T>
+__device__ __forceinline__ int grid_coord(const GridGeom& g, T v, int a) {
+  float f = floorf(((float)v - g.lo[a]) * g.inv_h);
+  int c = (f >= 0.f) ? (f < (float)g.dim[a] ? (int)f : g.dim[a] - 1) : 0;
+  return c;
+}
+
+template <class T>
+__device__ __forceinline__ int grid_cell(const GridGeom& g, V3<T> p) {
+  if (!finite3(p)) return g.cell_base + g.ncell;
+  int cx = grid_coord(g, p.x, 0), cy = grid_coord(g, p.y, 1), cz = grid_coord(g, p.z, 2);
+  return g.cell_base + (cz * g.dim[1] + cy) * g.dim[0] + cx;
+}
+
+// ---------------------------------------------------------------------------
+// top-K with (distance, index) keys
+// ---------------------------------------------------------------------------
+template <class T> struct KeyOps;
+
+// float: the key is (float bits << 32 | index); non-negative floats order as
+// their bit patterns, so one 64-bit compare orders by distance then index.
+template <> struct KeyOps<float> {
+  using Key = unsigned long long;
+  static __device__ __forceinline__ Key make(float d, uint32_t i) {
+    return ((Key)__float_as_uint(d) << 32) | (Key)i;
+  }
+  static __device__ __forceinline__ Key empty() { return ~0ull; }
+  static __device__ __forceinline__ bool less(Key a, Key b) { return a < b; }
+  static __device__ __forceinline__ Key kmin(Key a, Key b) { return a < b ? a : b; }
+  static __device__ __forceinline__ Key kmax(Key a, Key b) { return a < b ? b : a; }
+  static __device__ __forceinline__ uint32_t idx(Key k) { return (uint32_t)(k & 0xffffffffull); }
+  static __device__ __forceinline__ float dist(Key k) {
+    return k == ~0ull ? __int_as_float(0x7f800000) : __uint_as_float((uint32_t)(k >> 32));
+  }
+  static __device__ __forceinline__ bool is_empty(Key k) { return k == ~0ull; }
+};
+
+struct DKey { double d; uint32_t i; };
+template <> struct KeyOps<double> {
+  using Key = DKey;
+  static __device__ __forceinline__ Key make(double d, uint32_t i) { return {d, i}; }
+  static __device__ __forceinline__ Key empty() { return {__longlong_as_double(0x7ff0000000000000ll), 0xffffffffu}; }
+  static __device__ __forceinline__ bool less(Key a, Key b) { return a.d < b.d || (a.d == b.d && a.i < b.i); }
+  static __device__ __forceinline__ Key kmin(Key a, Key b) { return less(a, b) ? a : b; }
+  static __device__ __forceinline__ Key kmax(Key a, Key b) { return less(a, b) ? b : a; }
+  static __device__ __forceinline__ uint32_t idx(Key k) { return k.i; }
+  static __device__ __forceinline__ double dist(Key k) { return k.d; }
+  static __device__ __forceinline__ bool is_empty(Key k) { return k.i == 0xffffffffu && isinf(k.d); }
+};
+
+// Sorted register list; insertion keeps the KK smallest keys.  Branch-free
+// update new[j] = max(old[j-1], min(old[j], x)) keeps the list in registers.
+template <class T, int KK> struct TopK {
+  using O = KeyOps<T>;
+  typename O::Key k[KK];
+  __device__ __forceinline__ TopK() {
+#pragma unroll
+    for (int j = 0; j < KK; ++j) k[j] = O::empty();
+  }
+  __device__ __forceinline__ T worst_d() const { return O::dist(k[KK - 1]); }
+  __device__ __forceinline__ bool full() const { return !O::is_empty(k[KK - 1]); }
+  __device__ __forceinline__ void insert(typename O::Key x) {
+    if (!O::less(x, k[KK - 1])) return;
+#pragma unroll
+    for (int j = KK - 1; j > 0; --j) k[j] = O::kmax(k[j - 1], O::kmin(k[j], x));
+    k[0] = O::kmin(k[0], x);
+  }
+};
+
+// Exact KK-nearest search of q among the points of one grid.  accept(id)
+// filters candidates (used for the vertex-index exclusion quirk).
+template <class T, class PT, int KK, class Accept>
+__device__ __forceinline__ void grid_knn(const GridGeom& g, const int* __restrict__ cell_start,
+                                         const Pt4<PT>* __restrict__ pts, V3<T> q, TopK<T, KK>& top,
+                                         Accept accept) {
+  if (!finite3(q)) return;
+  const int cx = grid_coord(g, q.x, 0), cy = grid_coord(g, q.y, 1), cz = grid_coord(g, q.z, 2);
+  const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
+  const float slack = 1e-3f * g.h;
+  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
+  const int c[3] = {cx, cy, cz};
+  auto scan_range = [&](int b, int e) {
+    for (int k = b; k < e; ++k) {
+      Pt4<PT> p = pts[k];
+      if (!accept(p.id)) continue;
+      T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
+      if (d <= top.worst_d()) top.insert(KeyOps<T>::make(d, p.id));
+    }
+  };
+  for (int r = 1; r <= rmax; ++r) {
+    const int z0 = max(cz - r, 0), z1 = min(cz + r, g.dim[2] - 1);
+    const int y0 = max(cy - r, 0), y1 = min(cy + r, g.dim[1] - 1);
+    const int x0 = max(cx - r, 0), x1 = min(cx + r, g.dim[0] - 1);
+    for (int z = z0; z <= z1; ++z) {
+      for (int y = y0; y <= y1; ++y) {
+        const int row = g.cell_base + (z * g.dim[1] + y) * g.dim[0];
+        const bool full_row = (r == 1) || abs(z - cz) == r || abs(y - cy) == r;
+        if (full_row) {
+          scan_range(__ldg(cell_start + row + x0), __ldg(cell_start + row + x1 + 1));
+        } else {
+          if (cx - r >= 0) scan_range(__ldg(cell_start + row + cx - r), __ldg(cell_start + row + cx - r + 1));
+          if (cx + r < g.dim[0]) scan_range(__ldg(cell_start + row + cx + r), __ldg(cell_start + row + cx + r + 1));
+        }
+      }
+    }
+    // lower bound on the distance to any point outside the visited block
+    float m = __int_as_float(0x7f800000);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (c[a] - r > 0) m = fminf(m, qf[a] - (g.lo[a] + (float)(c[a] - r) * g.h));
+      if (c[a] + r < g.dim[a] - 1) m = fminf(m, (g.lo[a] + (float)(c[a] + r + 1) * g.h) - qf[a]);
+    }
+    if (isinf(m)) break;
+    m -= slack;
+    if (top.full() && m > 0.f && (double)top.worst_d() < (double)m * (double)m) break;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// grid build: count -> exclusive scan -> scatter
+// ---------------------------------------------------------------------------
+struct SegGrid {           // the minimal per-point view the build needs
+  const GridGeom* geom;    // one geometry per segment
+  const int* seg_of;       // segment of each point (nullptr: all segment 0)
+  const int* active;       // per-segment active flag (nullptr: all active)
+};
+
+template <class T>
+__global__ void k_grid_count(int n, const T* __restrict__ P, SegGrid sg, int* __restrict__ cell_count,
+                             int2* __restrict__ cellrank) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  int s = sg.seg_of ? sg.seg_of[g] : 0;
+  if (s < 0 || (sg.active && !sg.active[s])) { cellrank[g] = make_int2(-1, 0); return; }
+  GridGeom G = sg.geom[s];
+  int cell = grid_cell(G, ld3(P, g));
+  int rank = atomicAdd(cell_count + cell, 1);
+  cellrank[g] = make_int2(cell, rank);
+}
+
+template <class T>
+__global__ void k_grid_scatter(int n, const T* __restrict__ P, const int2* __restrict__ cellrank,
+                               const int* __restrict__ cell_start, Pt4<T>* __restrict__ sorted) {
+  int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  int2 cr = cellrank[g];
+  if (cr.x < 0) return;
+  V3<T> p = ld3(P, g);
+  Pt4<T> o;
+  o.x = p.x; o.y = p.y; o.z = p.z; o.id = (uint32_t)g;
+  sorted[cell_start[cr.x] + cr.y] = o;
+}
+
+// Exclusive scan of n ints (n <= 4096 * 4096): block sums, scan of the block
+// sums, then a block-local rescan with the block offset.  out[n] = total.
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* smem_warp, int& total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) smem_warp[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int w = (lane < (blockDim.x >> 5)) ? smem_warp[lane] : 0;
+    int ws = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += y;
+    }
+    smem_warp[lane] = ws - w;
+    if (lane == 31) smem_warp[32] = ws;
+  }
+  __syncthreads();
+  total = smem_warp[32];
+  int r = smem_warp[wid] + x - v;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(int n, const int* __restrict__ in, int* __restrict__ part) {
+  __shared__ int sw[33];
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) s += (base + k < n) ? in[base + k] : 0;
+  int total;
+  block_exclusive_scan(s, sw, total);
+  if (threadIdx.x == 0) part[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_partials(int nb, int* __restrict__ part) {
+  __shared__ int sw[33];
+  int base = threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) { v[k] = (base + k < nb) ? part[base + k] : 0; s += v[k]; }
+  int total;
+  int off = block_exclusive_scan(s, sw, total);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < nb) part[base + k] = off;
+    off += v[k];
+  }
+  if (threadIdx.x == 0) part[nb] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(int n, const int* __restrict__ in, const int* __restrict__ part,
+                                                             int* __restrict__ out) {
+  __shared__ int sw[33];
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int v[kScanItems];
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) { v[k] = (base + k < n) ? in[base + k] : 0; s += v[k]; }
+  int total;
+  int off = block_exclusive_scan(s, sw, total) + part[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < n) out[base + k] = off;
+    off += v[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) out[n] = part[gridDim.x];
+}
+
+inline int scan_blocks(int n) { return (n + kScanTile - 1) / kScanTile; }
+
+// part must hold scan_blocks(n) + 1 ints
+inline void launch_exclusive_scan(int n, const int* in, int* part, int* out, cudaStream_t st) {
+  int nb = scan_blocks(n);
+  if (nb < 1) nb = 1;
+  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(n, in, part);
+  k_scan_partials<<<1, kScanThreads, 0, st>>>(nb, part);
+  k_scan_apply<<<nb, kScanThreads, 0, st>>>(n, in, part, out);
+}
+
+}  // namespace cvt

@@ -1,0 +1,243 @@
+// Device geometry for the tangent-plane CVT Lloyd step.
+//
+// Rounding is pinned: the library is compiled with -fmad=false, so a*b+c is
+// two rounded operations unless an explicit fmaT() is written, and every
+// division / square root is the IEEE-rounded intrinsic.  The operation order
+// of each routine follows the reference kernels it replaces (cited below);
+// the reference's rsqrtf() becomes 1/sqrt (IEEE), a <=1-ulp difference.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace cvt {
+
+enum Profile { PROF_REF = 0, PROF_MIXED = 1, PROF_FP64 = 2 };
+
+template <class T> struct V3 { T x, y, z; };
+template <class T> struct V2 { T x, y; };
+
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float divT(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double divT(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ float sqrtT(float a) { return __fsqrt_rn(a); }
+__device__ __forceinline__ double sqrtT(double a) { return __dsqrt_rn(a); }
+__device__ __forceinline__ float absT(float a) { return fabsf(a); }
+__device__ __forceinline__ double absT(double a) { return fabs(a); }
+template <class T> __device__ __forceinline__ bool finiteT(T a) { return isfinite(a); }
+
+template <class T> __device__ __forceinline__ V3<T> sub3(V3<T> a, V3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class T> __device__ __forceinline__ T dot3(V3<T> a, V3<T> b) {
+  return fmaT(a.z, b.z, fmaT(a.y, b.y, a.x * b.x));
+}
+template <class T> __device__ __forceinline__ V3<T> cross3(V3<T> a, V3<T> b) {
+  return {fmaT(a.y, b.z, -(a.z * b.y)), fmaT(a.z, b.x, -(a.x * b.z)), fmaT(a.x, b.y, -(a.y * b.x))};
+}
+template <class T> __device__ __forceinline__ T dist2(V3<T> p, V3<T> q) {
+  T dx = p.x - q.x, dy = p.y - q.y, dz = p.z - q.z;
+  return fmaT(dz, dz, fmaT(dy, dy, dx * dx));
+}
+template <class T, class S> __device__ __forceinline__ V3<T> cvt3(V3<S> a) { return {(T)a.x, (T)a.y, (T)a.z}; }
+template <class T> __device__ __forceinline__ V3<T> ld3(const T* __restrict__ p, long i) {
+  return {p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+}
+template <class T> __device__ __forceinline__ void st3(T* __restrict__ p, long i, V3<T> v) {
+  p[3 * i] = v.x; p[3 * i + 1] = v.y; p[3 * i + 2] = v.z;
+}
+template <class T> __device__ __forceinline__ bool finite3(V3<T> a) {
+  return finiteT(a.x) && finiteT(a.y) && finiteT(a.z);
+}
+
+// --------------------------------------------------------------------------
+// tangent frame from a vertex normal (site_normals.cuh:69-110)
+// --------------------------------------------------------------------------
+template <class T> struct Frame { V3<T> u, v; };
+
+template <class T> __device__ __forceinline__ Frame<T> frame_from_normal(V3<T> n) {
+  const T tiny = (T)1e-30;
+  T inv = divT((T)1, sqrtT(dot3(n, n) + tiny));
+  n = {n.x * inv, n.y * inv, n.z * inv};
+  V3<T> h = (absT(n.z) > (T)0.9) ? V3<T>{1, 0, 0} : V3<T>{0, 0, 1};
+  V3<T> u = cross3(h, n);
+  T iu = divT((T)1, sqrtT(dot3(u, u) + tiny));
+  u = {u.x * iu, u.y * iu, u.z * iu};
+  V3<T> v = cross3(n, u);
+  T iv = divT((T)1, sqrtT(dot3(v, v) + tiny));
+  v = {v.x * iv, v.y * iv, v.z * iv};
+  return {u, v};
+}
+
+// --------------------------------------------------------------------------
+// centroid of the clipped polygon (2dClip.cuh:55-80); Neumaier compensation
+// in the MIXED profile.
+// --------------------------------------------------------------------------
+template <class T> struct CSum {
+  T s, c;
+  __device__ __forceinline__ CSum() : s(0), c(0) {}
+  __device__ __forceinline__ void add(T x) {
+    T t = s + x;
+    if (absT(s) >= absT(x)) c += (s - t) + x; else c += (x - t) + s;
+    s = t;
+  }
+  __device__ __forceinline__ T get() const { return s + c; }
+};
+
+// Polygon accessor: vertex k of the polygon currently held in a buffer.
+template <class P, class Buf>
+__device__ __forceinline__ V2<P> poly_centroid(const Buf& poly, int n, bool compensated) {
+  const P nanv = (P)NAN;
+  if (n < 3) return {nanv, nanv};
+  P A2, Cx, Cy;
+  if (!compensated) {
+    A2 = 0; Cx = 0; Cy = 0;
+    V2<P> p = poly.get(0);
+    for (int i = 0; i < n; ++i) {
+      V2<P> q = poly.get(i + 1 == n ? 0 : i + 1);
+      P cr = fmaT(p.x, q.y, -(q.x * p.y));
+      A2 = A2 + cr;
+      Cx = fmaT(p.x + q.x, cr, Cx);
+      Cy = fmaT(p.y + q.y, cr, Cy);
+      p = q;
+    }
+  } else {
+    CSum<P> a, x, y;
+    V2<P> p = poly.get(0);
+    for (int i = 0; i < n; ++i) {
+      V2<P> q = poly.get(i + 1 == n ? 0 : i + 1);
+      P cr = fmaT(p.x, q.y, -(q.x * p.y));
+      a.add(cr);
+      x.add((p.x + q.x) * cr);
+      y.add((p.y + q.y) * cr);
+      p = q;
+    }
+    A2 = a.get(); Cx = x.get(); Cy = y.get();
+  }
+  P A = (P)0.5 * A2;
+  if (absT(A) < (P)1e-18) {
+    P mx = 0, my = 0;
+    for (int i = 0; i < n; ++i) { V2<P> q = poly.get(i); mx = mx + q.x; my = my + q.y; }
+    return {divT(mx, (P)n), divT(my, (P)n)};
+  }
+  P inv6A = divT((P)1, (P)6 * A);
+  return {Cx * inv6A, Cy * inv6A};
+}
+
+// --------------------------------------------------------------------------
+// closest point on a triangle (near_project.cuh:12-53)
+// --------------------------------------------------------------------------
+template <class T> __device__ __forceinline__ V3<T> closest_point_tri(V3<T> P, V3<T> A, V3<T> B, V3<T> C) {
+  const T e = (T)1e-30;
+  V3<T> AB = sub3(B, A), AC = sub3(C, A), AP = sub3(P, A);
+  T d1 = dot3(AB, AP), d2 = dot3(AC, AP);
+  if (d1 <= 0 && d2 <= 0) return A;
+  V3<T> BP = sub3(P, B);
+  T d3 = dot3(AB, BP), d4 = dot3(AC, BP);
+  if (d3 >= 0 && d4 <= d3) return B;
+  T vc = fmaT(d1, d4, -(d3 * d2));
+  if (vc <= 0 && d1 >= 0 && d3 <= 0) {
+    T v = divT(d1, (d1 - d3) + e);
+    return {fmaT(AB.x, v, A.x), fmaT(AB.y, v, A.y), fmaT(AB.z, v, A.z)};
+  }
+  V3<T> CP = sub3(P, C);
+  T d5 = dot3(AB, CP), d6 = dot3(AC, CP);
+  if (d6 >= 0 && d5 <= d6) return C;
+  T vb = fmaT(d5, d2, -(d1 * d6));
+  if (vb <= 0 && d2 >= 0 && d6 <= 0) {
+    T w = divT(d2, (d2 - d6) + e);
+    return {fmaT(AC.x, w, A.x), fmaT(AC.y, w, A.y), fmaT(AC.z, w, A.z)};
+  }
+  T va = fmaT(d3, d6, -(d5 * d4));
+  if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+    T w = divT(d4 - d3, ((d4 - d3) + (d5 - d6)) + e);
+    V3<T> BC = sub3(C, B);
+    return {fmaT(BC.x, w, B.x), fmaT(BC.y, w, B.y), fmaT(BC.z, w, B.z)};
+  }
+  T denom = divT((T)1, ((va + vb) + vc) + e);
+  T v = vb * denom, w = vc * denom;
+  return {A.x + fmaT(AB.x, v, AC.x * w), A.y + fmaT(AB.y, v, AC.y * w), A.z + fmaT(AB.z, v, AC.z * w)};
+}
+
+// closest point over the one-rings of the kproj nearest vertices
+// (project_centroids_to_mesh, near_project.cuh:149-189).  Q is the
+// arithmetic type (double for the MIXED barycentrics).
+template <class T, class Q>
+__device__ __forceinline__ V3<T> project_onering(V3<T> c, const float* __restrict__ V, int nV,
+                                                 const int* __restrict__ F, int nF,
+                                                 const int* __restrict__ off, const int* __restrict__ fcs,
+                                                 const int* knnv, int kproj) {
+  V3<Q> cq = cvt3<Q>(c), bp = cq;
+  Q best = (Q)1e30;
+  for (int t = 0; t < kproj; ++t) {
+    int v = knnv[t];
+    if ((unsigned)v >= (unsigned)nV) continue;
+    int beg = __ldg(off + v), end = __ldg(off + v + 1);
+    for (int ii = beg; ii < end; ++ii) {
+      int fi = __ldg(fcs + ii);
+      if ((unsigned)fi >= (unsigned)nF) continue;
+      int ia = __ldg(F + 3 * fi), ib = __ldg(F + 3 * fi + 1), ic = __ldg(F + 3 * fi + 2);
+      V3<Q> A = {(Q)__ldg(V + 3 * ia), (Q)__ldg(V + 3 * ia + 1), (Q)__ldg(V + 3 * ia + 2)};
+      V3<Q> B = {(Q)__ldg(V + 3 * ib), (Q)__ldg(V + 3 * ib + 1), (Q)__ldg(V + 3 * ib + 2)};
+      V3<Q> C = {(Q)__ldg(V + 3 * ic), (Q)__ldg(V + 3 * ic + 1), (Q)__ldg(V + 3 * ic + 2)};
+      V3<Q> p = closest_point_tri(cq, A, B, C);
+      V3<Q> dd = sub3(p, cq);
+      Q d2 = dot3(dd, dd);
+      if (d2 < best) { best = d2; bp = p; }
+    }
+  }
+  return cvt3<T>(bp);
+}
+
+// --------------------------------------------------------------------------
+// evaluation primitives (evaluate.cuh:44-104)
+// --------------------------------------------------------------------------
+__device__ __forceinline__ float aabb_d2(V3<float> p, const float* bmin, const float* bmax) {
+  float d = 0.f;
+  float q[3] = {p.x, p.y, p.z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (q[a] < bmin[a]) { float t = bmin[a] - q[a]; d = fmaT(t, t, d); }
+    else if (q[a] > bmax[a]) { float t = q[a] - bmax[a]; d = fmaT(t, t, d); }
+  }
+  return d;
+}
+
+__device__ __forceinline__ float point_tri_d2(V3<float> p, V3<float> a, V3<float> b, V3<float> c) {
+  V3<float> ab = sub3(b, a), ac = sub3(c, a), ap = sub3(p, a);
+  float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  if (d1 <= 0.f && d2 <= 0.f) return dot3(ap, ap);
+  V3<float> bp = sub3(p, b);
+  float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+  if (d3 >= 0.f && d4 <= d3) return dot3(bp, bp);
+  float vc = fmaT(d1, d4, -(d3 * d2));
+  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+    float v = divT(d1, d1 - d3);
+    V3<float> pr{fmaT(ab.x, v, a.x), fmaT(ab.y, v, a.y), fmaT(ab.z, v, a.z)};
+    V3<float> d = sub3(p, pr);
+    return dot3(d, d);
+  }
+  V3<float> cp = sub3(p, c);
+  float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+  if (d6 >= 0.f && d5 <= d6) return dot3(cp, cp);
+  float vb = fmaT(d5, d2, -(d1 * d6));
+  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+    float w = divT(d2, d2 - d6);
+    V3<float> pr{fmaT(ac.x, w, a.x), fmaT(ac.y, w, a.y), fmaT(ac.z, w, a.z)};
+    V3<float> d = sub3(p, pr);
+    return dot3(d, d);
+  }
+  float va = fmaT(d3, d6, -(d5 * d4));
+  if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+    float w = divT(d4 - d3, (d4 - d3) + (d5 - d6));
+    V3<float> bc = sub3(c, b);
+    V3<float> pr{fmaT(bc.x, w, b.x), fmaT(bc.y, w, b.y), fmaT(bc.z, w, b.z)};
+    V3<float> d = sub3(p, pr);
+    return dot3(d, d);
+  }
+  float denom = divT(1.f, (va + vb) + vc);
+  float v = vb * denom, w = vc * denom;
+  V3<float> pr{a.x + fmaT(ab.x, v, ac.x * w), a.y + fmaT(ab.y, v, ac.y * w), a.z + fmaT(ab.z, v, ac.z * w)};
+  V3<float> d = sub3(p, pr);
+  return dot3(d, d);
+}
+
+}  // namespace cvt

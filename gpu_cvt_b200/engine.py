@@ -1,0 +1,219 @@
+"""Resident meshes and the multi-segment Lloyd engine (host side, ctypes).
+
+``Mesh``     -- a compacted, preprocessed mesh resident in HBM (vertex
+               normals, vertex->face CSR, vertex grid, BVH); mirrors the
+               set-up of main.cu:421-542.
+``Engine``   -- up to ``max_segments`` (mesh, site set) segments iterated
+               together: each Lloyd iteration of main.cu:669-881 is one pass
+               of fused kernels over every active segment, replayed from a
+               CUDA graph.
+``remesh``   -- one call with host arrays (upload, iterate, download).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import IterStats, MeshInfo, Params, call
+
+PROFILE = {"ref": 0, "mixed": 1, "fp64": 2}
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1, use_graph=True) -> Params:
+    p = Params()
+    _lib.load().cvt_params_default(C.byref(p))
+    p.k = int(k)
+    p.mode = int(mode)
+    p.profile = PROFILE[profile] if isinstance(profile, str) else int(profile)
+    p.kproj = int(kproj)
+    p.ex_quirk = int(bool(ex_quirk))
+    p.cell_factor = float(cell_factor)
+    p.use_graph = int(bool(use_graph))
+    return p
+
+
+class Mesh:
+    """A mesh uploaded and preprocessed once (host float32 V, int32 F in)."""
+
+    def __init__(self, V, F):
+        self.V_host = np.ascontiguousarray(V, dtype=np.float32)
+        self.F_host = np.ascontiguousarray(F, dtype=np.int32)
+        h = C.c_void_p()
+        call("cvt_mesh_create", _ptr(self.V_host), self.V_host.shape[0], _ptr(self.F_host),
+             self.F_host.shape[0], C.byref(h))
+        self.handle = h
+        inf = MeshInfo()
+        call("cvt_mesh_info", h, C.byref(inf))
+        self.nV, self.nF = inf.nV, inf.nF
+        self.R = float(inf.R)
+        self.area = float(inf.area)
+        self.bbox_lo = np.array(inf.bbox_lo[:], np.float32)
+        self.bbox_hi = np.array(inf.bbox_hi[:], np.float32)
+        self.diag = float(inf.diag)
+        self.device_bytes = int(inf.device_bytes)
+
+    def device_arrays(self):
+        """Raw device pointers (V, F, N, vf_off, vf_faces) of the compacted mesh."""
+        ptrs = [C.c_void_p() for _ in range(5)]
+        call("cvt_mesh_device_arrays", self.handle, *[C.byref(p) for p in ptrs])
+        return [p.value for p in ptrs]
+
+    def hausdorff_from(self, Vc, Fc, stream=None) -> float:
+        """One-sided Hausdorff distance from the probe set of the candidate
+        mesh (device pointers or torch CUDA tensors) to this mesh."""
+        out = C.c_float()
+        call("cvt_hausdorff_to_mesh", self.handle, _dptr(Vc), int(_rows(Vc)), _dptr(Fc), int(_rows(Fc)),
+             C.byref(out), stream)
+        return float(out.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().cvt_mesh_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _dptr(t):
+    if hasattr(t, "data_ptr"):
+        return C.c_void_p(t.data_ptr())
+    return C.c_void_p(int(t))
+
+
+def _rows(t):
+    return t.shape[0]
+
+
+class Engine:
+    """Capacity-based multi-segment engine."""
+
+    def __init__(self, p: Params, max_segments: int, max_sites: int, max_cells: int):
+        self.p = p
+        self.K = p.k
+        h = C.c_void_p()
+        call("cvt_engine_create", C.byref(p), int(max_segments), int(max_sites), int(max_cells), C.byref(h))
+        self.handle = h
+        self.meshes = {}
+        self.sizes = {}
+
+    def add(self, mesh: Mesh, sites, stream=None) -> int:
+        """Add a segment; ``sites`` is a host (n,3) array or a CUDA tensor."""
+        sid = C.c_int()
+        if hasattr(sites, "data_ptr"):
+            n = int(sites.shape[0])
+            call("cvt_engine_add_segment", self.handle, mesh.handle, C.c_void_p(sites.data_ptr()), n, 1,
+                 C.byref(sid), stream)
+        else:
+            s = np.ascontiguousarray(sites, dtype=np.float32)
+            n = int(s.shape[0])
+            call("cvt_engine_add_segment", self.handle, mesh.handle, _ptr(s), n, 0, C.byref(sid), stream)
+        self.meshes[sid.value] = mesh
+        self.sizes[sid.value] = n
+        return sid.value
+
+    def remove(self, seg: int) -> None:
+        call("cvt_engine_remove_segment", self.handle, int(seg))
+        self.meshes.pop(seg, None)
+        self.sizes.pop(seg, None)
+
+    def run(self, iters: int, stream=None) -> None:
+        call("cvt_engine_run", self.handle, int(iters), stream)
+
+    def sites(self, seg: int) -> np.ndarray:
+        out = np.zeros((self.sizes[seg], 3), np.float32)
+        call("cvt_engine_get_sites", self.handle, int(seg), _ptr(out), 0, None)
+        return out
+
+    def sites_to_device(self, seg: int, out_tensor, stream=None) -> None:
+        call("cvt_engine_get_sites", self.handle, int(seg), C.c_void_p(out_tensor.data_ptr()), 1, stream)
+
+    def sites_f64(self, seg: int) -> np.ndarray:
+        out = np.zeros((self.sizes[seg], 3), np.float64)
+        call("cvt_engine_get_sites_f64", self.handle, int(seg), _ptr(out), None)
+        return out
+
+    def state(self, seg: int):
+        n = self.sizes[seg]
+        knn = np.zeros((n, self.K), np.uint32)
+        knnv = np.zeros((n, 5), np.int32)
+        frozen = np.zeros(n, np.uint8)
+        tier = np.zeros(n, np.uint8)
+        call("cvt_engine_get_state", self.handle, int(seg), _ptr(knn), _ptr(knnv), _ptr(frozen), _ptr(tier), None)
+        return dict(knn=knn, knnv=knnv, frozen=frozen, tier=tier)
+
+    def stats(self, seg: int, it: int) -> dict:
+        s = IterStats()
+        call("cvt_engine_get_stats", self.handle, int(seg), int(it), C.byref(s), None)
+        return dict(same=s.same, low=s.low, both=s.both, newly_frozen=s.newly_frozen, max_motion=s.max_motion,
+                    iter=s.iter)
+
+    def iters(self, seg: int) -> int:
+        v = C.c_int()
+        call("cvt_engine_segment_iters", self.handle, int(seg), C.byref(v))
+        return v.value
+
+    def profile(self, iters: int, stream=None):
+        """Per-kernel-group ms per iteration: grid, knn, cell, tail."""
+        ms = (C.c_float * 4)()
+        call("cvt_engine_profile", self.handle, int(iters), ms, stream)
+        return dict(zip(("grid", "knn", "cell", "tail"), [float(x) for x in ms]))
+
+    def last_launches(self) -> int:
+        v = C.c_longlong()
+        call("cvt_engine_last_launches", self.handle, C.byref(v))
+        return int(v.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.load().cvt_engine_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def grid_cells(mesh: Mesh, n_sites: int, k: int, cell_factor: float = 1.1) -> int:
+    """Cells a segment of ``n_sites`` sites on ``mesh`` reserves (mirrors the
+    library's surface-grid sizing; used to size engine capacity)."""
+    lo = mesh.bbox_lo.astype(np.float64)
+    hi = mesh.bbox_hi.astype(np.float64)
+    ext = hi - lo
+    emax = max(float(ext.max()), 1e-20)
+    dens = max(n_sites, 1) / max(mesh.area, 1e-30)
+    h = cell_factor * np.sqrt((k + 1) / (np.pi * dens))
+    h = max(h, emax / 2048.0)
+    pad = 1e-4 * emax
+    cap = 8 * n_sites + 64
+    for _ in range(200):
+        dims = [max(1, int(np.ceil((e + 2 * pad) / h))) for e in ext]
+        prod = dims[0] * dims[1] * dims[2]
+        if prod <= cap:
+            break
+        h *= 1.05
+    return int(prod) + 1
+
+
+def remesh(V, F, sites, k=24, mode=0, profile="ref", iters=50, ex_quirk=True, cell_factor=1.1, with_counts=False):
+    """One-call remesh through ``cvt_remesh`` (host arrays in and out)."""
+    V = np.ascontiguousarray(V, np.float32)
+    F = np.ascontiguousarray(F, np.int32)
+    S = np.ascontiguousarray(sites, np.float32)
+    out = np.zeros_like(S)
+    counts = np.zeros((max(iters, 1), 4), np.int32)
+    p = params(k=k, mode=mode, profile=profile, ex_quirk=ex_quirk, cell_factor=cell_factor)
+    call("cvt_remesh", _ptr(V), V.shape[0], _ptr(F), F.shape[0], _ptr(S), S.shape[0], C.byref(p), int(iters),
+         _ptr(out), _ptr(counts))
+    return (out, counts[:iters]) if with_counts else out

@@ -1,0 +1,233 @@
+/*
+ * gpu_cvt.h -- C ABI of the B200 tangent-plane CVT remesher (libgpucvt.so).
+ *
+ * Drop-in for the stage functions of Harper-Yan/GPU_CVT (header-only CUDA
+ * kernels driven by main.cu) plus a resident multi-mesh engine.  Plain
+ * pointers and sizes only: positions are float[3] records (the reference's
+ * float3 AoS), faces int[3], neighbour indices uint32 (the reference's idx_t)
+ * unless stated, masks uint8.  `stream` is a cudaStream_t (NULL = legacy
+ * default stream).  Stage functions are asynchronous on `stream`; they take
+ * caller-owned DEVICE pointers and allocate their temporaries stream-ordered
+ * (cudaMallocAsync), freeing them before return in stream order.
+ *
+ * Every function returns cvt_status_t; CVT_OK is 0.  cvt_last_error() gives
+ * the message of the last failure on the calling thread.  (The reference
+ * reports nothing and exits the process on CUDA errors, cuda_util.cuh:3-11.)
+ *
+ * Numerical profiles (cvt_params_t.profile / `profile` arguments):
+ *   0 CVT_PROFILE_REF   FP32, the reference kernels' operation order
+ *   1 CVT_PROFILE_MIXED FP32 state; FP64 clip predicates/intersections and
+ *                       projection barycentrics; compensated centroid sums;
+ *                       a NaN centroid keeps the old site
+ *   2 CVT_PROFILE_FP64  FP64 state and arithmetic (engine only)
+ */
+#ifndef GPU_CVT_H_
+#define GPU_CVT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  CVT_OK = 0,
+  CVT_ERR_INVALID = 1,   /* bad argument (sizes, null pointers, unsupported K) */
+  CVT_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+  CVT_ERR_OOM = 3,       /* device allocation failed */
+  CVT_ERR_UNSUPPORTED = 4,
+  CVT_ERR_CAPACITY = 5   /* request does not fit the configured capacity */
+} cvt_status_t;
+
+enum { CVT_PROFILE_REF = 0, CVT_PROFILE_MIXED = 1, CVT_PROFILE_FP64 = 2 };
+
+const char* cvt_status_string(cvt_status_t s);
+const char* cvt_last_error(void);
+int cvt_version(void);
+/* Number of kernel launches this library has issued in this process. */
+unsigned long long cvt_launch_count(void);
+
+/* ======================================================================
+ * Stage API -- one function per reference stage, caller-owned device memory
+ * ==================================================================== */
+
+/* Replaces run_knn_bitonic_hubs (site_knn.cuh:20-52, C_and_Q
+ * bitonic-hubs-grid.cuh:1142): exact kk nearest points of every point (self
+ * included), ascending squared distance, ties by lower index.  knn: n*kk
+ * uint32, dist: n*kk float (squared distances; may be NULL).  Rows of points
+ * with frozen[i] != 0 are left untouched (frozen may be NULL).  Entries
+ * beyond the number of points are 0xFFFFFFFF / +inf.  kk in 1..64. */
+cvt_status_t cvt_knn_sites(const float* pts, int n, int kk, const uint8_t* frozen,
+                           uint32_t* knn, float* dist, void* stream);
+
+/* Replaces run_knn_bitonic_query_to_mesh (site_knn.cuh:57-77): the kk nearest
+ * of the n_cand candidate points for each of n_query query points. */
+cvt_status_t cvt_knn_query_to_points(const float* cand, int n_cand, const float* query, int n_query,
+                                     int kk, const uint8_t* frozen, uint32_t* knn, float* dist,
+                                     void* stream);
+
+/* Replaces knn_vertices_bruteforce_k<KPROJ,EXCLUDE_SELF> (near_project.cuh:54-92):
+ * int output (n_query*k), -1 when fewer than k vertices; exclude_self != 0
+ * skips vertex index == query index (the reference's mode-0 quirk). */
+cvt_status_t cvt_knn_vertices(const float* V, int nV, const float* Q, int nQ, int k,
+                              int exclude_self, const uint8_t* frozen, int* out, void* stream);
+
+/* Replaces knn_drop_self_kernel<KIN,KOUT> (site_knn.cuh:79-103). */
+cvt_status_t cvt_knn_drop_self(const uint32_t* in, int n, int kin, int kout, uint32_t* out,
+                               void* stream);
+
+/* Replaces restore_prev_knn_for_frozen_kernel (main.cu:301-312) and
+ * restore_prev_knn_vertices_kernel (near_project.cuh:95-104): rows of frozen
+ * entries are copied from prev to cur (k 32-bit words per row). */
+cvt_status_t cvt_restore_frozen_rows(const uint8_t* frozen, const uint32_t* prev, uint32_t* cur,
+                                     int n, int k, void* stream);
+
+/* Replaces zero_normals + accumulate_face_normals_atomic + normalize_normals
+ * (site_normals.cuh:14-41): area-weighted vertex normals, summed per vertex
+ * in face order through the vertex->face CSR (deterministic). */
+cvt_status_t cvt_vertex_normals(const float* V, int nV, const int* F, int nF, const int* vf_off,
+                                const int* vf_faces, float* N, void* stream);
+
+/* Replaces uv_from_nearest_vertex_normal<KPROJ> (site_normals.cuh:69-110):
+ * frame of site i from the normal of vertex knnV[i*kproj]. */
+cvt_status_t cvt_frames(const float* N0, const int* knnV, int kproj, int n, float* U, float* V,
+                        void* stream);
+
+/* Replaces centroids_tangent_voronoi (2dClip.cuh:82-135): clip [-R,R]^2 by the
+ * bisectors of the K listed neighbours (list order), area centroid mapped back
+ * to 3-D.  nverts (may be NULL): final polygon vertex count per site. */
+cvt_status_t cvt_clip_centroids(const float* S, const float* U, const float* V, const uint32_t* knn,
+                                int n, int K, float R, int profile, float* cent, int* nverts,
+                                void* stream);
+
+/* Replaces project_centroids_to_mesh<KPROJ> (near_project.cuh:149-189):
+ * closest point over the one-rings of the kproj listed vertices.  Sold is
+ * read only by the MIXED profile (NaN centroid keeps the old site). */
+cvt_status_t cvt_project(const float* cent, const float* V, const int* F, const int* vf_off,
+                         const int* vf_faces, const int* knnV, int kproj, int nV, int nF, int nQ,
+                         int profile, const float* Sold, float* Snew, void* stream);
+
+/* Replaces freeze_test_kernel_streak (freezetest.cuh:155-212, tier == NULL:
+ * thr2_tier[0] / need_tier[0] for every site) and
+ * freeze_test_kernel_streak_tiered (freezetest.cuh:270-327) followed by
+ * freeze_apply_cand_kernel (freezetest.cuh:451-466).  need_tier[t] = the
+ * number of consecutive passing transitions required (the reference's
+ * streak[t]-1, at least 1).  thr2_tier/need_tier: 6 entries, host memory.
+ * counts (device, 4 ints) accumulates {same, low, both, newly frozen}. */
+cvt_status_t cvt_freeze(const float* S, const float* Snew, const uint32_t* knn, const uint32_t* prev_knn,
+                        int n, int K, int has_prev, const uint8_t* tier, const float* thr2_tier,
+                        const int* need_tier, uint8_t* streak, uint8_t* cand, uint8_t* frozen,
+                        int* counts, void* stream);
+
+/* Replaces count_frozen_kernel (freezetest.cuh:50-54): *out_sum += #frozen. */
+cvt_status_t cvt_count_frozen(const uint8_t* frozen, int n, int* out_sum, void* stream);
+
+/* Replaces the host tier assignment (main.cu:18-150, called at 640-667):
+ * mode 1 = five tiers by normal variation, mode 2 = six tiers with the
+ * covariance split.  site_normal: n*3 floats (unit normals). */
+cvt_status_t cvt_tiers(int mode, int n, int K, const float* site_normal, const uint32_t* knn,
+                       uint8_t* tier, void* stream);
+
+/* Replaces hausdorff_cand_to_ref_gpu (evaluate.cuh:291-383): one-sided
+ * Hausdorff distance from the probe set of (Vc,Fc) (vertices, face
+ * centroids, edge midpoints) to the surface of `ref_mesh`.  Synchronous;
+ * result in *out (host). */
+typedef struct cvt_mesh* cvt_mesh_t;
+cvt_status_t cvt_hausdorff_to_mesh(cvt_mesh_t ref_mesh, const float* Vc, int nVc, const int* Fc, int nFc,
+                                   float* out, void* stream);
+
+/* ======================================================================
+ * Resident meshes (main.cu:421-542: load, compact, normals, VF CSR, BVH)
+ * ==================================================================== */
+typedef struct {
+  int nV, nF;          /* after dropping unreferenced vertices */
+  float R;             /* longest bbox edge of the input vertices */
+  float area;
+  float bbox_lo[3], bbox_hi[3];
+  float diag;          /* bbox diagonal */
+  size_t device_bytes; /* HBM held by the mesh */
+} cvt_mesh_info_t;
+
+/* Host arrays in; the mesh is compacted, uploaded and preprocessed (vertex
+ * normals, vertex->face CSR, vertex grid, BVH) and stays resident. */
+cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, int nF, cvt_mesh_t* out);
+/* Cell edge of the vertex grid of meshes created afterwards, in units of the
+ * radius expected to hold 6 vertices (default 1.5; a tuning knob only). */
+void cvt_set_vertex_cell_factor(float f);
+cvt_status_t cvt_mesh_info(cvt_mesh_t m, cvt_mesh_info_t* info);
+/* Device views of the compacted mesh (valid until cvt_mesh_destroy). */
+cvt_status_t cvt_mesh_device_arrays(cvt_mesh_t m, const float** V, const int** F, const float** N,
+                                    const int** vf_off, const int** vf_faces);
+cvt_status_t cvt_mesh_destroy(cvt_mesh_t m);
+
+/* ======================================================================
+ * Engine: many (mesh, site set) segments iterated together; each Lloyd
+ * iteration is one pass of fused kernels over all active segments, captured
+ * in a CUDA graph.  Follows main.cu:669-881 per segment.
+ * ==================================================================== */
+typedef struct {
+  int k;              /* neighbours per site after dropping self: 8,12,16,20,24,32 */
+  int mode;           /* 0 freezing off, 1 five tiers, 2 six tiers */
+  int profile;        /* CVT_PROFILE_* */
+  int kproj;          /* nearest vertices for the projection (5) */
+  int ex_quirk;       /* mode 0: centroid->vertex KNN skips vertex index == site index */
+  float cell_factor;  /* site-grid cell edge / expected (K+1)-th neighbour radius */
+  int use_graph;      /* capture iterations in a CUDA graph */
+} cvt_params_t;
+
+void cvt_params_default(cvt_params_t* p);
+
+typedef struct cvt_engine* cvt_engine_t;
+
+/* Per-segment statistics of one iteration (freezetest.cuh counts +
+ * motion).  max_motion is the largest site displacement (not squared). */
+typedef struct {
+  int same, low, both, newly_frozen;
+  float max_motion;
+  int iter;
+} cvt_iter_stats_t;
+
+/* Capacity-based engine: up to max_segments segments holding up to
+ * max_sites sites and max_cells grid cells in total. */
+cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segments, int max_sites, int max_cells,
+                               cvt_engine_t* out);
+cvt_status_t cvt_engine_destroy(cvt_engine_t e);
+/* Place a segment: `sites` (n*3 floats, host or device per sites_on_device)
+ * on `mesh`.  Returns the segment id.  The segment starts at iteration 0. */
+cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, const float* sites, int n,
+                                    int sites_on_device, int* seg_id, void* stream);
+/* Free a segment's slot (its sites stop being iterated at once). */
+cvt_status_t cvt_engine_remove_segment(cvt_engine_t e, int seg_id);
+/* Run `iters` Lloyd iterations of every active segment (asynchronous). */
+cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream);
+/* Copy a segment's current sites out (n*3 floats; FP64 engines convert). */
+cvt_status_t cvt_engine_get_sites(cvt_engine_t e, int seg_id, float* out, int out_on_device, void* stream);
+/* FP64 engines: the double-precision sites (n*3 doubles, host). */
+cvt_status_t cvt_engine_get_sites_f64(cvt_engine_t e, int seg_id, double* out, void* stream);
+/* Host copies of per-site state: knn (n*k uint32, local indices), knnv
+ * (n*kproj int), frozen / tier (n uint8).  Any pointer may be NULL.  Sync. */
+cvt_status_t cvt_engine_get_state(cvt_engine_t e, int seg_id, uint32_t* knn, int* knnv, uint8_t* frozen,
+                                  uint8_t* tier, void* stream);
+/* Statistics of the segment's iteration `iter` (must be one of the last
+ * 256 it ran).  Sync. */
+cvt_status_t cvt_engine_get_stats(cvt_engine_t e, int seg_id, int iter, cvt_iter_stats_t* out, void* stream);
+/* Iterations the segment has completed (host-side count). */
+cvt_status_t cvt_engine_segment_iters(cvt_engine_t e, int seg_id, int* iters);
+/* Run `iters` iterations without a graph, timing each kernel group with CUDA
+ * events on `stream`; ms[4] = average ms per iteration of {grid build, site
+ * KNN kernel, per-site cell kernel, fallback + bookkeeping}.  Synchronous. */
+cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms, void* stream);
+/* Kernel launches issued by the last cvt_engine_run (graph nodes included). */
+cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n);
+
+/* One-call remesh with HOST buffers (the main.cu driver without I/O):
+ * upload, `iters` Lloyd iterations, download.  counts (iters*4 ints, may be
+ * NULL) receives {same, low, both, newly frozen} per iteration. */
+cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF, const float* sites_in, int n_sites,
+                        const cvt_params_t* p, int iters, float* sites_out, int* counts);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPU_CVT_H_ */

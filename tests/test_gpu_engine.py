@@ -1,0 +1,153 @@
+"""Whole-run parity of the fused engine with the CPU oracle's Lloyd loop
+(main.cu:669-881), for every mode and profile, plus batching and
+segment admission mid-run ("same result alone and in the mix")."""
+import numpy as np
+import pytest
+
+from gpu_cvt_b200 import meshgen as mg
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def eng():
+    from gpu_cvt_b200 import engine
+    assert torch.cuda.is_available()
+    return engine
+
+
+def run_engine(eng, mesh_np, S0, k, mode, iters, profile="ref", ex_quirk=True):
+    m = eng.Mesh(mesh_np.V, mesh_np.F)
+    cells = eng.grid_cells(m, len(S0), k)
+    e = eng.Engine(eng.params(k=k, mode=mode, profile=profile, ex_quirk=ex_quirk), 1, len(S0), cells)
+    seg = e.add(m, S0)
+    e.run(iters)
+    S = e.sites_f64(seg) if profile == "fp64" else e.sites(seg)
+    st = e.state(seg)
+    counts = np.array([[e.stats(seg, i)[f] for f in ("same", "low", "both", "newly_frozen")] for i in range(iters)])
+    e.close()
+    m.close()
+    return S, st, counts
+
+
+@pytest.fixture(scope="module")
+def c1():
+    m, S, p = mg.workload_mesh("icosphere_2k")
+    return m, S
+
+
+@pytest.fixture(scope="module")
+def small_torus():
+    m = mg.torus(1.0, 0.3, 80, 40, noise_sigma=0.002, seed=1)
+    return m, mg.sample_sites(m.V, m.F, 4000, seed=1)
+
+
+@pytest.mark.parametrize("iters", [1, 2, 5])
+def test_mode0_ref_bitexact_early(eng, oracle, c1, iters):
+    m, S0 = c1
+    S, st, counts = run_engine(eng, m, S0, 20, 0, iters)
+    r = oracle.lloyd_run(m.V, m.F, S0, 20, 0, iters)
+    assert np.array_equal(S, r["S"])
+    assert np.array_equal(st["knn"], r["knn"])
+    assert np.array_equal(st["knnv"], r["knnv"])
+    assert np.array_equal(counts, r["counts"])
+
+
+def test_mode0_ref_icosphere_2k_full_run(eng, oracle, c1):
+    """The 2k-site icosphere workload: K=20, 50 iterations, freezing off."""
+    m, S0 = c1
+    S, st, counts = run_engine(eng, m, S0, 20, 0, 50)
+    r = oracle.lloyd_run(m.V, m.F, S0, 20, 0, 50)
+    diag = mg.bbox_diag(m.V)
+    err = np.abs(S.astype(np.float64) - r["S"]).max() / diag
+    assert err == 0.0, f"max deviation {err:.3e} of the bbox diagonal"
+    assert np.array_equal(counts, r["counts"])
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_freezing_modes_bitexact(eng, oracle, small_torus, mode):
+    m, S0 = small_torus
+    S, st, counts = run_engine(eng, m, S0, 24, mode, 30)
+    r = oracle.lloyd_run(m.V, m.F, S0, 24, mode, 30)
+    assert np.array_equal(st["tier"], r["tier"])
+    assert np.array_equal(counts, r["counts"])
+    assert np.array_equal(st["frozen"], r["frozen"]) and st["frozen"].sum() > 0
+    assert np.array_equal(S, r["S"])
+
+
+def test_mixed_profile_bitexact(eng, oracle, small_torus):
+    m, S0 = small_torus
+    S, st, counts = run_engine(eng, m, S0, 24, 1, 10, profile="mixed")
+    r = oracle.lloyd_run(m.V, m.F, S0, 24, 1, 10, profile=oracle.P_MIXED)
+    assert np.array_equal(S, r["S"]) and np.array_equal(counts, r["counts"])
+
+
+def test_fp64_profile_matches_fp64_oracle(eng, oracle, c1):
+    m, S0 = c1
+    S, st, counts = run_engine(eng, m, S0, 20, 0, 10, profile="fp64")
+    r = oracle.lloyd_run(m.V, m.F, S0, 20, 0, 10, profile=oracle.P_FP64)
+    assert np.array_equal(S, r["S"])
+    assert np.array_equal(counts, r["counts"])
+
+
+def test_batched_segments_equal_alone(eng, c1, small_torus):
+    """Three meshes in one engine give, per mesh, the same bits as alone."""
+    (m1, S1), (m2, S2) = c1, small_torus
+    m3 = mg.superquadric(4.0, 8000, axes=(1.0, 0.7, 0.5), name="sq")
+    S3 = mg.sample_sites(m3.V, m3.F, 1500, seed=7)
+    alone = [run_engine(eng, m, S, 24, 1, 12)[0] for m, S in ((m1, S1), (m2, S2), (m3, S3))]
+    meshes = [eng.Mesh(m.V, m.F) for m in (m1, m2, m3)]
+    sites = (S1, S2, S3)
+    cells = sum(eng.grid_cells(mm, len(S), 24) for mm, S in zip(meshes, sites))
+    e = eng.Engine(eng.params(k=24, mode=1), 4, sum(len(S) for S in sites), cells)
+    segs = [e.add(mm, S) for mm, S in zip(meshes, sites)]
+    e.run(12)
+    for sg, a in zip(segs, alone):
+        assert np.array_equal(e.sites(sg), a)
+    e.close()
+
+
+def test_admission_mid_run_equals_alone(eng, c1, small_torus):
+    """A segment admitted while another is iterating (continuous batching)
+    ends identical to running alone; removal frees its slot for reuse."""
+    (m1, S1), (m2, S2) = c1, small_torus
+    a1 = run_engine(eng, m1, S1, 24, 0, 9)[0]
+    a2 = run_engine(eng, m2, S2, 24, 0, 5)[0]
+    M1, M2 = eng.Mesh(m1.V, m1.F), eng.Mesh(m2.V, m2.F)
+    cells = eng.grid_cells(M1, len(S1), 24) + eng.grid_cells(M2, len(S2), 24)
+    e = eng.Engine(eng.params(k=24, mode=0), 2, len(S1) + len(S2), cells)
+    g1 = e.add(M1, S1)
+    e.run(4)
+    g2 = e.add(M2, S2)
+    e.run(5)
+    assert e.iters(g1) == 9 and e.iters(g2) == 5
+    assert np.array_equal(e.sites(g1), a1)
+    assert np.array_equal(e.sites(g2), a2)
+    e.remove(g1)
+    g3 = e.add(M1, S1)
+    e.run(9)
+    assert np.array_equal(e.sites(g3), a1)
+    e.close()
+
+
+def test_remesh_one_call_equals_engine(eng, c1):
+    m, S0 = c1
+    out, counts = eng.remesh(m.V, m.F, S0, k=20, mode=0, iters=7, with_counts=True)
+    S, _, c2 = run_engine(eng, m, S0, 20, 0, 7)
+    assert np.array_equal(out, S) and np.array_equal(counts, c2)
+
+
+def test_nan_and_tiny_segments(eng, oracle):
+    m = mg.icosphere(3)
+    S0 = mg.sample_sites(m.V, m.F, 30, seed=4)
+    S0[3] = np.nan
+    S, st, counts = run_engine(eng, m, S0, 32, 0, 3)
+    r = oracle.lloyd_run(m.V, m.F, S0, 32, 0, 3)
+    assert np.array_equal(S, r["S"], equal_nan=True)
+    assert np.isnan(S[3]).all() and np.isfinite(np.delete(S, 3, 0)).all()
+    # MIXED keeps the site that has no centroid instead of propagating NaN
+    S2, _, _ = run_engine(eng, m, S0, 32, 0, 3, profile="mixed")
+    r2 = oracle.lloyd_run(m.V, m.F, S0, 32, 0, 3, profile=oracle.P_MIXED)
+    assert np.array_equal(S2, r2["S"], equal_nan=True)

@@ -1,0 +1,238 @@
+"""Stage-by-stage parity of the libgpucvt kernels with the CPU oracle.
+
+Integer outputs (neighbour lists, masks, counts) must be identical; FP32
+outputs too, because kernels and oracle follow the same pinned operation
+order (explicit FMAs, IEEE division and square root).
+"""
+import numpy as np
+import pytest
+
+from gpu_cvt_b200 import meshgen as mg
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def dev(a, dtype=None):
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    if dtype is not None:
+        t = t.to(dtype)
+    return t.cuda()
+
+
+def host(t):
+    torch.cuda.synchronize()
+    return t.cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def st():
+    from gpu_cvt_b200 import stages
+    assert torch.cuda.is_available()
+    return stages
+
+
+@pytest.fixture(scope="module")
+def c1():
+    m, S, p = mg.workload_mesh("icosphere_2k")
+    return m, S
+
+
+@pytest.mark.parametrize("kk", [1, 5, 21, 25, 33])
+def test_knn_sites_bitexact(st, oracle, c1, kk):
+    _, S = c1
+    n = len(S)
+    knn = torch.zeros((n, kk), dtype=torch.int32, device="cuda")
+    dist = torch.zeros((n, kk), dtype=torch.float32, device="cuda")
+    st.run_knn_bitonic_hubs(n, kk, None, dev(S), knn, dist)
+    ok, od = oracle.knn_points(S, kk, method="bf")
+    assert np.array_equal(host(knn).view(np.uint32), ok)
+    assert np.array_equal(host(dist), od)
+
+
+def test_knn_sites_frozen_rows_untouched(st, oracle, c1):
+    _, S = c1
+    n = len(S)
+    frozen = np.zeros(n, np.uint8)
+    frozen[::2] = 1
+    knn = torch.full((n, 21), 7, dtype=torch.int32, device="cuda")
+    st.run_knn_bitonic_hubs(n, 21, dev(frozen), dev(S), knn, None)
+    k = host(knn)
+    assert (k[::2] == 7).all()
+    ok, _ = oracle.knn_points(S, 21, method="bf")
+    assert np.array_equal(k[1::2].view(np.uint32), ok[1::2])
+
+
+def test_knn_small_and_degenerate_inputs(st, oracle):
+    rng = np.random.default_rng(0)
+    for n in (1, 3, 40):
+        P = rng.random((n, 3)).astype(np.float32)
+        knn = torch.zeros((n, 9), dtype=torch.int32, device="cuda")
+        dist = torch.zeros((n, 9), dtype=torch.float32, device="cuda")
+        st.run_knn_bitonic_hubs(n, 9, None, dev(P), knn, dist)
+        ok, od = oracle.knn_points(P, 9, method="bf")
+        assert np.array_equal(host(knn).view(np.uint32), ok) and np.array_equal(host(dist), od)
+    # duplicates and a lattice full of exact ties; a planar set (zero z extent)
+    g = np.stack(np.meshgrid(np.arange(20), np.arange(20), [0.0], indexing="ij"), -1).reshape(-1, 3)
+    P = np.concatenate([g, g[:50]]).astype(np.float32)
+    knn = torch.zeros((len(P), 13), dtype=torch.int32, device="cuda")
+    st.run_knn_bitonic_hubs(len(P), 13, None, dev(P), knn, None)
+    ok, _ = oracle.knn_points(P, 13, method="bf")
+    assert np.array_equal(host(knn).view(np.uint32), ok)
+
+
+@pytest.mark.parametrize("ex", [False, True])
+def test_knn_vertices_bitexact(st, oracle, c1, ex):
+    m, S = c1
+    out = torch.zeros((len(S), 5), dtype=torch.int32, device="cuda")
+    st.knn_vertices_bruteforce_k(dev(m.V), m.nV, dev(S), len(S), None, out, 5, exclude_self=ex)
+    assert np.array_equal(host(out), oracle.knn_vertices(m.V, S, 5, exclude_self=ex))
+
+
+def test_knn_query_to_mesh(st, oracle, c1):
+    m, S = c1
+    knn = torch.zeros((len(S), 5), dtype=torch.int32, device="cuda")
+    st.run_knn_bitonic_query_to_mesh(m.nV, dev(m.V), dev(S), len(S), 5, None, knn, None)
+    assert np.array_equal(host(knn), oracle.knn_vertices(m.V, S, 5))
+
+
+def test_drop_self_and_restore(st, oracle, c1):
+    _, S = c1
+    raw, _ = oracle.knn_points(S, 21, method="bf")
+    raw[5] = raw[5][::-1]                       # self last
+    raw[7, :] = 7                               # only self
+    out = torch.zeros((len(S), 20), dtype=torch.int32, device="cuda")
+    st.knn_drop_self(dev(raw.view(np.int32)), out, len(S), 21, 20)
+    assert np.array_equal(host(out).view(np.uint32), oracle.drop_self(raw, 20))
+    frozen = (np.arange(len(S)) % 3 == 0).astype(np.uint8)
+    prev = torch.full((len(S), 20), -5, dtype=torch.int32, device="cuda")
+    st.restore_prev_knn_for_frozen(dev(frozen), prev, out, len(S), 20)
+    h = host(out)
+    assert (h[::3] == -5).all() and not (h[1::3] == -5).any()
+
+
+def test_normals_and_frames_bitexact(st, oracle, c1):
+    m, S = c1
+    off, fcs = oracle.build_vf(m.nV, m.F)
+    N = torch.zeros((m.nV, 3), dtype=torch.float32, device="cuda")
+    st.vertex_normals(dev(m.V), dev(m.F), dev(off), dev(fcs), N)
+    No = oracle.vertex_normals(m.V, m.F)
+    assert np.array_equal(host(N), No)
+    knnv = oracle.knn_vertices(m.V, S, 5)
+    knnv[3, 0] = -1
+    U = torch.zeros((len(S), 3), dtype=torch.float32, device="cuda")
+    V = torch.zeros_like(U)
+    st.uv_from_nearest_vertex_normal(N, dev(knnv), U, V)
+    Uo, Vo = oracle.frames(No, knnv[:, 0])
+    assert np.array_equal(host(U), Uo) and np.array_equal(host(V), Vo)
+
+
+@pytest.mark.parametrize("profile", [0, 1])
+def test_clip_centroids_bitexact(st, oracle, c1, profile):
+    m, S = c1
+    No = oracle.vertex_normals(m.V, m.F)
+    knnv = oracle.knn_vertices(m.V, S, 5)
+    Uo, Vo = oracle.frames(No, knnv[:, 0])
+    raw, _ = oracle.knn_points(S, 21, method="bf")
+    knn = oracle.drop_self(raw, 20)
+    R = mg.bbox_max_edge(m.V)
+    cent = torch.zeros((len(S), 3), dtype=torch.float32, device="cuda")
+    nv = torch.zeros(len(S), dtype=torch.int32, device="cuda")
+    st.centroids_tangent_voronoi(dev(S), dev(Uo), dev(Vo), dev(knn.view(np.int32)), len(S), 20, R, cent, profile, nv)
+    co, nvo = oracle.clip_centroids(S, Uo, Vo, knn, R, profile=profile, return_nverts=True)
+    assert np.array_equal(host(nv), nvo)
+    assert np.array_equal(host(cent), co)
+
+
+def test_clip_overflow_fallback_exact(st, oracle):
+    # a site with many neighbours on a circle: its cell has >32 vertices, so
+    # the shared-memory path hands it to the 64-vertex fallback
+    k = 40
+    ang = np.linspace(0, 2 * np.pi, k, endpoint=False)
+    P = np.concatenate([[[0, 0, 0]], np.stack([np.cos(ang), np.sin(ang), np.zeros(k)], 1) * 0.1]).astype(np.float32)
+    n = len(P)
+    knn = np.zeros((n, 40), np.uint32)
+    for i in range(n):
+        knn[i] = [j for j in range(n) if j != i][:40]
+    U = np.tile(np.array([1, 0, 0], np.float32), (n, 1))
+    V = np.tile(np.array([0, 1, 0], np.float32), (n, 1))
+    cent = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
+    nv = torch.zeros(n, dtype=torch.int32, device="cuda")
+    st.centroids_tangent_voronoi(dev(P), dev(U), dev(V), dev(knn.view(np.int32)), n, 40, 1.0, cent, 0, nv)
+    co, nvo = oracle.clip_centroids(P, U, V, knn, 1.0, return_nverts=True)
+    assert nvo[0] == 40
+    assert np.array_equal(host(nv), nvo) and np.array_equal(host(cent), co)
+
+
+@pytest.mark.parametrize("profile", [0, 1])
+def test_project_bitexact(st, oracle, c1, profile):
+    m, S = c1
+    rng = np.random.default_rng(1)
+    cent = (S * 1.01 + rng.normal(scale=0.01, size=S.shape)).astype(np.float32)
+    cent[11] = np.nan
+    knnv = oracle.knn_vertices(m.V, cent, 5)
+    off, fcs = oracle.build_vf(m.nV, m.F)
+    out = torch.zeros_like(dev(cent))
+    st.project_centroids_to_mesh(dev(cent), dev(m.V), dev(m.F), dev(off), dev(fcs), dev(knnv), m.nV, m.nF, len(S),
+                                 dev(S), out, 5, profile)
+    exp = oracle.project(cent, m.V, m.F, knnv, profile=profile, Sold=S)
+    assert np.array_equal(host(out), exp, equal_nan=True)
+
+
+@pytest.mark.parametrize("tiered", [False, True])
+def test_freeze_bitexact(st, oracle, c1, tiered):
+    _, S = c1
+    n = len(S)
+    rng = np.random.default_rng(2)
+    Snew = (S + rng.normal(scale=0.01, size=S.shape)).astype(np.float32)
+    raw, _ = oracle.knn_points(S, 21, method="bf")
+    knn = oracle.drop_self(raw, 20)
+    prev = knn.copy()
+    prev[rng.random(n) < 0.2, 3] = 0
+    tier = rng.integers(0, 6, n).astype(np.uint8) if tiered else None
+    thr = [1e-4, 1e-4, 2e-4, 2e-4, 1e-4, 3e-4]
+    need = [4, 9, 14, 19, 24, 9] if tiered else [4] * 6
+    streak = rng.integers(0, 30, n).astype(np.uint8)
+    frozen = (rng.random(n) < 0.1).astype(np.uint8)
+    d_streak, d_frozen = dev(streak), dev(frozen)
+    d_cand = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    counts = torch.zeros(4, dtype=torch.int32, device="cuda")
+    st.freeze_test_streak(dev(S), dev(Snew), dev(knn.view(np.int32)), dev(prev.view(np.int32)), 20, 1, thr, need,
+                          d_streak, d_cand, d_frozen, counts, tier=dev(tier) if tiered else None)
+    s2, f2 = streak.copy(), frozen.copy()
+    cand, cnt = oracle.freeze(S, Snew, knn, prev, True, tier, thr, need, s2, f2)
+    assert np.array_equal(host(d_streak), s2) and np.array_equal(host(d_frozen), f2)
+    assert np.array_equal(host(d_cand), cand) and np.array_equal(host(counts), cnt)
+    total = torch.zeros(1, dtype=torch.int32, device="cuda")
+    st.count_frozen(d_frozen, n, total)
+    assert int(host(total)[0]) == int(f2.sum())
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_tiers_bitexact(st, oracle, c1, mode):
+    m, S = c1
+    No = oracle.vertex_normals(m.V, m.F)
+    nn = oracle.knn_vertices(m.V, S, 1)[:, 0]
+    sn = No[nn]
+    raw, _ = oracle.knn_points(S, 21, method="bf")
+    knn = oracle.drop_self(raw, 20)
+    tier = torch.zeros(len(S), dtype=torch.uint8, device="cuda")
+    st.tier_ids(mode, dev(sn), dev(knn.view(np.int32)), tier)
+    exp, _, _ = oracle.tiers(mode, sn, knn)
+    assert np.array_equal(host(tier), exp)
+
+
+def test_hausdorff(oracle):
+    from gpu_cvt_b200.engine import Mesh
+    ref = mg.icosphere(5)
+    mesh = Mesh(ref.V, ref.F)
+    c = mg.icosphere(3)
+    Vc = (c.V * np.float32(1.01)).astype(np.float32)
+    Vc[::5] *= np.float32(0.985)
+    got = mesh.hausdorff_from(dev(Vc), dev(c.F))
+    exp = oracle.hausdorff_one_sided(Vc, c.F, ref.V, ref.F)
+    # same minima; a near-first traversal may prune a box whose bound ties the
+    # best distance to the last ulp, hence a relative 1e-6 tolerance
+    assert abs(got - exp) <= 1e-6 * exp
+    mesh.close()
