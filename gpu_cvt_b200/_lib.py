@@ -32,6 +32,11 @@ class Params(C.Structure):
                 ("cell_factor", f32), ("use_graph", i32)]
 
 
+class EvalOut(C.Structure):
+    _fields_ = [("dH", f32), ("Qmin", f32), ("Qavg", f32), ("theta_min", f32), ("theta_min_avg", f32),
+                ("theta_lt_30_pct", f32), ("theta_gt_90_pct", f32), ("n_faces", i32), ("diag", f32)]
+
+
 class IterStats(C.Structure):
     _fields_ = [("same", i32), ("low", i32), ("both", i32), ("newly_frozen", i32), ("max_motion", f32),
                 ("iter", i32)]
@@ -74,6 +79,9 @@ _SIGS = {
     "cvt_engine_segment_iters": [vp, i32, vp],
     "cvt_engine_last_launches": [vp, vp],
     "cvt_engine_profile": [vp, i32, vp, vp],
+    "cvt_engine_evaluate": [vp, i32, vp, vp],
+    "cvt_extract_faces": [vp, vp, vp, vp, i32, i32, f32, vp, i32, vp, vp],
+    "cvt_quality": [vp, vp, i32, vp, vp],
     "cvt_remesh": [vp, i32, vp, i32, vp, i32, vp, i32, vp, vp],
 }
 _RESTYPES = {"cvt_status_string": C.c_char_p, "cvt_last_error": C.c_char_p, "cvt_version": i32,

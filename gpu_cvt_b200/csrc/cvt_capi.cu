@@ -9,6 +9,9 @@
 #include <string>
 #include <vector>
 
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_select.cuh>
+
 #include "../../include/gpu_cvt.h"
 #include "cvt_eval.cuh"
 #include "cvt_stage.cuh"
@@ -888,7 +891,7 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   k_site_cell<PROF, BLK, kCellCap><<<cdiv(ns, BLK), BLK, smem, st>>>(a, parity);
   L++;
   if (ev) CK(cudaEventRecord(ev[3], st));
-  k_site_cell_fallback<PROF><<<148, 64, 0, st>>>(a, parity);
+  k_cell_overflow<PROF><<<148, 64, 0, st>>>(a, parity);
   L++;
   k_seg_advance<<<1, 256, 0, st>>>(e->d_segs, e->d_active, e->max_seg, e->d_stats, e->d_ovf);
   L++;
@@ -1102,4 +1105,190 @@ extern "C" cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF,
   cvt_engine_destroy(e);
   cvt_mesh_destroy(m);
   return s;
+}
+
+// ---------------------------------------------------------------------------
+// evaluation: dual triangles, quality, Hausdorff (evaluate stage)
+// ---------------------------------------------------------------------------
+extern "C" cvt_status_t cvt_extract_faces(const float* S, const float* U, const float* V, const uint32_t* knn, int n, int K,
+                                          float R2, int* F_out, int max_faces, int* n_faces, void* stream) {
+  if (n < 0 || K < 1 || !n_faces || (n > 0 && (!S || !U || !V || !knn)) || (max_faces > 0 && !F_out))
+    return fail(CVT_ERR_INVALID, "cvt_extract_faces: bad arguments");
+  *n_faces = 0;
+  if (n == 0) return CVT_OK;
+  cudaStream_t st = S_(stream);
+  Scratch sc(st);
+  int* cnt;
+  CK(sc.get(&cnt, 1));
+  int cap = std::max(16 * n, 1024);
+  unsigned long long* keys = nullptr;
+  int nk = 0;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    Scratch ks(st);
+    CK(ks.get(&keys, (size_t)cap));
+    CK(cudaMemsetAsync(cnt, 0, sizeof(int), st));
+    k_face_keys<<<cdiv(n, 64), 64, 0, st>>>(S, U, V, knn, n, K, R2, 1e-8f, 1e-7f, keys, cnt, cap);
+    CKLAUNCH();
+    CK(cudaMemcpyAsync(&nk, cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (nk <= cap) {
+      // sort + unique on the device (the reference sorts on the host, main.cu:952-954)
+      unsigned long long *sorted, *uniq;
+      int* nu_d;
+      CK(sc.get(&sorted, (size_t)std::max(nk, 1)));
+      CK(sc.get(&uniq, (size_t)std::max(nk, 1)));
+      CK(sc.get(&nu_d, 1));
+      size_t tb = 0, tb2 = 0;
+      CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, keys, sorted, nk, 0, 63, st));
+      CK(cub::DeviceSelect::Unique(nullptr, tb2, sorted, uniq, nu_d, nk, st));
+      void* tmp;
+      CK(sc.get((char**)&tmp, std::max(tb, tb2)));
+      size_t tbs = std::max(tb, tb2);
+      CK(cub::DeviceRadixSort::SortKeys(tmp, tbs, keys, sorted, nk, 0, 63, st));
+      tbs = std::max(tb, tb2);
+      CK(cub::DeviceSelect::Unique(tmp, tbs, sorted, uniq, nu_d, nk, st));
+      LAUNCHED(2);
+      int nu = 0;
+      CK(cudaMemcpyAsync(&nu, nu_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (nu == 0) return CVT_OK;
+      int *tri, *keep, *pos, *part;
+      CK(sc.get(&tri, 3 * (size_t)nu));
+      CK(sc.get(&keep, (size_t)nu));
+      CK(sc.get(&pos, (size_t)nu + 1));
+      CK(sc.get(&part, (size_t)scan_blocks(nu) + 2));
+      k_face_decode<<<cdiv(nu, 256), 256, 0, st>>>(uniq, nu, S, n, 1e-6f, tri, keep);
+      CKLAUNCH();
+      launch_exclusive_scan(nu, keep, part, pos, st);
+      LAUNCHED(3);
+      int nf = 0;
+      CK(cudaMemcpyAsync(&nf, pos + nu, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      *n_faces = nf;
+      if (nf > max_faces) return fail(CVT_ERR_CAPACITY, "cvt_extract_faces: more faces than max_faces (needed count in *n_faces)");
+      k_face_compact<<<cdiv(nu, 256), 256, 0, st>>>(tri, keep, pos, nu, F_out);
+      CKLAUNCH();
+      return CVT_OK;
+    }
+    cap = nk;  // retry with the exact key count
+  }
+  return fail(CVT_ERR_CUDA, "cvt_extract_faces: key count changed between passes");
+}
+
+extern "C" cvt_status_t cvt_quality(const float* V, const int* F, int nF, float* out, void* stream) {
+  if (nF < 0 || !out || (nF > 0 && (!V || !F))) return fail(CVT_ERR_INVALID, "cvt_quality: bad arguments");
+  for (int k = 0; k < 6; ++k) out[k] = 0.f;
+  if (nF == 0) { out[0] = 1e30f; out[2] = 1e30f; return CVT_OK; }
+  cudaStream_t st = S_(stream);
+  Scratch sc(st);
+  double* acc;
+  unsigned* mins;
+  CK(sc.get(&acc, 4));
+  CK(sc.get(&mins, 2));
+  CK(cudaMemsetAsync(acc, 0, 4 * sizeof(double), st));
+  CK(cudaMemsetAsync(mins, 0x7f, 2 * sizeof(unsigned), st));
+  k_quality<<<cdiv(nF, 256), 256, 0, st>>>(V, F, nF, acc, mins);
+  CKLAUNCH();
+  double h[4];
+  unsigned m[2];
+  CK(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(m, mins, sizeof(m), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float qmin, tmin;
+  std::memcpy(&qmin, &m[0], 4);
+  std::memcpy(&tmin, &m[1], 4);
+  out[0] = qmin;
+  out[1] = (float)(h[0] / nF);
+  out[2] = tmin;
+  out[3] = (float)(h[1] / nF);
+  out[4] = (float)(h[2] * 100.0 / (3.0 * nF));
+  out[5] = (float)(h[3] * 100.0 / (3.0 * nF));
+  return CVT_OK;
+}
+
+// frames of the current sites (frozen sites keep their vertex list; the rest
+// take their nearest mesh vertex): main.cu:883-897
+template <class T>
+__global__ void k_eval_frames(const T* __restrict__ S, int base, int n, const uint8_t* __restrict__ frozen,
+                              const int* __restrict__ knnv, int mode, MeshDev md, float* __restrict__ Sf,
+                              float* __restrict__ U, float* __restrict__ Vv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int g = base + i;
+  V3<T> p = ld3(S, g);
+  st3(Sf, i, cvt3<float>(p));
+  int nn;
+  if (mode != 0 && frozen[g]) {
+    nn = knnv[(size_t)g * kKProj];
+  } else {
+    TopK<T, 1> v1;
+    grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, p, v1, [](uint32_t) { return true; });
+    nn = (int)KeyOps<T>::idx(v1.k[0]);
+  }
+  if (nn < 0) { st3(U, i, V3<float>{1, 0, 0}); st3(Vv, i, V3<float>{0, 1, 0}); return; }
+  Frame<float> fr = frame_from_normal(ld3(md.N, nn));
+  st3(U, i, fr.u);
+  st3(Vv, i, fr.v);
+}
+
+extern "C" cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int s, cvt_eval_t* out, void* stream) {
+  if (!e || !out || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_evaluate: bad segment");
+  cudaStream_t st = S_(stream);
+  const SegDev& sd = e->segs[s];
+  const int n = sd.n_sites;
+  const cvt_mesh* m = e->seg_mesh[s];
+  Scratch sc(st);
+  float *Sf, *U, *V;
+  CK(sc.get(&Sf, 3 * (size_t)n));
+  CK(sc.get(&U, 3 * (size_t)n));
+  CK(sc.get(&V, 3 * (size_t)n));
+  if (e->f64)
+    k_eval_frames<double><<<cdiv(n, 128), 128, 0, st>>>((const double*)e->d_S[e->parity], sd.site_base, n, e->d_frozen,
+                                                         e->d_knnv, sd.mode, m->dev(), Sf, U, V);
+  else
+    k_eval_frames<float><<<cdiv(n, 128), 128, 0, st>>>((const float*)e->d_S[e->parity], sd.site_base, n, e->d_frozen,
+                                                        e->d_knnv, sd.mode, m->dev(), Sf, U, V);
+  CKLAUNCH();
+  // R2 = longest bbox edge of the current sites (main.cu:899-909)
+  int* bb;
+  CK(sc.get(&bb, 6));
+  k_bbox_init<<<1, 32, 0, st>>>(bb);
+  CKLAUNCH();
+  k_bbox<<<cdiv(n, 256), 256, 0, st>>>(n, Sf, bb);
+  CKLAUNCH();
+  int hb[6];
+  CK(cudaMemcpyAsync(hb, bb, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  float lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    int o = hb[a] >= 0 ? hb[a] : hb[a] ^ 0x7fffffff;
+    int q = hb[3 + a] >= 0 ? hb[3 + a] : hb[3 + a] ^ 0x7fffffff;
+    std::memcpy(&lo[a], &o, 4);
+    std::memcpy(&hi[a], &q, 4);
+  }
+  float R2 = 2.0f * 0.5f * std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+  const uint32_t* knn = e->d_knn[e->parity ^ 1] + (size_t)e->K * sd.site_base;
+  int max_faces = 4 * n + 64;
+  int* Fc;
+  CK(sc.get(&Fc, 3 * (size_t)max_faces));
+  int nf = 0;
+  cvt_status_t r = cvt_extract_faces(Sf, U, V, knn, n, e->K, R2, Fc, max_faces, &nf, stream);
+  if (r == CVT_ERR_CAPACITY) {
+    max_faces = nf;
+    CK(sc.get(&Fc, 3 * (size_t)max_faces));
+    r = cvt_extract_faces(Sf, U, V, knn, n, e->K, R2, Fc, max_faces, &nf, stream);
+  }
+  if (r != CVT_OK) return r;
+  float q[6];
+  r = cvt_quality(Sf, Fc, nf, q, stream);
+  if (r != CVT_OK) return r;
+  float dH = 0.f;
+  r = cvt_hausdorff_to_mesh(const_cast<cvt_mesh*>(m), Sf, n, Fc, nf, &dH, stream);
+  if (r != CVT_OK) return r;
+  out->dH = dH;
+  out->Qmin = q[0]; out->Qavg = q[1]; out->theta_min = q[2]; out->theta_min_avg = q[3];
+  out->theta_lt_30_pct = q[4]; out->theta_gt_90_pct = q[5];
+  out->n_faces = nf;
+  out->diag = m->diag;
+  return CVT_OK;
 }

@@ -13,7 +13,7 @@
 //                and apply (freezetest.cuh:155-212, 270-327, 451-466),
 //                tier assignment on the segment's first iteration
 //                (main.cu:640-667)
-//   k_site_cell_fallback  the same for the rare cells whose polygon
+//   k_cell_overflow  the same for the rare cells whose polygon
 //                outgrows the shared-memory buffer (exact 64-vertex cap)
 //   k_seg_advance  per-segment iteration counters / statistics slots
 // All sizes come from device memory, so the whole iteration is captured once
@@ -466,7 +466,7 @@ __global__ void __launch_bounds__(BLOCK) k_site_cell(EngineArgs<typename PT<PROF
 }
 
 template <int PROF>
-__global__ void __launch_bounds__(64) k_site_cell_fallback(EngineArgs<typename PT<PROF>::T> a, int parity) {
+__global__ void __launch_bounds__(64) k_cell_overflow(EngineArgs<typename PT<PROF>::T> a, int parity) {
   using PP = typename PT<PROF>::PP;
   V2<PP> buf[2][kFallbackCap];
   const int n = *(volatile int*)a.ovf;

@@ -240,3 +240,83 @@ __global__ void __launch_bounds__(64) k_face_keys(const float* __restrict__ S, c
 }
 
 }  // namespace cvt
+
+namespace cvt {
+
+// decode the sorted unique keys (buildmesh.cuh:99-109) and drop degenerate
+// triangles (buildmesh.cuh:225-241, eps 1e-6); flags[k] = keep
+__global__ void k_face_decode(const unsigned long long* __restrict__ keys, int nk, const float* __restrict__ S, int n,
+                              float eps, int* __restrict__ tri, int* __restrict__ keep) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk) return;
+  unsigned long long key = keys[k];
+  int a = (int)(key & 0x1FFFFFull), b = (int)((key >> 21) & 0x1FFFFFull), c = (int)((key >> 42) & 0x1FFFFFull);
+  bool deg = (a == b || b == c || a == c) || a >= n || b >= n || c >= n;
+  if (!deg) {
+    V3<float> A = ld3(S, a), B = ld3(S, b), C = ld3(S, c);
+    V3<float> e0 = sub3(B, A), e1 = sub3(C, B), e2 = sub3(A, C);
+    float l0 = sqrtT(dot3(e0, e0)), l1 = sqrtT(dot3(e1, e1)), l2 = sqrtT(dot3(e2, e2));
+    V3<float> cr = cross3(sub3(B, A), sub3(C, A));
+    float ar = sqrtT(dot3(cr, cr));
+    deg = !(l0 > eps && l1 > eps && l2 > eps && ar > eps);
+  }
+  tri[3 * k] = a; tri[3 * k + 1] = b; tri[3 * k + 2] = c;
+  keep[k] = deg ? 0 : 1;
+}
+
+__global__ void k_face_compact(const int* __restrict__ tri, const int* __restrict__ keep, const int* __restrict__ pos,
+                               int nk, int* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk || !keep[k]) return;
+  int p = pos[k];
+  out[3 * p] = tri[3 * k]; out[3 * p + 1] = tri[3 * k + 1]; out[3 * p + 2] = tri[3 * k + 2];
+}
+
+// quality metrics (evaluate.cuh:388-462) as a device reduction: acc[0] Qsum,
+// acc[1] min-angle sum, acc[2] #angles < 30, acc[3] #angles > 90 (doubles);
+// mins[0] Qmin bits, mins[1] theta_min bits (non-negative floats as uint)
+__global__ void k_quality(const float* __restrict__ V, const int* __restrict__ F, int nF, double* acc, unsigned* mins) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  double q = 0.0, th = 0.0, lt = 0.0, gt = 0.0;
+  float qmin = 3.0e38f, tmin = 3.0e38f;
+  if (f < nF) {
+    V3<float> a = ld3(V, F[3 * f]), b = ld3(V, F[3 * f + 1]), c = ld3(V, F[3 * f + 2]);
+    V3<float> ab = sub3(b, a), ac = sub3(c, a), ba = sub3(a, b), bc = sub3(c, b), ca = sub3(a, c), cb = sub3(b, c);
+    auto ang = [](V3<float> u, V3<float> v) {
+      float du = sqrtT(dot3(u, u)), dv = sqrtT(dot3(v, v));
+      float den = fmaxf(du * dv, 1e-30f);
+      float cs = divT(dot3(u, v), den);
+      cs = fminf(1.f, fmaxf(-1.f, cs));
+      return acosf(cs) * (180.0f / 3.14159265358979323846f);
+    };
+    float A = ang(ab, ac), B = ang(ba, bc), Cc = ang(ca, cb);
+    tmin = fminf(A, fminf(B, Cc));
+    th = tmin;
+    lt = (A < 30.f) + (B < 30.f) + (Cc < 30.f);
+    gt = (A > 90.f) + (B > 90.f) + (Cc > 90.f);
+    float l0 = sqrtT(dot3(ab, ab)), l1 = sqrtT(dot3(bc, bc)), l2 = sqrtT(dot3(ca, ca));
+    V3<float> cr = cross3(ab, ac);
+    float area = 0.5f * sqrtT(dot3(cr, cr));
+    float s = 0.5f * ((l0 + l1) + l2);
+    float e = fmaxf(l0, fmaxf(l1, l2));
+    float den = fmaxf(s * e, 1e-30f);
+    float qq = divT(6.0f, sqrtT(3.0f)) * divT(area, den);
+    qmin = qq;
+    q = qq;
+  }
+  for (int o = 16; o; o >>= 1) {
+    q += __shfl_xor_sync(0xffffffffu, q, o);
+    th += __shfl_xor_sync(0xffffffffu, th, o);
+    lt += __shfl_xor_sync(0xffffffffu, lt, o);
+    gt += __shfl_xor_sync(0xffffffffu, gt, o);
+    qmin = fminf(qmin, __shfl_xor_sync(0xffffffffu, qmin, o));
+    tmin = fminf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicAdd(acc + 0, q); atomicAdd(acc + 1, th); atomicAdd(acc + 2, lt); atomicAdd(acc + 3, gt);
+    atomicMin(mins + 0, __float_as_uint(qmin));
+    atomicMin(mins + 1, __float_as_uint(tmin));
+  }
+}
+
+}  // namespace cvt

@@ -16,7 +16,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from ._lib import IterStats, MeshInfo, Params, call
+from ._lib import EvalOut, IterStats, MeshInfo, Params, call
 
 PROFILE = {"ref": 0, "mixed": 1, "fp64": 2}
 
@@ -167,6 +167,15 @@ class Engine:
         ms = (C.c_float * 4)()
         call("cvt_engine_profile", self.handle, int(iters), ms, stream)
         return dict(zip(("grid", "knn", "cell", "tail"), [float(x) for x in ms]))
+
+    def evaluate(self, seg: int, stream=None) -> dict:
+        """Dual-triangle mesh of the current sites: quality and one-sided
+        Hausdorff distance to the segment's mesh (dH_rel = dH / bbox diag)."""
+        o = EvalOut()
+        call("cvt_engine_evaluate", self.handle, int(seg), C.byref(o), stream)
+        d = {f: getattr(o, f) for f, _ in EvalOut._fields_}
+        d["dH_rel"] = d["dH"] / d["diag"] if d["diag"] > 0 else float("nan")
+        return d
 
     def last_launches(self) -> int:
         v = C.c_longlong()

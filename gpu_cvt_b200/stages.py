@@ -127,5 +127,31 @@ def hausdorff_cand_to_ref(ref_mesh, Vcand, Fcand) -> float:
     return ref_mesh.hausdorff_from(Vcand, Fcand, _stream())
 
 
+def extract_faces(S, U, V, knn, R2, max_faces=None):
+    """Dual triangles of the sites (cell_poly2d_kernel + emit_faces_from_labels_kernel
+    + sort/unique/degenerate filter, main.cu:928-974).  Returns an int32
+    CUDA tensor (nF, 3)."""
+    n, K = knn.shape
+    cap = int(max_faces or 4 * n + 64)
+    out = torch.empty((cap, 3), dtype=torch.int32, device=S.device)
+    nf = C.c_int()
+    try:
+        call("cvt_extract_faces", _p(S), _p(U), _p(V), _p(knn), int(n), int(K), float(R2), _p(out), cap,
+             C.byref(nf), _stream())
+    except _lib.CvtError as e:
+        if e.status != 5:
+            raise
+        return extract_faces(S, U, V, knn, R2, max_faces=nf.value)
+    return out[:nf.value]
+
+
+def quality(V, F) -> dict:
+    """Triangle quality metrics (eval_quality_angles_cpu, evaluate.cuh:388)."""
+    out = (C.c_float * 6)()
+    call("cvt_quality", _p(V), _p(F), F.shape[0], out, _stream())
+    keys = ["Qmin", "Qavg", "theta_min", "theta_min_avg", "theta_lt_30_pct", "theta_gt_90_pct"]
+    return dict(zip(keys, [float(x) for x in out]))
+
+
 def launch_count() -> int:
     return _lib.launch_count()

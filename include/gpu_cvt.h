@@ -137,6 +137,21 @@ typedef struct cvt_mesh* cvt_mesh_t;
 cvt_status_t cvt_hausdorff_to_mesh(cvt_mesh_t ref_mesh, const float* Vc, int nVc, const int* Fc, int nFc,
                                    float* out, void* stream);
 
+/* Replaces the in-repo surface extraction (cell_poly2d_kernel
+ * near_project.cuh:246-352, emit_faces_from_labels_kernel buildmesh.cuh:170-201,
+ * host sort/unique/decode/degenerate filter main.cu:928-974): dual triangles
+ * (i, j1, j2) of the sites' restricted Voronoi cells, sorted by their packed
+ * key, unique, degenerate ones (edge or area <= 1e-6) removed.  F_out: device,
+ * max_faces*3 ints; *n_faces (host) gets the count (also on CVT_ERR_CAPACITY,
+ * then nothing is written).  Synchronous. */
+cvt_status_t cvt_extract_faces(const float* S, const float* U, const float* V, const uint32_t* knn, int n, int K,
+                               float R2, int* F_out, int max_faces, int* n_faces, void* stream);
+
+/* Replaces eval_quality_angles_cpu (evaluate.cuh:388-462) as a device
+ * reduction.  out[6] (host) = Qmin, Qavg, theta_min, theta_min_avg,
+ * theta_lt_30_pct, theta_gt_90_pct.  Synchronous. */
+cvt_status_t cvt_quality(const float* V, const int* F, int nF, float* out, void* stream);
+
 /* ======================================================================
  * Resident meshes (main.cu:421-542: load, compact, normals, VF CSR, BVH)
  * ==================================================================== */
@@ -218,6 +233,16 @@ cvt_status_t cvt_engine_segment_iters(cvt_engine_t e, int seg_id, int* iters);
  * events on `stream`; ms[4] = average ms per iteration of {grid build, site
  * KNN kernel, per-site cell kernel, fallback + bookkeeping}.  Synchronous. */
 cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms, void* stream);
+/* The evaluation of main.cu:883-1040 for one segment: frames of the current
+ * sites, dual triangles with the last iteration's neighbour lists, quality,
+ * and the one-sided Hausdorff distance to the segment's mesh.  Synchronous. */
+typedef struct {
+  float dH;
+  float Qmin, Qavg, theta_min, theta_min_avg, theta_lt_30_pct, theta_gt_90_pct;
+  int n_faces;
+  float diag;  /* bbox diagonal of the segment's mesh */
+} cvt_eval_t;
+cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int seg_id, cvt_eval_t* out, void* stream);
 /* Kernel launches issued by the last cvt_engine_run (graph nodes included). */
 cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n);
 

@@ -1,0 +1,113 @@
+"""Fixtures from the reference's own CUDA build (GPU box only).
+
+    make -C oracle ref                      # in a container with the reference checkout
+    python tests/golden/make_ref_cuda_golden.py [out_dir]
+
+Runs oracle/_ref/ref_harness -- the reference's unmodified stage kernels
+(site_knn.cuh, 2dClip.cuh, near_project.cuh, site_normals.cuh,
+freezetest.cuh, buildmesh.cuh, evaluate.cuh) driven like main.cu:669-974 --
+on seeded workloads and stores small .npz fixtures (the oracle tests compare
+against them) plus ref_cuda_summary.json: the torus workload (100k sites,
+K=24, 100 iterations, mode 1) run by the reference kernels and by libgpucvt,
+with timings, Hausdorff figures and the site drift between the two.
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+
+from gpu_cvt_b200 import meshgen as mg  # noqa: E402
+from oracle import ref_runner  # noqa: E402
+
+
+def small_cases(out):
+    m, S, _ = mg.workload_mesh("icosphere_2k")
+    r = ref_runner.run(m.V, m.F, S, 20, 0, 50, dump=[1, 2, 5, 10, 50])
+    np.savez_compressed(os.path.join(out, "ref_cuda_icosphere_2k.npz"), S0=S, **{k: v for k, v in r.items()
+                                                                               if k not in ("stage_ms",)})
+    t = mg.torus(1.0, 0.3, 80, 40, noise_sigma=0.002, seed=1)
+    St = mg.sample_sites(t.V, t.F, 4000, seed=1)
+    for mode, dump in ((1, [1, 5, 30]), (2, [30])):
+        r = ref_runner.run(t.V, t.F, St, 24, mode, 30, dump=dump)
+        np.savez_compressed(os.path.join(out, f"ref_cuda_torus4k_mode{mode}.npz"), S0=St,
+                            **{k: v for k, v in r.items() if k not in ("stage_ms",)})
+
+
+def torus_100k(out):
+    import torch
+    from gpu_cvt_b200 import engine as E
+    m, S, p = mg.workload_mesh("torus_100k")
+    K, mode, iters = p["k"], p["mode"], p["iters"]
+    t0 = time.perf_counter()
+    r = ref_runner.run(m.V, m.F, S, K, mode, iters, dump=[1, iters])
+    ref_wall = time.perf_counter() - t0
+    diag = mg.bbox_diag(m.V)
+    summ = {"workload": "torus_100k", "sites": int(S.shape[0]), "k": K, "mode": mode, "iters": iters,
+            "reference_cuda": {"loop_wall_ms": r["wall_ms"], "process_wall_s": ref_wall,
+                               "stage_ms_sum": float(r["stage_ms"].sum()),
+                               "stage_ms_per_iter_mean": [float(x) for x in r["stage_ms"].mean(0)],
+                               "stage_names": ["knn_sites", "knn_site_to_mesh", "uv", "centroids",
+                                               "knn_centroid_to_mesh", "project"],
+                               "sites_iters_per_s_loop": S.shape[0] * iters / (r["wall_ms"] / 1e3),
+                               "frozen_end": int(r["frozen"].sum()), "dH": r["dH"], "dH_rel": r["dH"] / diag,
+                               "quality": [float(x) for x in r["quality"]], "n_faces": r["nfaces"],
+                               "counts_last": r["counts"][-1].tolist()}}
+    M = E.Mesh(m.V, m.F)
+    cells = E.grid_cells(M, S.shape[0], K)
+    for prof in ("ref", "mixed", "fp64"):
+        e = E.Engine(E.params(k=K, mode=mode, profile=prof), 1, S.shape[0], cells)
+        g = e.add(M, S)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e.run(iters)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        Sg = e.sites_f64(g) if prof == "fp64" else e.sites(g).astype(np.float64)
+        ev = e.evaluate(g)
+        st = e.state(g)
+        summ[f"gpucvt_{prof}"] = {"run_wall_ms": dt * 1e3, "frozen_end": int(st["frozen"].sum()), "dH": ev["dH"],
+                                  "dH_rel": ev["dH"] / diag, "n_faces": ev["n_faces"], "Qavg": ev["Qavg"],
+                                  "sites": Sg}
+        e.close()
+    ref_final = r["S"][-1].astype(np.float64)
+    ref_it1 = r["S"][0].astype(np.float64)
+    S64 = summ["gpucvt_fp64"]["sites"]
+    for prof in ("ref", "mixed", "fp64"):
+        Sg = summ[f"gpucvt_{prof}"].pop("sites")
+        d = np.linalg.norm(Sg - ref_final, axis=1) / diag
+        summ[f"gpucvt_{prof}"]["drift_vs_reference_cuda"] = {"max": float(d.max()), "mean": float(d.mean()),
+                                                            "p99": float(np.percentile(d, 99))}
+        d64 = np.linalg.norm(Sg - S64, axis=1) / diag
+        summ[f"gpucvt_{prof}"]["drift_vs_fp64"] = {"max": float(d64.max()), "mean": float(d64.mean())}
+    d = np.linalg.norm(ref_final - S64, axis=1) / diag
+    summ["reference_cuda"]["drift_vs_fp64"] = {"max": float(d.max()), "mean": float(d.mean())}
+    # first iteration: all profiles start from identical sites
+    e = E.Engine(E.params(k=K, mode=mode, profile="ref"), 1, S.shape[0], cells)
+    g = e.add(M, S)
+    e.run(1)
+    d1 = np.linalg.norm(e.sites(g).astype(np.float64) - ref_it1, axis=1) / diag
+    summ["gpucvt_ref"]["drift_vs_reference_cuda_iter1"] = {"max": float(d1.max()), "mean": float(d1.mean())}
+    e.close()
+    with open(os.path.join(out, "ref_cuda_summary.json"), "w") as fh:
+        json.dump(summ, fh, indent=1)
+    print(json.dumps(summ, indent=1))
+
+
+def main(out):
+    os.makedirs(out, exist_ok=True)
+    if not ref_runner.available():
+        raise SystemExit("oracle/_ref/ref_harness is missing: build it with `make -C oracle ref`")
+    small_cases(out)
+    torus_100k(out)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else HERE)

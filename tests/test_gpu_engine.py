@@ -151,3 +151,30 @@ def test_nan_and_tiny_segments(eng, oracle):
     S2, _, _ = run_engine(eng, m, S0, 32, 0, 3, profile="mixed")
     r2 = oracle.lloyd_run(m.V, m.F, S0, 32, 0, 3, profile=oracle.P_MIXED)
     assert np.array_equal(S2, r2["S"], equal_nan=True)
+
+
+def test_engine_evaluate_matches_oracle_pipeline(eng, oracle, small_torus):
+    """Evaluation after a freezing run: dual mesh, quality and Hausdorff of
+    the engine equal the oracle pipeline applied to the oracle's state."""
+    m, S0 = small_torus
+    M = eng.Mesh(m.V, m.F)
+    e = eng.Engine(eng.params(k=24, mode=1), 1, len(S0), eng.grid_cells(M, len(S0), 24))
+    g = e.add(M, S0)
+    e.run(12)
+    ev = e.evaluate(g)
+    r = oracle.lloyd_run(m.V, m.F, S0, 24, 1, 12)
+    S = r["S"]
+    No = oracle.vertex_normals(m.V, m.F)
+    nn = oracle.knn_vertices(m.V, S, 1)[:, 0]
+    nn = np.where(r["frozen"] > 0, r["knnv"][:, 0], nn)
+    U, V = oracle.frames(No, nn)
+    ext = S.max(0) - S.min(0)
+    R2 = float(np.float32(2.0) * np.float32(0.5) * np.float32(ext.max()))
+    F = oracle.extract_faces(S, U, V, r["knn"], R2)
+    assert ev["n_faces"] == len(F)
+    dH = oracle.hausdorff_one_sided(S, F, m.V, m.F)
+    assert abs(ev["dH"] - dH) <= 1e-6 * max(dH, 1e-12)
+    q = oracle.quality(S, F)
+    assert abs(ev["Qavg"] - q["Qavg"]) < 1e-5
+    e.close()
+    M.close()

@@ -236,3 +236,20 @@ def test_hausdorff(oracle):
     # best distance to the last ulp, hence a relative 1e-6 tolerance
     assert abs(got - exp) <= 1e-6 * exp
     mesh.close()
+
+
+def test_extract_faces_and_quality(st, oracle):
+    m = mg.icosphere(4)
+    S = mg.sample_sites(m.V, m.F, 1500, seed=2)
+    N = (S / np.linalg.norm(S, axis=1, keepdims=True)).astype(np.float32)
+    U, V = oracle.frames(N, np.arange(len(S)))
+    raw, _ = oracle.knn_points(S, 21, method="bf")
+    knn = oracle.drop_self(raw, 20)
+    R2 = float(mg.bbox_max_edge(S))
+    F = st.extract_faces(dev(S), dev(U), dev(V), dev(knn.view(np.int32)), R2)
+    Fo = oracle.extract_faces(S, U, V, knn, R2)
+    assert np.array_equal(host(F), Fo)
+    q = st.quality(dev(S), F)
+    qo = oracle.quality(S, Fo)
+    for k in qo:
+        assert abs(q[k] - qo[k]) <= 1e-4 * max(1.0, abs(qo[k])), k
