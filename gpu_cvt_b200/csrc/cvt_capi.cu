@@ -630,7 +630,11 @@ struct cvt_engine {
   MeshDev* d_meshes = nullptr;
   int* d_site_seg = nullptr;
   void* d_S[2] = {nullptr, nullptr};
-  uint32_t* d_knn[2] = {nullptr, nullptr};
+  uint32_t* d_knn = nullptr;
+  uint8_t* d_same = nullptr;
+  float* d_kth = nullptr;
+  int* d_act = nullptr;
+  int* d_act_count = nullptr;
   int* d_knnv = nullptr;
   int* d_nnv = nullptr;
   uint8_t* d_frozen = nullptr;
@@ -654,8 +658,8 @@ static void engine_free(cvt_engine* e) {
   for (int k = 0; k < 2; ++k) {
     if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
     cudaFree(e->d_S[k]);
-    cudaFree(e->d_knn[k]);
   }
+  cudaFree(e->d_knn); cudaFree(e->d_same); cudaFree(e->d_kth); cudaFree(e->d_act); cudaFree(e->d_act_count);
   cudaFree(e->d_segs); cudaFree(e->d_geom); cudaFree(e->d_active); cudaFree(e->d_meshes); cudaFree(e->d_site_seg);
   cudaFree(e->d_knnv); cudaFree(e->d_nnv); cudaFree(e->d_frozen); cudaFree(e->d_streak); cudaFree(e->d_tier);
   cudaFree(e->d_cellrank); cudaFree(e->d_sorted); cudaFree(e->d_cell_count); cudaFree(e->d_cell_start);
@@ -706,10 +710,12 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   ECK(cudaMalloc(&e->d_active, sizeof(int) * max_segments));
   ECK(cudaMalloc(&e->d_meshes, sizeof(MeshDev) * max_segments));
   ECK(cudaMalloc(&e->d_site_seg, sizeof(int) * ns));
-  for (int k = 0; k < 2; ++k) {
-    ECK(cudaMalloc(&e->d_S[k], tsz * 3 * ns));
-    ECK(cudaMalloc(&e->d_knn[k], sizeof(uint32_t) * e->K * ns));
-  }
+  for (int k = 0; k < 2; ++k) ECK(cudaMalloc(&e->d_S[k], tsz * 3 * ns));
+  ECK(cudaMalloc(&e->d_knn, sizeof(uint32_t) * e->K * ns));
+  ECK(cudaMalloc(&e->d_same, ns));
+  ECK(cudaMalloc(&e->d_kth, sizeof(float) * ns));
+  ECK(cudaMalloc(&e->d_act, sizeof(int) * ns));
+  ECK(cudaMalloc(&e->d_act_count, sizeof(int)));
   ECK(cudaMalloc(&e->d_knnv, sizeof(int) * kKProj * ns));
   ECK(cudaMalloc(&e->d_nnv, sizeof(int) * ns));
   ECK(cudaMalloc(&e->d_frozen, ns));
@@ -728,10 +734,9 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   ECK(cudaMemset(e->d_meshes, 0, sizeof(MeshDev) * max_segments));
   ECK(cudaMemset(e->d_stats, 0, sizeof(int) * (size_t)max_segments * kStatsRing * kStatsWords));
   ECK(cudaMemset(e->d_ovf, 0, sizeof(int)));
-  for (int k = 0; k < 2; ++k) {
-    ECK(cudaMemset(e->d_S[k], 0, tsz * 3 * ns));
-    ECK(cudaMemset(e->d_knn[k], 0, sizeof(uint32_t) * e->K * ns));
-  }
+  for (int k = 0; k < 2; ++k) ECK(cudaMemset(e->d_S[k], 0, tsz * 3 * ns));
+  ECK(cudaMemset(e->d_knn, 0, sizeof(uint32_t) * e->K * ns));
+  ECK(cudaMemset(e->d_same, 0, ns));
   k_fill_int<<<cdiv((long)ns, 256), 256>>>(e->d_site_seg, (int)ns, -1);
   LAUNCHED(1);
   ECK(cudaGetLastError());
@@ -769,6 +774,8 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   sd.mode = e->p.mode;
   sd.ex_quirk = e->p.ex_quirk;
   sd.iter = 0;
+  // twice the (K+1)-th squared distance of a uniform planar density n/area
+  sd.kth_est = (float)(2.0 * (e->K + 1) * (double)mesh->area / (M_PI * (double)n));
   MeshDev md = mesh->dev();
   static const int kStreak1[6] = {5, 10, 15, 20, 25, 25};  // main.cu:22, 543-553
   static const int kStreak2[6] = {5, 10, 15, 20, 25, 10};  // main.cu:39, 554-563
@@ -810,7 +817,10 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   CK(cudaMemsetAsync(e->d_frozen + base, 0, n, st));
   CK(cudaMemsetAsync(e->d_streak + base, 0, n, st));
   CK(cudaMemsetAsync(e->d_tier + base, 0, n, st));
-  for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(e->d_knn[k] + (size_t)e->K * base, 0, sizeof(uint32_t) * e->K * (size_t)n, st));
+  CK(cudaMemsetAsync(e->d_knn + (size_t)e->K * base, 0, sizeof(uint32_t) * e->K * (size_t)n, st));
+  CK(cudaMemsetAsync(e->d_same + base, 0, n, st));
+  k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_kth) + base, n, (int)0xbf800000);  // -1.0f
+  CKLAUNCH();
   CK(cudaMemsetAsync(e->d_stats + (size_t)s * kStatsRing * kStatsWords, 0, sizeof(int) * kStatsRing * kStatsWords, st));
   CK(cudaMemcpyAsync(e->d_active + s, &e->active[s], sizeof(int), cudaMemcpyHostToDevice, st));
   // the host mirrors above are read by the async copies; keep them stable
@@ -835,13 +845,13 @@ extern "C" cvt_status_t cvt_engine_remove_segment(cvt_engine_t e, int s) {
 
 constexpr int kCellBlockF = 128;
 constexpr int kCellBlockD = 64;
-constexpr int kCellCap = 32;
+constexpr int kCellCap = 16;
 
 template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   EngineArgs<T> a;
   a.segs = e->d_segs; a.geom = e->d_geom; a.active = e->d_active; a.meshes = e->d_meshes; a.site_seg = e->d_site_seg;
   a.S[0] = (T*)e->d_S[0]; a.S[1] = (T*)e->d_S[1];
-  a.knn[0] = e->d_knn[0]; a.knn[1] = e->d_knn[1];
+  a.knn = e->d_knn; a.same = e->d_same; a.kth = e->d_kth; a.act = e->d_act; a.act_count = e->d_act_count;
   a.knnv = e->d_knnv; a.nnv = e->d_nnv;
   a.frozen = e->d_frozen; a.streak = e->d_streak; a.tier = e->d_tier;
   a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
@@ -850,8 +860,8 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
 }
 
 template <class T, int KK>
-static void launch_site_knn(const EngineArgs<T>& a, int nsites, int parity, cudaStream_t st) {
-  k_site_knn<T, KK><<<cdiv(nsites, 128), 128, 0, st>>>(a, parity);
+static void launch_site_knn(const EngineArgs<T>& a, int nsites, int, cudaStream_t st) {
+  k_site_knn<T, KK><<<cdiv(nsites, kKnnBlock), kKnnBlock, 0, st>>>(a);
 }
 
 // ev (optional, 5 events): recorded before the grid build, after it, after
@@ -873,9 +883,12 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   k_grid_scatter<T><<<cdiv(ns, 256), 256, 0, st>>>(ns, (const T*)e->d_S[parity], e->d_cellrank, e->d_cell_start,
                                                    (Pt4<T>*)e->d_sorted);
   L++;
-  if (ev) CK(cudaEventRecord(ev[1], st));
   // cell_start[max_cells] is the number of gridded sites (read on the device)
   a.total_cells = e->max_cells;
+  CK(cudaMemsetAsync(e->d_act_count, 0, sizeof(int), st));
+  k_active_list<T><<<cdiv(ns, 256), 256, 0, st>>>(a);
+  L++;
+  if (ev) CK(cudaEventRecord(ev[1], st));
   switch (e->K) {
     case 8: launch_site_knn<T, 9>(a, ns, parity, st); break;
     case 12: launch_site_knn<T, 13>(a, ns, parity, st); break;
@@ -1033,7 +1046,7 @@ extern "C" cvt_status_t cvt_engine_get_state(cvt_engine_t e, int s, uint32_t* kn
   const SegDev& sd = e->segs[s];
   const size_t n = sd.n_sites, b = sd.site_base;
   // the list of the last completed iteration sits in the buffer it wrote
-  const uint32_t* kl = e->d_knn[e->parity ^ 1];
+  const uint32_t* kl = e->d_knn;
   if (knn) CK(cudaMemcpyAsync(knn, kl + (size_t)e->K * b, sizeof(uint32_t) * e->K * n, cudaMemcpyDeviceToHost, st));
   if (knnv) CK(cudaMemcpyAsync(knnv, e->d_knnv + 5 * b, sizeof(int) * 5 * n, cudaMemcpyDeviceToHost, st));
   if (frozen) CK(cudaMemcpyAsync(frozen, e->d_frozen + b, n, cudaMemcpyDeviceToHost, st));
@@ -1267,7 +1280,7 @@ extern "C" cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int s, cvt_eval_t* o
     std::memcpy(&hi[a], &q, 4);
   }
   float R2 = 2.0f * 0.5f * std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
-  const uint32_t* knn = e->d_knn[e->parity ^ 1] + (size_t)e->K * sd.site_base;
+  const uint32_t* knn = e->d_knn + (size_t)e->K * sd.site_base;
   int max_faces = 4 * n + 64;
   int* Fc;
   CK(sc.get(&Fc, 3 * (size_t)max_faces));

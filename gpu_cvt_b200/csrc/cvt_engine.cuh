@@ -27,6 +27,8 @@ constexpr int kStatsRing = 256;   // iterations of per-segment statistics kept
 constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter, -, -
 constexpr int kKProj = 5;         // KPROJ (main.cu:394)
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
+constexpr int kKnnBlock = 128;    // threads per block of the site KNN kernel
+constexpr int kKnnBuf = 32;       // parked candidates per thread (shared memory)
 
 struct MeshDev {
   const float* V;
@@ -49,6 +51,7 @@ struct SegDev {
   int mode;       // 0 / 1 / 2
   int ex_quirk;
   int iter;       // iterations completed (device-side count)
+  float kth_est;  // first-iteration estimate of the (K+1)-th squared distance
   float thr2_tier[6];
   int need_tier[6];
 };
@@ -65,7 +68,11 @@ template <class T> struct EngineArgs {
   const MeshDev* meshes;
   const int* site_seg;
   T* S[2];
-  uint32_t* knn[2];
+  uint32_t* knn;      // K neighbours per site (local indices), the current list
+  uint8_t* same;      // list unchanged vs the previous iteration (site KNN kernel)
+  float* kth;         // last (K+1)-th squared distance per site, < 0 unknown
+  int* act;           // sorted positions of the sites whose list is recomputed
+  int* act_count;
   int* knnv;
   int* nnv;
   uint8_t* frozen;
@@ -253,32 +260,51 @@ __device__ inline int tier_of(int mode, int i, int n, int K, const uint32_t* row
 }
 
 // ---------------------------------------------------------------------------
-// k_site_knn
+// k_active_list: sorted positions of the sites whose neighbour list is
+// recomputed this iteration (frozen sites keep theirs, main.cu:678); the
+// warp-aggregated append keeps runs of 32 spatially adjacent sites together
 // ---------------------------------------------------------------------------
-template <class T, int KK>
-__global__ void __launch_bounds__(128) k_site_knn(EngineArgs<T> a, int parity) {
+template <class T>
+__global__ void k_active_list(EngineArgs<T> a) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
-  if (t >= n_grid) return;
-  const Pt4<T> me = a.sorted[t];
+  bool act = false;
+  if (t < n_grid) {
+    const int g = (int)a.sorted[t].id;
+    act = !(a.segs[__ldg(a.site_seg + g)].mode != 0 && a.frozen[g]);
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, act);
+  const int lane = threadIdx.x & 31;
+  int base = 0;
+  if (lane == 0 && m) base = atomicAdd(a.act_count, __popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (act) a.act[base + __popc(m & ((1u << lane) - 1u))] = t;
+}
+
+// ---------------------------------------------------------------------------
+// k_site_knn: exact (K+1)-NN of every active site within its segment, self
+// dropped (site_knn.cuh:79-103); sets same[g] (list equal to the stored one)
+// and the frame vertex nnv[g]
+// ---------------------------------------------------------------------------
+template <class T, int KK>
+__global__ void __launch_bounds__(kKnnBlock) k_site_knn(EngineArgs<T> a) {
+  __shared__ uint32_t parked[kKnnBuf * kKnnBlock];
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= __ldg(a.act_count)) return;
+  const Pt4<T> me = a.sorted[a.act[t]];
   const int g = (int)me.id;
   const int s = __ldg(a.site_seg + g);
   const SegDev& sd = a.segs[s];
   const MeshDev& md = a.meshes[sd.mesh];
   constexpr int K = KK - 1;
-  uint32_t* row = a.knn[parity] + (size_t)g * K;
-  if (sd.mode != 0 && a.frozen[g]) {
-    const uint32_t* prow = a.knn[parity ^ 1] + (size_t)g * K;
-#pragma unroll
-    for (int k = 0; k < K; k += 4)
-      *reinterpret_cast<uint4*>(row + k) = *reinterpret_cast<const uint4*>(prow + k);
-    a.nnv[g] = a.knnv[(size_t)g * kKProj];
-    return;
-  }
   const V3<T> q{me.x, me.y, me.z};
   const GridGeom G = a.geom[s];
+  const float kp = a.kth[g];
+  const T thr0 = kp >= 0.f ? (T)kp * (T)1.5 : (T)sd.kth_est;
   TopK<T, KK> top;
-  grid_knn<T, T, KK>(G, a.cell_start, a.sorted, q, top, [](uint32_t) { return true; });
+  grid_knn_buffered<T, T, KK, kKnnBuf>(G, a.cell_start, a.sorted, q, top, thr0, parked + threadIdx.x, kKnnBlock,
+                                       [](uint32_t) { return true; });
+  a.kth[g] = top.full() ? (float)top.worst_d() : -1.f;
   // drop self (site_knn.cuh:79-103); local indices.  A point occurs at most
   // once in the list, so dropping it is a shift of the entries after it and
   // the K kept entries never need the reference's pad-with-last fallback.
@@ -292,6 +318,8 @@ __global__ void __launch_bounds__(128) k_site_knn(EngineArgs<T> a, int parity) {
     loc[k] = gid == 0xffffffffu ? 0xffffffffu : gid - base;
     if (loc[k] == i) p = k;
   }
+  uint32_t* row = a.knn + (size_t)g * K;
+  bool same = true;
 #pragma unroll
   for (int k = 0; k < K; k += 4) {
     uint4 v;
@@ -299,8 +327,13 @@ __global__ void __launch_bounds__(128) k_site_knn(EngineArgs<T> a, int parity) {
     v.y = (k + 1 < p) ? loc[k + 1] : loc[k + 2];
     v.z = (k + 2 < p) ? loc[k + 2] : loc[k + 3];
     v.w = (k + 3 < p) ? loc[k + 3] : loc[k + 4];
-    *reinterpret_cast<uint4*>(row + k) = v;
+    const uint4 o = *reinterpret_cast<const uint4*>(row + k);
+    if (o.x != v.x || o.y != v.y || o.z != v.z || o.w != v.w) {
+      same = false;
+      *reinterpret_cast<uint4*>(row + k) = v;
+    }
   }
+  a.same[g] = same ? 1 : 0;
   // nearest mesh vertex of the site (frame vertex)
   TopK<T, 1> v1;
   grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, v1, [](uint32_t) { return true; });
@@ -327,13 +360,13 @@ __device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>
   const MeshDev& md = a.meshes[sd.mesh];
   const int K = a.K;
   const T* __restrict__ S = a.S[parity];
-  const uint32_t* row = a.knn[parity] + (size_t)g * K;
+  const uint32_t* row = a.knn + (size_t)g * K;
   const int i = g - sd.site_base;
   const bool fz = sd.mode != 0 && a.frozen[g];
   const V3<T> si = ld3(S, g);
 
-  // frame from the nearest vertex normal
-  const int nn = a.nnv[g];
+  // frame from the nearest vertex normal (frozen sites: their kept vertex list)
+  const int nn = fz ? a.knnv[(size_t)g * kKProj] : a.nnv[g];
   Frame<T> fr;
   if (nn < 0) fr = {{(T)1, (T)0, (T)0}, {(T)0, (T)1, (T)0}};
   else fr = frame_from_normal(V3<T>{(T)__ldg(md.N + 3 * nn), (T)__ldg(md.N + 3 * nn + 1), (T)__ldg(md.N + 3 * nn + 2)});
@@ -400,13 +433,8 @@ __device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>
     a.streak[g] = 0;
   } else {
     const int tt = min((int)a.tier[g], 5);
-    const uint32_t* prow = a.knn[parity ^ 1] + (size_t)g * K;
-    bool same = true;
-    for (int k = 0; k < K; k += 4) {
-      uint4 x = *reinterpret_cast<const uint4*>(row + k);
-      uint4 y = *reinterpret_cast<const uint4*>(prow + k);
-      same = same && x.x == y.x && x.y == y.y && x.z == y.z && x.w == y.w;
-    }
+    // a frozen site's list is the previous one by construction
+    const bool same = fz || a.same[g] != 0;
     const bool low = d2 <= (T)sd.thr2_tier[tt];
     const bool both = same && low;
     int st = a.streak[g];

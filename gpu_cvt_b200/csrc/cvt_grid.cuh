@@ -144,6 +144,88 @@ __device__ __forceinline__ void grid_knn(const GridGeom& g, const int* __restric
   }
 }
 
+// Same search with buffered insertion.  Candidates with d <= thr are parked
+// in a per-thread shared-memory column (their sorted positions) and inserted
+// in batches, so the lanes of a warp run the insertion network together
+// instead of once per candidate that any one lane accepts.  thr starts at a
+// caller estimate (e.g. last iteration's K-th distance) and tightens to the
+// current K-th distance at every flush.  The result is exact whatever the
+// estimate: every skipped candidate lies above a threshold that is >= the
+// final K-th distance, and a threshold that proves too tight (the list is not
+// full although every point within it has been visited) restarts the search
+// with thr = +inf.
+template <class T, class PT, int KK, int CAPB, class Accept>
+__device__ __forceinline__ void grid_knn_buffered(const GridGeom& g, const int* __restrict__ cell_start,
+                                                  const Pt4<PT>* __restrict__ pts, V3<T> q, TopK<T, KK>& top,
+                                                  T thr0, uint32_t* buf, int stride, Accept accept) {
+  if (!finite3(q)) return;
+  const int cx = grid_coord(g, q.x, 0), cy = grid_coord(g, q.y, 1), cz = grid_coord(g, q.z, 2);
+  const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
+  const float slack = 1e-3f * g.h;
+  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
+  const int c[3] = {cx, cy, cz};
+  const T INF = (T)INFINITY;
+  T thr = thr0 > (T)0 ? thr0 : INF;
+  int cnt = 0;
+  auto flush = [&]() {
+    for (int k = 0; k < cnt; ++k) {
+      const Pt4<PT> p = pts[buf[k * stride]];
+      const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
+      top.insert(KeyOps<T>::make(d, p.id));
+    }
+    cnt = 0;
+    if (top.full()) thr = fmin(thr, top.worst_d());
+  };
+  auto scan_range = [&](int b, int e) {
+    for (int k = b; k < e; ++k) {
+      const Pt4<PT> p = pts[k];
+      if (!accept(p.id)) continue;
+      const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
+      if (d <= thr) {
+        if (cnt == CAPB) flush();
+        if (d <= thr) buf[(cnt++) * stride] = (uint32_t)k;
+      }
+    }
+  };
+  for (int r = 1; r <= rmax; ++r) {
+    const int z0 = max(cz - r, 0), z1 = min(cz + r, g.dim[2] - 1);
+    const int y0 = max(cy - r, 0), y1 = min(cy + r, g.dim[1] - 1);
+    const int x0 = max(cx - r, 0), x1 = min(cx + r, g.dim[0] - 1);
+    for (int z = z0; z <= z1; ++z) {
+      for (int y = y0; y <= y1; ++y) {
+        const int row = g.cell_base + (z * g.dim[1] + y) * g.dim[0];
+        const bool full_row = (r == 1) || abs(z - cz) == r || abs(y - cy) == r;
+        if (full_row) {
+          scan_range(__ldg(cell_start + row + x0), __ldg(cell_start + row + x1 + 1));
+        } else {
+          if (cx - r >= 0) scan_range(__ldg(cell_start + row + cx - r), __ldg(cell_start + row + cx - r + 1));
+          if (cx + r < g.dim[0]) scan_range(__ldg(cell_start + row + cx + r), __ldg(cell_start + row + cx + r + 1));
+        }
+      }
+    }
+    flush();
+    float m = __int_as_float(0x7f800000);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      if (c[a] - r > 0) m = fminf(m, qf[a] - (g.lo[a] + (float)(c[a] - r) * g.h));
+      if (c[a] + r < g.dim[a] - 1) m = fminf(m, (g.lo[a] + (float)(c[a] + r + 1) * g.h) - qf[a]);
+    }
+    const bool all_seen = isinf(m);
+    m -= slack;
+    if (top.full()) {
+      if (all_seen || (m > 0.f && (double)top.worst_d() < (double)m * (double)m)) break;
+    } else if (thr < INF && (all_seen || (m > 0.f && (double)thr < (double)m * (double)m))) {
+      // every point within the estimate has been seen and the list is not
+      // full: the estimate was too tight -- search again without it
+      thr = INF;
+      top = TopK<T, KK>();
+      r = 0;
+    } else if (all_seen) {
+      break;
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // grid build: count -> exclusive scan -> scatter
 // ---------------------------------------------------------------------------

@@ -159,7 +159,9 @@ template <class T> __device__ __forceinline__ V3<T> closest_point_tri(V3<T> P, V
 
 // closest point over the one-rings of the kproj nearest vertices
 // (project_centroids_to_mesh, near_project.cuh:149-189).  Q is the
-// arithmetic type (double for the MIXED barycentrics).
+// arithmetic type (double for the MIXED barycentrics).  A face that contains
+// an earlier listed vertex was already tested in that vertex's one-ring with
+// the same inputs; a repeat can never pass the strict '<', so it is skipped.
 template <class T, class Q>
 __device__ __forceinline__ V3<T> project_onering(V3<T> c, const float* __restrict__ V, int nV,
                                                  const int* __restrict__ F, int nF,
@@ -175,6 +177,12 @@ __device__ __forceinline__ V3<T> project_onering(V3<T> c, const float* __restric
       int fi = __ldg(fcs + ii);
       if ((unsigned)fi >= (unsigned)nF) continue;
       int ia = __ldg(F + 3 * fi), ib = __ldg(F + 3 * fi + 1), ic = __ldg(F + 3 * fi + 2);
+      bool seen = false;
+      for (int s = 0; s < t; ++s) {
+        const int w = knnv[s];
+        seen = seen || w == ia || w == ib || w == ic;
+      }
+      if (seen) continue;
       V3<Q> A = {(Q)__ldg(V + 3 * ia), (Q)__ldg(V + 3 * ia + 1), (Q)__ldg(V + 3 * ia + 2)};
       V3<Q> B = {(Q)__ldg(V + 3 * ib), (Q)__ldg(V + 3 * ib + 1), (Q)__ldg(V + 3 * ib + 2)};
       V3<Q> C = {(Q)__ldg(V + 3 * ic), (Q)__ldg(V + 3 * ic + 1), (Q)__ldg(V + 3 * ic + 2)};

@@ -14,8 +14,16 @@
 // The untimed duplicate KNN work of main.cu:883-909 does not change the
 // state and is skipped.
 //
+// knn_mode 0 uses the reference's hub KNN (run_knn_bitonic_hubs /
+// run_knn_bitonic_query_to_mesh).  knn_mode 1 replaces it by an exact
+// brute-force search (harness kernel below for site->site; the reference's
+// knn_vertices_bruteforce_k for site/centroid->vertex in modes 1/2), keeping
+// every other stage kernel of the reference: built for sm_100a with nvcc
+// 12.9 the hub KNN returns corrupted neighbour ids on B200 (most rows zero),
+// which makes knn_mode 0 unusable as a parity reference there.
+//
 // Usage: ref_harness <in.bin> <out.bin>
-//   in : int32 nV, nF, nS, K, mode, iters, ndump, dump_iters[ndump];
+//   in : int32 nV, nF, nS, K, mode, iters, knn_mode, ndump, dump_iters[ndump];
 //        float32 V[nV*3]; int32 F[nF*3]; float32 S[nS*3]
 //   out: int32 iters, ndump; float32 S_dump[ndump][nS*3]; int32 counts[iters*4];
 //        uint32 knn_it0[nS*K]; int32 knnv_it0[nS*5]; float32 cent_it0[nS*3];
@@ -41,6 +49,33 @@ namespace harness {
 
 constexpr int KPROJ = 5;
 constexpr int MAX_POLY = 256;
+
+// exact kk nearest sites (self included), ascending (distance, index);
+// frozen rows untouched (the contract of bitonic-hubs-grid.cuh:862-995)
+template <int KK>
+__global__ void bf_knn_sites(const float3* __restrict__ P, int n, const unsigned char* __restrict__ frozen,
+                             idx_t* __restrict__ knn, float* __restrict__ dist) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || frozen[i]) return;
+  float bd[KK];
+  idx_t bi[KK];
+  for (int t = 0; t < KK; ++t) { bd[t] = 3.0e38f; bi[t] = 0xffffffffu; }
+  float3 q = P[i];
+  for (int j = 0; j < n; ++j) {
+    float3 p = P[j];
+    float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+    float d = dx * dx + dy * dy + dz * dz;
+    if (d > bd[KK - 1] || (d == bd[KK - 1] && (idx_t)j > bi[KK - 1])) continue;
+    int pos = KK - 1;
+    bd[pos] = d; bi[pos] = (idx_t)j;
+    while (pos > 0 && (bd[pos] < bd[pos - 1] || (bd[pos] == bd[pos - 1] && bi[pos] < bi[pos - 1]))) {
+      float td = bd[pos - 1]; bd[pos - 1] = bd[pos]; bd[pos] = td;
+      idx_t ti = bi[pos - 1]; bi[pos - 1] = bi[pos]; bi[pos] = ti;
+      --pos;
+    }
+  }
+  for (int t = 0; t < KK; ++t) { knn[(size_t)i * KK + t] = bi[t]; dist[(size_t)i * KK + t] = bd[t]; }
+}
 
 template <int K>
 __global__ void restore_rows(const unsigned char* frozen, const idx_t* prev, idx_t* cur, int n) {
@@ -125,7 +160,7 @@ static void tiers(int mode, int n, int K, const std::vector<float>& sn, const st
 }
 
 struct In {
-  int nV, nF, nS, K, mode, iters;
+  int nV, nF, nS, K, mode, iters, knn_mode;
   std::vector<int> dump;
   std::vector<float> V, S;
   std::vector<int> F;
@@ -206,6 +241,31 @@ int run(const In& in, FILE* fo) {
   cudaMemcpy(dFcs, fcs.data(), fcs.size() * sizeof(int), cudaMemcpyHostToDevice);
 
   dim3 blk(256), grd((nS + 255) / 256);
+  cudaEvent_t k0, k1;
+  cudaEventCreate(&k0);
+  cudaEventCreate(&k1);
+  auto site_knn = [&](const float3* pts) -> float {
+    if (in.knn_mode == 0) return run_knn_bitonic_hubs(nS, K_SITE, dFrozen, pts, dRaw, dDist);
+    cudaEventRecord(k0);
+    bf_knn_sites<K_SITE><<<grd, blk>>>(pts, nS, dFrozen, dRaw, dDist);
+    cudaEventRecord(k1);
+    cudaEventSynchronize(k1);
+    float t = 0;
+    cudaEventElapsedTime(&t, k0, k1);
+    return t;
+  };
+  // site/centroid -> 5 nearest vertices for modes 1/2 (frozen rows untouched)
+  auto vertex_knn = [&](const float3* q, const char* name) -> float {
+    if (in.knn_mode == 0)
+      return run_knn_bitonic_query_to_mesh(nV, dV, q, nS, KPROJ, dFrozen, (idx_t*)dKnnV, dKnnVdist, name);
+    cudaEventRecord(k0);
+    knn_vertices_bruteforce_k<KPROJ, false><<<grd, blk>>>(dV, nV, q, nS, dFrozen, dKnnV);
+    cudaEventRecord(k1);
+    cudaEventSynchronize(k1);
+    float t = 0;
+    cudaEventElapsedTime(&t, k0, k1);
+    return t;
+  };
   std::vector<unsigned char> hTier(nS, 0);
   if (mode != 0) {
     static const int S1[6] = {5, 10, 15, 20, 25, 25};
@@ -214,7 +274,7 @@ int run(const In& in, FILE* fo) {
     for (int t = 0; t < 6; ++t) thr[t] = freeze_disp;
     cudaMemcpy(dThr, thr, sizeof(thr), cudaMemcpyHostToDevice);
     cudaMemcpy(dStreakTier, mode == 1 ? S1 : S2, 6 * sizeof(int), cudaMemcpyHostToDevice);
-    run_knn_bitonic_hubs(nS, K_SITE, dFrozen, dS, dRaw, dDist);
+    site_knn(dS);
     knn_drop_self_kernel<K_SITE, K_NEIGH, idx_t><<<grd, blk>>>(dRaw, dKNN, nS);
     knn_vertices_bruteforce_k<KPROJ, false><<<grd, blk>>>(dV, nV, dS, nS, dFrozen, dKnnV);
     cudaDeviceSynchronize();
@@ -247,12 +307,12 @@ int run(const In& in, FILE* fo) {
 
   for (int it = 0; it < iters; ++it) {
     float* st = &stage[(size_t)it * 6];
-    st[0] = run_knn_bitonic_hubs(nS, K_SITE, dFrozen, dS, dRaw, dDist);
+    st[0] = site_knn(dS);
     knn_drop_self_kernel<K_SITE, K_NEIGH, idx_t><<<grd, blk>>>(dRaw, dKNN, nS);
     if (mode != 0) restore_rows<K_NEIGH><<<grd, blk>>>(dFrozen, dPrev, dKNN, nS);
     if (mode != 0) {
       cudaMemcpy(dPrevKnnV, dKnnV, (size_t)nS * KPROJ * sizeof(int), cudaMemcpyDeviceToDevice);
-      st[1] = run_knn_bitonic_query_to_mesh(nV, dV, dS, nS, KPROJ, dFrozen, (idx_t*)dKnnV, dKnnVdist, "site_to_mesh");
+      st[1] = vertex_knn(dS, "site_to_mesh");
       restore_prev_knn_vertices_kernel<KPROJ><<<grd, blk>>>(dFrozen, dPrevKnnV, dKnnV, nS);
     } else {
       cudaEventRecord(e0);
@@ -270,7 +330,7 @@ int run(const In& in, FILE* fo) {
     st[3] = ms();
     if (mode != 0) {
       cudaMemcpy(dPrevKnnV, dKnnV, (size_t)nS * KPROJ * sizeof(int), cudaMemcpyDeviceToDevice);
-      st[4] = run_knn_bitonic_query_to_mesh(nV, dV, dCent, nS, KPROJ, dFrozen, (idx_t*)dKnnV, dKnnVdist, "centroid_to_mesh");
+      st[4] = vertex_knn(dCent, "centroid_to_mesh");
       restore_prev_knn_vertices_kernel<KPROJ><<<grd, blk>>>(dFrozen, dPrevKnnV, dKnnV, nS);
     } else {
       cudaEventRecord(e0);
@@ -321,7 +381,7 @@ int run(const In& in, FILE* fo) {
   cudaMemcpy(hS.data(), dS, nS * sizeof(float3), cudaMemcpyDeviceToHost);
   if (mode != 0) {
     cudaMemcpy(dPrevKnnV, dKnnV, (size_t)nS * KPROJ * sizeof(int), cudaMemcpyDeviceToDevice);
-    run_knn_bitonic_query_to_mesh(nV, dV, dS, nS, KPROJ, dFrozen, (idx_t*)dKnnV, dKnnVdist, "site_to_mesh");
+    vertex_knn(dS, "site_to_mesh");
     restore_prev_knn_vertices_kernel<KPROJ><<<grd, blk>>>(dFrozen, dPrevKnnV, dKnnV, nS);
   } else {
     knn_vertices_bruteforce_k<KPROJ, false><<<grd, blk>>>(dV, nV, dS, nS, dFrozen, dKnnV);
@@ -415,11 +475,12 @@ int main(int argc, char** argv) {
   FILE* fi = fopen(argv[1], "rb");
   if (!fi) return 2;
   harness::In in;
-  int hdr[7];
-  if (fread(hdr, 4, 7, fi) != 7) return 2;
+  int hdr[8];
+  if (fread(hdr, 4, 8, fi) != 8) return 2;
   in.nV = hdr[0]; in.nF = hdr[1]; in.nS = hdr[2]; in.K = hdr[3]; in.mode = hdr[4]; in.iters = hdr[5];
-  in.dump.resize(hdr[6]);
-  if (hdr[6] && fread(in.dump.data(), 4, hdr[6], fi) != (size_t)hdr[6]) return 2;
+  in.knn_mode = hdr[6];
+  in.dump.resize(hdr[7]);
+  if (hdr[7] && fread(in.dump.data(), 4, hdr[7], fi) != (size_t)hdr[7]) return 2;
   in.V.resize((size_t)in.nV * 3);
   in.F.resize((size_t)in.nF * 3);
   in.S.resize((size_t)in.nS * 3);
@@ -428,7 +489,7 @@ int main(int argc, char** argv) {
   if (fread(in.S.data(), 4, in.S.size(), fi) != in.S.size()) return 2;
   fclose(fi);
   // the hub index needs >= 1024 points per cell (bitonic-hubs-grid.cuh:1313-1318)
-  if (in.nS < 1024 || in.nV < 1024) {
+  if (in.knn_mode == 0 && (in.nS < 1024 || in.nV < 1024)) {
     fprintf(stderr, "the reference KNN needs at least 1024 sites and vertices\n");
     return 4;
   }

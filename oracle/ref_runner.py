@@ -21,7 +21,9 @@ def available() -> bool:
     return os.path.exists(BIN)
 
 
-def run(V, F, S, K, mode, iters, dump=(), timeout=1800):
+def run(V, F, S, K, mode, iters, dump=(), knn_mode=1, timeout=1800):
+    """knn_mode 0: the reference's hub KNN; 1: exact brute-force KNN with every
+    other stage done by the reference's kernels."""
     V = np.ascontiguousarray(V, np.float32)
     F = np.ascontiguousarray(F, np.int32)
     S = np.ascontiguousarray(S, np.float32)
@@ -30,7 +32,7 @@ def run(V, F, S, K, mode, iters, dump=(), timeout=1800):
     with tempfile.TemporaryDirectory() as td:
         fi, fo = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
         with open(fi, "wb") as fh:
-            fh.write(struct.pack("7i", nV, nF, nS, K, mode, iters, len(dump)))
+            fh.write(struct.pack("8i", nV, nF, nS, K, mode, iters, int(knn_mode), len(dump)))
             if dump:
                 fh.write(np.asarray(dump, np.int32).tobytes())
             fh.write(V.tobytes())
