@@ -28,7 +28,7 @@ constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter
 constexpr int kKProj = 5;         // KPROJ (main.cu:394)
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
 constexpr int kKnnBlock = 128;    // threads per block of the site KNN kernel
-constexpr int kKnnBuf = 32;       // parked candidates per thread (shared memory)
+constexpr int kKnnBuf = 64;       // parked candidates per thread (shared memory)
 
 struct MeshDev {
   const float* V;
@@ -148,10 +148,17 @@ __device__ __forceinline__ int clip_cell(const typename PT<PROF>::T* __restrict_
   cur.set(0, {-r, -r}); cur.set(1, {r, -r}); cur.set(2, {r, r}); cur.set(3, {-r, r});
   int n = 4;
   bool ovf = false;
+  // the next neighbour's position is loaded while the current one clips
+  uint32_t jn = __ldg(row);
+  V3<T> sn = jn < (uint32_t)n_sites ? ld3(S, (long)site_base + jn) : si;
   for (int t = 0; t < K; ++t) {
-    uint32_t j = __ldg(row + t);
+    const uint32_t j = jn;
+    const V3<T> sj = sn;
+    if (t + 1 < K) {
+      jn = __ldg(row + t + 1);
+      if (jn < (uint32_t)n_sites) sn = ld3(S, (long)site_base + jn);
+    }
     if (j >= (uint32_t)n_sites) continue;
-    V3<T> sj = ld3(S, (long)site_base + j);
     Q a, b, c;
     if (PROF == PROF_MIXED) {
       V3<double> d{(double)sj.x - (double)si.x, (double)sj.y - (double)si.y, (double)sj.z - (double)si.z};

@@ -146,18 +146,20 @@ __device__ __forceinline__ void grid_knn(const GridGeom& g, const int* __restric
 
 // Same search with buffered insertion.  Candidates with d <= thr are parked
 // in a per-thread shared-memory column (their sorted positions) and inserted
-// in batches, so the lanes of a warp run the insertion network together
-// instead of once per candidate that any one lane accepts.  thr starts at a
-// caller estimate (e.g. last iteration's K-th distance) and tightens to the
-// current K-th distance at every flush.  The result is exact whatever the
-// estimate: every skipped candidate lies above a threshold that is >= the
-// final K-th distance, and a threshold that proves too tight (the list is not
-// full although every point within it has been visited) restarts the search
-// with thr = +inf.
+// at the end of each ring, when every lane of the warp flushes at once, so the
+// lanes run the insertion network together instead of once per candidate that
+// any one lane accepts.  thr starts at a caller estimate (last iteration's
+// K-th distance) and tightens to the current K-th distance at every flush.
+// The result is exact whatever the estimate: a skipped candidate lies above a
+// threshold that is >= the final K-th distance; an estimate that proves too
+// tight (the list is not full although every point within it was visited)
+// restarts the search with thr = +inf; a buffer overflow restarts it in
+// direct-insertion mode (the plain search above).  CAPB >= KK.
 template <class T, class PT, int KK, int CAPB, class Accept>
 __device__ __forceinline__ void grid_knn_buffered(const GridGeom& g, const int* __restrict__ cell_start,
                                                   const Pt4<PT>* __restrict__ pts, V3<T> q, TopK<T, KK>& top,
                                                   T thr0, uint32_t* buf, int stride, Accept accept) {
+  static_assert(CAPB >= KK, "the buffer must hold a full list");
   if (!finite3(q)) return;
   const int cx = grid_coord(g, q.x, 0), cy = grid_coord(g, q.y, 1), cz = grid_coord(g, q.z, 2);
   const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
@@ -166,24 +168,18 @@ __device__ __forceinline__ void grid_knn_buffered(const GridGeom& g, const int* 
   const int c[3] = {cx, cy, cz};
   const T INF = (T)INFINITY;
   T thr = thr0 > (T)0 ? thr0 : INF;
+  bool direct = false, dropped = false;
   int cnt = 0;
-  auto flush = [&]() {
-    for (int k = 0; k < cnt; ++k) {
-      const Pt4<PT> p = pts[buf[k * stride]];
-      const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
-      top.insert(KeyOps<T>::make(d, p.id));
-    }
-    cnt = 0;
-    if (top.full()) thr = fmin(thr, top.worst_d());
-  };
   auto scan_range = [&](int b, int e) {
     for (int k = b; k < e; ++k) {
       const Pt4<PT> p = pts[k];
       if (!accept(p.id)) continue;
       const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
-      if (d <= thr) {
-        if (cnt == CAPB) flush();
-        if (d <= thr) buf[(cnt++) * stride] = (uint32_t)k;
+      if (direct) {
+        if (d <= top.worst_d()) top.insert(KeyOps<T>::make(d, p.id));
+      } else if (d <= thr) {
+        if (cnt < CAPB) buf[(cnt++) * stride] = (uint32_t)k;
+        else dropped = true;
       }
     }
   };
@@ -203,7 +199,22 @@ __device__ __forceinline__ void grid_knn_buffered(const GridGeom& g, const int* 
         }
       }
     }
-    flush();
+    if (!direct) {
+      for (int k = 0; k < cnt; ++k) {
+        const Pt4<PT> p = pts[buf[k * stride]];
+        const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
+        top.insert(KeyOps<T>::make(d, p.id));
+      }
+      cnt = 0;
+      if (dropped) {  // candidates within thr were not parked: start over, direct
+        top = TopK<T, KK>();
+        direct = true;
+        dropped = false;
+        r = 0;
+        continue;
+      }
+      if (top.full()) thr = fmin(thr, top.worst_d());
+    }
     float m = __int_as_float(0x7f800000);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -214,10 +225,11 @@ __device__ __forceinline__ void grid_knn_buffered(const GridGeom& g, const int* 
     m -= slack;
     if (top.full()) {
       if (all_seen || (m > 0.f && (double)top.worst_d() < (double)m * (double)m)) break;
-    } else if (thr < INF && (all_seen || (m > 0.f && (double)thr < (double)m * (double)m))) {
-      // every point within the estimate has been seen and the list is not
-      // full: the estimate was too tight -- search again without it
+    } else if (!direct && thr < INF && (all_seen || (m > 0.f && (double)thr < (double)m * (double)m))) {
+      // every point within the estimate was visited and the list is not full:
+      // the estimate was too tight -- search again, inserting directly
       thr = INF;
+      direct = true;
       top = TopK<T, KK>();
       r = 0;
     } else if (all_seen) {

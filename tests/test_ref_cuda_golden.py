@@ -1,0 +1,85 @@
+"""The oracle against the reference's own CUDA stage kernels.
+
+Fixtures: tests/golden/ref_cuda_*.npz, written on a B200 by
+tests/golden/make_ref_cuda_golden.py through oracle/ref_harness.cu, which runs
+the reference's unmodified kernels (frames, clip/centroid, vertex KNN,
+projection, freeze, normals, face extraction, Hausdorff) in the order of
+main.cu:669-974, with an exact brute-force site KNN in place of the hub KNN
+(whose output is corrupted on that GPU, see the first test).
+
+Bounds: identical neighbour lists and freeze counts; positions within 1e-6 of
+the bbox diagonal for the first iterations, 1e-5 after 10; after 30-50
+iterations Lloyd's sensitivity to last-bit differences (rsqrtf vs 1/sqrt, FMA
+contraction) allows an occasional flipped neighbour, so the mean stays below
+1e-6 and the max below 1e-4 of the diagonal.  Hausdorff within 1e-4 of the
+diagonal.  The libgpucvt kernels equal the oracle bit for bit (test_gpu_*), so
+the same bounds hold for them.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from gpu_cvt_b200 import meshgen as mg
+
+G = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(G, name))
+
+
+def test_reference_hub_knn_is_corrupted_on_b200(oracle):
+    g = load("ref_cuda_hubknn_icosphere_2k.npz")
+    raw, _ = oracle.knn_points(g["S0"], 21, method="bf")
+    exact = oracle.drop_self(raw, 20)
+    zero_rows = (g["knn0"] == 0).all(axis=1).mean()
+    overlap = np.mean([len(set(a) & set(b)) / 20 for a, b in zip(g["knn0"], exact)])
+    # documented defect of bitonic-hubs-grid.cuh / bitonic-shared.cuh on sm_100a
+    assert zero_rows > 0.5 and overlap < 0.2
+
+
+def test_icosphere_2k_against_reference_kernels(oracle):
+    g = load("ref_cuda_icosphere_2k.npz")
+    m, S0, p = mg.workload_mesh("icosphere_2k")
+    assert np.array_equal(g["S0"], S0)
+    diag = mg.bbox_diag(m.V)
+    raw, _ = oracle.knn_points(S0, 21, method="bf")
+    assert np.array_equal(g["knn0"], oracle.drop_self(raw, 20))
+    r1 = oracle.lloyd_run(m.V, m.F, S0, 20, 0, 1)
+    assert np.abs(g["cent0"] - r1["cent"]).max() / diag < 1e-6
+    for k, it in enumerate(g["dump_iters"]):
+        r = oracle.lloyd_run(m.V, m.F, S0, 20, 0, int(it))
+        d = np.linalg.norm(g["S"][k] - r["S"], axis=1) / diag
+        if it <= 10:
+            assert d.max() < (1e-6 if it <= 2 else 1e-5), it
+            assert np.array_equal(g["counts"][:it], r["counts"]), it
+        else:
+            assert d.mean() < 1e-6 and d.max() < 1e-4, it
+    # evaluation after 50 iterations: dual mesh + one-sided Hausdorff
+    r = oracle.lloyd_run(m.V, m.F, S0, 20, 0, 50)
+    S = r["S"]
+    No = oracle.vertex_normals(m.V, m.F)
+    U, V = oracle.frames(No, oracle.knn_vertices(m.V, S, 1)[:, 0])
+    ext = S.max(0) - S.min(0)
+    F = oracle.extract_faces(S, U, V, r["knn"], float(np.float32(ext.max())))
+    dH = oracle.hausdorff_one_sided(S, F, m.V, m.F)
+    assert abs(dH - float(g["dH"])) / diag < 1e-4
+    assert abs(len(F) - int(g["nfaces"])) <= 0.01 * len(F)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_torus_freezing_against_reference_kernels(oracle, mode):
+    g = load(f"ref_cuda_torus4k_mode{mode}.npz")
+    t = mg.torus(1.0, 0.3, 80, 40, noise_sigma=0.002, seed=1)
+    diag = mg.bbox_diag(t.V)
+    last = int(g["dump_iters"][-1])
+    r = oracle.lloyd_run(t.V, t.F, g["S0"], 24, mode, last)
+    assert np.array_equal(g["tier"], r["tier"])
+    assert abs(int(g["frozen"].sum()) - int(r["frozen"].sum())) <= 0.01 * len(r["frozen"])
+    assert (g["frozen"] == r["frozen"]).mean() > 0.99
+    d = np.linalg.norm(g["S"][-1] - r["S"], axis=1) / diag
+    assert d.mean() < 1e-6 and d.max() < 1e-4
+    if g["dump_iters"][0] == 1:
+        r1 = oracle.lloyd_run(t.V, t.F, g["S0"], 24, mode, 1)
+        assert np.linalg.norm(g["S"][0] - r1["S"], axis=1).max() / diag < 1e-6
