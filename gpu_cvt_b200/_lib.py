@@ -49,6 +49,7 @@ _SIGS = {
     "cvt_version": [],
     "cvt_launch_count": [],
     "cvt_knn_sites": [vp, i32, i32, vp, vp, vp, vp],
+    "cvt_knn_sites_noalloc": [vp, i32, i32, vp, vp, vp, vp],
     "cvt_knn_query_to_points": [vp, i32, vp, i32, i32, vp, vp, vp, vp],
     "cvt_knn_vertices": [vp, i32, vp, i32, i32, i32, vp, vp, vp],
     "cvt_knn_drop_self": [vp, i32, i32, i32, vp, vp],

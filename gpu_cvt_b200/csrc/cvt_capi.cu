@@ -1305,3 +1305,8 @@ extern "C" cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int s, cvt_eval_t* o
   out->diag = m->diag;
   return CVT_OK;
 }
+
+// ---------------------------------------------------------------------------
+// allocation-free site KNN (scratch in a fixed device array)
+// ---------------------------------------------------------------------------
+#include "cvt_noalloc.cu"

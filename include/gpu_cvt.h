@@ -61,6 +61,20 @@ unsigned long long cvt_launch_count(void);
 cvt_status_t cvt_knn_sites(const float* pts, int n, int kk, const uint8_t* frozen,
                            uint32_t* knn, float* dist, void* stream);
 
+/* No counterpart in the reference.  The same answer as cvt_knn_sites, for
+ * callers that cannot allocate device memory while they run (a serving
+ * process that reserved a fixed HBM budget up front, or a host whose own
+ * allocator owns the device heap): the search's temporaries live in one
+ * fixed array compiled into the library (about 5 MB, held on every GPU that
+ * loads the library until the process exits), so the call allocates and
+ * frees nothing.  At most CVT_NOALLOC_MAX_POINTS points (larger n returns
+ * CVT_ERR_CAPACITY).  All calls share the array: calls that overlap on the
+ * GPU race; keep them ordered on one stream.  The first call on a device
+ * looks up the array's address; make it before any stream capture. */
+#define CVT_NOALLOC_MAX_POINTS 131072
+cvt_status_t cvt_knn_sites_noalloc(const float* pts, int n, int kk, const uint8_t* frozen,
+                                   uint32_t* knn, float* dist, void* stream);
+
 /* Replaces run_knn_bitonic_query_to_mesh (site_knn.cuh:57-77): the kk nearest
  * of the n_cand candidate points for each of n_query query points. */
 cvt_status_t cvt_knn_query_to_points(const float* cand, int n_cand, const float* query, int n_query,
