@@ -861,7 +861,8 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
 
 template <class T, int KK>
 static void launch_site_knn(const EngineArgs<T>& a, int nsites, int, cudaStream_t st) {
-  k_site_knn<T, KK><<<cdiv(nsites, kKnnBlock), kKnnBlock, 0, st>>>(a);
+  // one warp per site
+  k_site_knn<T, KK><<<cdiv((long)nsites * 32, kKnnBlock), kKnnBlock, 0, st>>>(a);
 }
 
 // ev (optional, 5 events): recorded before the grid build, after it, after

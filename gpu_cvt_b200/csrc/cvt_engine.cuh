@@ -289,16 +289,18 @@ __global__ void k_active_list(EngineArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// k_site_knn: exact (K+1)-NN of every active site within its segment, self
-// dropped (site_knn.cuh:79-103); sets same[g] (list equal to the stored one)
-// and the frame vertex nnv[g]
+// k_site_knn: one warp per active site.  Exact (K+1)-NN within its segment,
+// self dropped (site_knn.cuh:79-103); lane j holds the j-th neighbour, so the
+// list row is read (for the freeze test's equality) and written coalesced.
+// Sets same[g] (new list == stored list), kth[g] and the frame vertex nnv[g].
 // ---------------------------------------------------------------------------
 template <class T, int KK>
 __global__ void __launch_bounds__(kKnnBlock) k_site_knn(EngineArgs<T> a) {
-  __shared__ uint32_t parked[kKnnBuf * kKnnBlock];
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= __ldg(a.act_count)) return;
-  const Pt4<T> me = a.sorted[a.act[t]];
+  using O = KeyOps<T>;
+  const int lane = threadIdx.x & 31;
+  const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  if (w >= __ldg(a.act_count)) return;  // whole warp
+  const Pt4<T> me = a.sorted[a.act[w]];
   const int g = (int)me.id;
   const int s = __ldg(a.site_seg + g);
   const SegDev& sd = a.segs[s];
@@ -308,43 +310,45 @@ __global__ void __launch_bounds__(kKnnBlock) k_site_knn(EngineArgs<T> a) {
   const GridGeom G = a.geom[s];
   const float kp = a.kth[g];
   const T thr0 = kp >= 0.f ? (T)kp * (T)1.5 : (T)sd.kth_est;
-  TopK<T, KK> top;
-  grid_knn_buffered<T, T, KK, kKnnBuf>(G, a.cell_start, a.sorted, q, top, thr0, parked + threadIdx.x, kKnnBlock,
-                                       [](uint32_t) { return true; });
-  a.kth[g] = top.full() ? (float)top.worst_d() : -1.f;
-  // drop self (site_knn.cuh:79-103); local indices.  A point occurs at most
-  // once in the list, so dropping it is a shift of the entries after it and
-  // the K kept entries never need the reference's pad-with-last fallback.
+  constexpr int R = (KK + 31) / 32;
+  typename O::Key key[R];
+  warp_knn<T, T, KK>(G, a.cell_start, a.sorted, q, thr0, lane, [](uint32_t) { return true; }, key);
+  const auto kth = shfl_key(key[(KK - 1) / 32], (KK - 1) % 32);
+  const bool full = !O::is_empty(kth);
+  if (lane == 0) a.kth[g] = full ? (float)O::dist(kth) : -1.f;
+  // drop self: the entries after self move down one place
   const uint32_t base = (uint32_t)sd.site_base;
   const uint32_t i = (uint32_t)g - base;
-  uint32_t loc[KK];
+  uint32_t loc[R];
+  unsigned selfmask[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const uint32_t gid = O::idx(key[r]);
+    loc[r] = gid == 0xffffffffu ? 0xffffffffu : gid - base;
+    selfmask[r] = __ballot_sync(0xffffffffu, 32 * r + lane < KK && loc[r] == i);
+  }
   int p = K;
 #pragma unroll
-  for (int k = KK - 1; k >= 0; --k) {
-    uint32_t gid = KeyOps<T>::idx(top.k[k]);
-    loc[k] = gid == 0xffffffffu ? 0xffffffffu : gid - base;
-    if (loc[k] == i) p = k;
+  for (int r = R - 1; r >= 0; --r)
+    if (selfmask[r]) p = 32 * r + __ffs(selfmask[r]) - 1;
+  // entry j of the output (j < K <= 32) is loc[j] before self, loc[j+1] after
+  uint32_t next = __shfl_down_sync(0xffffffffu, loc[0], 1);
+  if (R > 1) {
+    const uint32_t first1 = __shfl_sync(0xffffffffu, loc[R - 1], 0);
+    if (lane == 31) next = first1;
   }
+  const uint32_t out = lane < p ? loc[0] : next;
   uint32_t* row = a.knn + (size_t)g * K;
-  bool same = true;
-#pragma unroll
-  for (int k = 0; k < K; k += 4) {
-    uint4 v;
-    v.x = (k + 0 < p) ? loc[k + 0] : loc[k + 1];
-    v.y = (k + 1 < p) ? loc[k + 1] : loc[k + 2];
-    v.z = (k + 2 < p) ? loc[k + 2] : loc[k + 3];
-    v.w = (k + 3 < p) ? loc[k + 3] : loc[k + 4];
-    const uint4 o = *reinterpret_cast<const uint4*>(row + k);
-    if (o.x != v.x || o.y != v.y || o.z != v.z || o.w != v.w) {
-      same = false;
-      *reinterpret_cast<uint4*>(row + k) = v;
-    }
+  bool diff = false;
+  if (lane < K) {
+    diff = row[lane] != out;
+    if (diff) row[lane] = out;
   }
-  a.same[g] = same ? 1 : 0;
+  const unsigned changed = __ballot_sync(0xffffffffu, diff);
+  if (lane == 0) a.same[g] = changed ? 0 : 1;
   // nearest mesh vertex of the site (frame vertex)
-  TopK<T, 1> v1;
-  grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, v1, [](uint32_t) { return true; });
-  a.nnv[g] = (int)KeyOps<T>::idx(v1.k[0]);
+  const auto nv = warp_nearest<T, float>(md.vg, md.vcell_start, md.vsorted, q, lane);
+  if (lane == 0) a.nnv[g] = (int)O::idx(nv);
 }
 
 // ---------------------------------------------------------------------------

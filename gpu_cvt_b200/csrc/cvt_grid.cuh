@@ -239,6 +239,196 @@ __device__ __forceinline__ void grid_knn_buffered(const GridGeom& g, const int* 
 }
 
 // ---------------------------------------------------------------------------
+// warp-cooperative search: one warp per query point
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long shfl_key(unsigned long long k, int src) {
+  return __shfl_sync(0xffffffffu, k, src);
+}
+__device__ __forceinline__ DKey shfl_key(DKey k, int src) {
+  return {__shfl_sync(0xffffffffu, k.d, src), __shfl_sync(0xffffffffu, k.i, src)};
+}
+__device__ __forceinline__ unsigned long long shfl_up_key(unsigned long long k) {
+  return __shfl_up_sync(0xffffffffu, k, 1);
+}
+__device__ __forceinline__ DKey shfl_up_key(DKey k) {
+  return {__shfl_up_sync(0xffffffffu, k.d, 1), __shfl_up_sync(0xffffffffu, k.i, 1)};
+}
+__device__ __forceinline__ unsigned long long min_key(unsigned long long) { return 0ull; }
+__device__ __forceinline__ DKey min_key(DKey) { return {-INFINITY, 0u}; }
+
+// Visit the candidates of Chebyshev ring r around (cx,cy,cz) in chunks of 32:
+// every lane calls visit(pos) the same number of times, pos = a sorted
+// position or -1.  The ring's cell ranges (two slots per (z,y) row: the whole
+// x-range for rows on the shell's faces, else the two end cells) are spread
+// over the lanes, their lengths warp-scanned, and each lane finds the range of
+// its candidate by a shuffle binary search over the prefix sums.
+template <class Visit>
+__device__ __forceinline__ void warp_ring(const GridGeom& g, const int* __restrict__ cell_start, int cx, int cy,
+                                          int cz, int r, int lane, Visit&& visit) {
+  const int z0 = max(cz - r, 0), z1 = min(cz + r, g.dim[2] - 1);
+  const int y0 = max(cy - r, 0), y1 = min(cy + r, g.dim[1] - 1);
+  const int x0 = max(cx - r, 0), x1 = min(cx + r, g.dim[0] - 1);
+  const int ny = y1 - y0 + 1;
+  const int nslots = 2 * (z1 - z0 + 1) * ny;
+  for (int base = 0; base < nslots; base += 32) {
+    const int slot = base + lane;
+    int b = 0, e = 0;
+    if (slot < nslots) {
+      const int rowi = slot >> 1, which = slot & 1;
+      const int z = z0 + rowi / ny, y = y0 + rowi % ny;
+      const int row = g.cell_base + (z * g.dim[1] + y) * g.dim[0];
+      const bool full_row = (r == 1) || abs(z - cz) == r || abs(y - cy) == r;
+      if (full_row) {
+        if (which == 0) { b = __ldg(cell_start + row + x0); e = __ldg(cell_start + row + x1 + 1); }
+      } else {
+        const int x = which == 0 ? cx - r : cx + r;
+        if (x >= 0 && x < g.dim[0]) { b = __ldg(cell_start + row + x); e = __ldg(cell_start + row + x + 1); }
+      }
+    }
+    const int len = e - b;
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - len;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    for (int c = 0; c < total; c += 32) {
+      const int i = c + lane;
+      int lo = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int probe = lo + step;
+        const int ex = __shfl_sync(0xffffffffu, excl, probe & 31);
+        if (probe < 32 && ex <= i) lo = probe;
+      }
+      const int rb = __shfl_sync(0xffffffffu, b, lo);
+      const int rex = __shfl_sync(0xffffffffu, excl, lo);
+      visit(i < total ? rb + (i - rex) : -1);
+    }
+  }
+}
+
+// lower bound on the distance from q to any cell outside ring r (+inf when
+// the visited block covers the grid)
+__device__ __forceinline__ float ring_margin(const GridGeom& g, const float qf[3], const int c[3], int r) {
+  float m = __int_as_float(0x7f800000);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    if (c[a] - r > 0) m = fminf(m, qf[a] - (g.lo[a] + (float)(c[a] - r) * g.h));
+    if (c[a] + r < g.dim[a] - 1) m = fminf(m, (g.lo[a] + (float)(c[a] + r + 1) * g.h) - qf[a]);
+  }
+  return m;
+}
+
+// Exact KK nearest points of q (uniform across the warp), KK <= 64.  The
+// sorted list spans R = ceil(KK/32) registers per lane: list[r] at lane j is
+// entry 32*r + j.  Candidates beyond the estimate thr0 are skipped; an
+// estimate that proves too tight restarts the search without it (see
+// grid_knn_buffered for why the result is exact).
+template <class T, class PT, int KK, class Accept>
+__device__ __forceinline__ void warp_knn(const GridGeom& g, const int* __restrict__ cell_start,
+                                         const Pt4<PT>* __restrict__ pts, V3<T> q, T thr0, int lane, Accept accept,
+                                         typename KeyOps<T>::Key (&list)[(KK + 31) / 32]) {
+  constexpr int R = (KK + 31) / 32;
+  static_assert(KK <= 64, "at most two keys per lane");
+  using O = KeyOps<T>;
+  using Key = typename O::Key;
+#pragma unroll
+  for (int r = 0; r < R; ++r) list[r] = O::empty();
+  if (!finite3(q)) return;
+  const int c[3] = {grid_coord(g, q.x, 0), grid_coord(g, q.y, 1), grid_coord(g, q.z, 2)};
+  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
+  const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
+  const float slack = 1e-3f * g.h;
+  const T INF = (T)INFINITY;
+  constexpr int KR = (KK - 1) / 32, KL = (KK - 1) % 32;  // the K-th entry
+  T thr = thr0 > (T)0 ? thr0 : INF;
+  Key kth = O::empty();
+  for (int ring = 1; ring <= rmax; ++ring) {
+    warp_ring(g, cell_start, c[0], c[1], c[2], ring, lane, [&](int pos) {
+      Key key = O::empty();
+      bool pass = false;
+      if (pos >= 0) {
+        const Pt4<PT> p = pts[pos];
+        if (accept(p.id)) {
+          const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
+          key = O::make(d, p.id);
+          pass = d <= thr && O::less(key, kth);
+        }
+      }
+      unsigned mask = __ballot_sync(0xffffffffu, pass);
+      if (mask) {
+        while (mask) {
+          const int src = __ffs(mask) - 1;
+          mask &= mask - 1;
+          const Key x = shfl_key(key, src);
+          // new[j] = max(old[j-1], min(old[j], x)) over the whole list.  A key
+          // that is no longer below the K-th entry leaves entries < KK
+          // unchanged, so the K-th entry is refreshed once per chunk; lanes
+          // past the list's end hold overflow entries that are never read.
+          Key carry = min_key(x);
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            Key prev = shfl_up_key(list[r]);
+            if (lane == 0) prev = carry;
+            if (r + 1 < R) carry = shfl_key(list[r], 31);
+            list[r] = O::kmax(prev, O::kmin(list[r], x));
+          }
+        }
+        kth = shfl_key(list[KR], KL);
+      }
+    });
+    const bool full = !O::is_empty(kth);
+    if (full) thr = fmin(thr, O::dist(kth));
+    float m = ring_margin(g, qf, c, ring);
+    const bool all_seen = isinf(m);
+    m -= slack;
+    if (full) {
+      if (all_seen || (m > 0.f && (double)O::dist(kth) < (double)m * (double)m)) break;
+    } else if (thr < INF && (all_seen || (m > 0.f && (double)thr < (double)m * (double)m))) {
+      thr = INF;
+#pragma unroll
+      for (int r = 0; r < R; ++r) list[r] = O::empty();
+      kth = O::empty();
+      ring = 0;
+    } else if (all_seen) {
+      break;
+    }
+  }
+}
+
+// Nearest point of q (uniform across the warp); every lane returns its key.
+template <class T, class PT>
+__device__ __forceinline__ typename KeyOps<T>::Key warp_nearest(const GridGeom& g, const int* __restrict__ cell_start,
+                                                                const Pt4<PT>* __restrict__ pts, V3<T> q, int lane) {
+  using O = KeyOps<T>;
+  using Key = typename O::Key;
+  Key best = O::empty();
+  if (!finite3(q)) return best;
+  const int c[3] = {grid_coord(g, q.x, 0), grid_coord(g, q.y, 1), grid_coord(g, q.z, 2)};
+  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
+  const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
+  const float slack = 1e-3f * g.h;
+  for (int r = 1; r <= rmax; ++r) {
+    warp_ring(g, cell_start, c[0], c[1], c[2], r, lane, [&](int pos) {
+      if (pos >= 0) {
+        const Pt4<PT> p = pts[pos];
+        best = O::kmin(best, O::make(dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q), p.id));
+      }
+    });
+#pragma unroll
+    for (int o = 16; o; o >>= 1) best = O::kmin(best, shfl_key(best, lane ^ o));
+    float m = ring_margin(g, qf, c, r);
+    if (isinf(m)) break;
+    m -= slack;
+    if (!O::is_empty(best) && m > 0.f && (double)O::dist(best) < (double)m * (double)m) break;
+  }
+  return best;
+}
+
+// ---------------------------------------------------------------------------
 // grid build: count -> exclusive scan -> scatter
 // ---------------------------------------------------------------------------
 struct SegGrid {           // the minimal per-point view the build needs
