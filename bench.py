@@ -127,9 +127,10 @@ def knn_bytes_per_site(K):
 
 
 def cell_bytes_per_site(K):
-    # position 12 + ids read 4K (clip) + previous ids 4K (freeze) + frame id 4
-    # + frozen/streak/tier 3 + vertex ids 20 (write) + new position 12 + flags 2
-    return 12 + 8 * K + 4 + 3 + 20 + 12 + 2
+    # position 12 + neighbour ids read 4K + frame vertex 4 + flags read 4
+    # (frozen, streak, tier, same) + vertex ids 20 + new position 12 + flags
+    # written 2
+    return 12 + 4 * K + 4 + 4 + 20 + 12 + 2
 
 
 def traffic_from_profiles(kernel_key):
@@ -288,9 +289,10 @@ def run_ours(args):
     h2d = int(V.nbytes + F.nbytes + S.nbytes)
     d2h = int(S.nbytes + 16 * iters)
 
-    # ---- per-kernel timing (CUDA events on the launching stream) ---------
+    # ---- per-kernel timing (CUDA events on the launching stream) over one
+    # whole remesh: average per launch of each kernel group --------------
     reset()
-    prof = eng.profile(10, sp)
+    prof = eng.profile(iters, sp)
     K = p["k"]
     groups = {"k_site_knn": (prof["knn"], knn_bytes_per_site(K)), "k_site_cell": (prof["cell"], cell_bytes_per_site(K))}
     dom = max(groups, key=lambda g: groups[g][0])
@@ -340,6 +342,26 @@ def run_ours(args):
     return 0
 
 
+def run_batched(args):
+    """many procedural meshes in one engine vs the plain
+    per-mesh loop (same kernels, one mesh at a time)."""
+    import torch
+    from gpu_cvt_b200 import workloads
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    r = workloads.batched_vs_plain(n_meshes=args.meshes, iters=100, k=24, mode=0, profile="ref", seed=3)
+    line = {"metric": METRIC, "value": r["batched_sites_iters_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1,
+            "warmup": 1, "ms_per_step": r["batched_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched_{args.meshes}_meshes", "seed": 3, "k": 24, "iters": 100, "mode": 0,
+                       "profile": "ref", "sites_total": r["sites_total"],
+                       "tris_per_mesh": [r["tris_min"], r["tris_max"]]},
+            "plain_loop": {"value": r["plain_sites_iters_per_s"], "ms": r["plain_loop_s"] * 1e3},
+            "batched_over_plain": r["speedup"], "identical_results": r["identical_results"],
+            "mesh_generation_s": r["mesh_generation_s"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -349,9 +371,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--workload", choices=["torus_100k", "batched"], default="torus_100k")
+    ap.add_argument("--meshes", type=int, default=256)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
     return run_ours(args)
 
 

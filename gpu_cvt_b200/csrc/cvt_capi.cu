@@ -677,6 +677,8 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   if (p->kproj != kKProj) return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: kproj must be 5");
   if (p->mode < 0 || p->mode > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: mode must be 0, 1 or 2");
   if (p->profile < 0 || p->profile > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: profile");
+  if ((long)max_cells > (long)kScanTile * kScanThreads * kScanItems)
+    return fail(CVT_ERR_CAPACITY, "cvt_engine_create: max_cells above the scan limit (16,777,216)");
   cvt_engine* e = new cvt_engine();
   e->p = *p;
   e->K = p->k;

@@ -1,0 +1,116 @@
+"""The multi-mesh workloads: batched (many meshes in one engine) and the
+plain per-mesh loop it is measured against.
+
+Batched: a seeded set of procedural meshes (spheres, tori, superquadrics,
+5k-200k triangles each) with log-uniform site counts, all placed as segments
+of ONE engine, so every Lloyd iteration of every mesh is one pass of the fused
+kernels replayed from a CUDA graph.  Plain loop: the same meshes one after
+another through the same engine type (one segment at a time) -- the way the
+reference's driver handles one mesh per process run.
+"""
+from __future__ import annotations
+
+import math
+import time
+
+import numpy as np
+
+from . import engine as E
+from . import meshgen as mg
+
+
+def batched_set(seed: int = 3, n_meshes: int = 256, tri_lo: int = 5_000, tri_hi: int = 200_000,
+                site_lo: int = 1_000, site_hi: int = 50_000):
+    """[(name, V, F, sites)] for the batched workload (seeded)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_meshes):
+        m = mg.procedural_family(rng, tri_lo, tri_hi)
+        n = int(round(math.exp(rng.uniform(math.log(site_lo), math.log(site_hi)))))
+        S = mg.sample_sites(m.V, m.F, n, seed=int(rng.integers(0, 2**31 - 1)))
+        out.append((m.name, m.V, m.F, S))
+    return out
+
+
+def _sync():
+    import torch
+    torch.cuda.synchronize()
+
+
+def run_batched(meshes, k=24, mode=0, profile="ref", iters=100, stream=None):
+    """All meshes as segments of one engine; returns (seconds, engine, segs).
+    Mesh upload/preprocessing is outside the timed region."""
+    import torch
+    M = [E.Mesh(V, F) for _, V, F, _ in meshes]
+    n_tot = sum(S.shape[0] for *_, S in meshes)
+    cells = sum(E.grid_cells(m, S.shape[0], k) for m, (*_, S) in zip(M, meshes))
+    eng = E.Engine(E.params(k=k, mode=mode, profile=profile), len(meshes), n_tot, cells)
+    segs = [eng.add(m, S) for m, (*_, S) in zip(M, meshes)]
+    eng.run(1, stream)          # graph capture + first iteration (untimed warm-up)
+    _sync()
+    for s in list(segs):        # restart every segment from its initial sites
+        eng.remove(s)
+    segs = [eng.add(m, S) for m, (*_, S) in zip(M, meshes)]
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    eng.run(iters, C_stream(st))
+    e1.record(st)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / 1e3, eng, segs, M
+
+
+def run_plain_loop(meshes, k=24, mode=0, profile="ref", iters=100):
+    """One mesh at a time through one engine sized for the largest; every
+    mesh's 100 iterations replayed from the same CUDA graphs."""
+    import torch
+    M = [E.Mesh(V, F) for _, V, F, _ in meshes]
+    nmax = max(S.shape[0] for *_, S in meshes)
+    cells = max(E.grid_cells(m, S.shape[0], k) for m, (*_, S) in zip(M, meshes))
+    eng = E.Engine(E.params(k=k, mode=mode, profile=profile), 1, nmax, cells)
+    st = torch.cuda.current_stream()
+    g = eng.add(M[0], meshes[0][3])
+    eng.run(2, C_stream(st))    # graph capture (untimed)
+    _sync()
+    eng.remove(g)
+    total = 0.0
+    finals = []
+    for m, (*_, S) in zip(M, meshes):
+        g = eng.add(m, S)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        eng.run(iters, C_stream(st))
+        e1.record(st)
+        e1.synchronize()
+        total += e0.elapsed_time(e1) / 1e3
+        finals.append(eng.sites(g))
+        eng.remove(g)
+    eng.close()
+    for m in M:
+        m.close()
+    return total, finals
+
+
+def C_stream(st):
+    import ctypes
+    return ctypes.c_void_p(st.cuda_stream)
+
+
+def batched_vs_plain(n_meshes=256, iters=100, k=24, mode=0, profile="ref", seed=3, check=True):
+    t0 = time.perf_counter()
+    meshes = batched_set(seed=seed, n_meshes=n_meshes)
+    gen_s = time.perf_counter() - t0
+    n_tot = sum(S.shape[0] for *_, S in meshes)
+    tb, eng, segs, M = run_batched(meshes, k=k, mode=mode, profile=profile, iters=iters)
+    batched_sites = [eng.sites(s) for s in segs]
+    eng.close()
+    for m in M:
+        m.close()
+    tp, finals = run_plain_loop(meshes, k=k, mode=mode, profile=profile, iters=iters)
+    same = all(np.array_equal(a, b) for a, b in zip(batched_sites, finals)) if check else None
+    tris = [F.shape[0] for _, _, F, _ in meshes]
+    return {"meshes": n_meshes, "sites_total": int(n_tot), "tris_min": int(min(tris)), "tris_max": int(max(tris)),
+            "k": k, "mode": mode, "profile": profile, "iters": iters,
+            "batched_s": tb, "plain_loop_s": tp,
+            "batched_sites_iters_per_s": n_tot * iters / tb, "plain_sites_iters_per_s": n_tot * iters / tp,
+            "speedup": tp / tb, "identical_results": same, "mesh_generation_s": gen_s}
