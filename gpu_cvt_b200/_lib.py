@@ -80,6 +80,9 @@ _SIGS = {
     "cvt_engine_segment_iters": [vp, i32, vp],
     "cvt_engine_last_launches": [vp, vp],
     "cvt_engine_profile": [vp, i32, vp, vp],
+    "cvt_engine_set_stop": [vp, i32, f32, i32],
+    "cvt_engine_poll": [vp, vp, vp, i32, vp],
+    "cvt_mesh_sample_sites": [vp, i32, u64, vp, vp],
     "cvt_engine_evaluate": [vp, i32, vp, vp],
     "cvt_extract_faces": [vp, vp, vp, vp, i32, i32, f32, vp, i32, vp, vp],
     "cvt_quality": [vp, vp, i32, vp, vp],

@@ -331,6 +331,7 @@ struct cvt_mesh {
   int* doff = nullptr;
   int* dfcs = nullptr;
   float* dN = nullptr;
+  double* dcdf = nullptr;  // face-area prefix sums (site sampler)
   GridGeom vg{};
   int* dvcell_start = nullptr;
   Pt4<float>* dvsorted = nullptr;
@@ -352,7 +353,7 @@ struct cvt_mesh {
 
 static void mesh_free(cvt_mesh* m) {
   if (!m) return;
-  cudaFree(m->dV); cudaFree(m->dF); cudaFree(m->doff); cudaFree(m->dfcs); cudaFree(m->dN);
+  cudaFree(m->dV); cudaFree(m->dF); cudaFree(m->doff); cudaFree(m->dfcs); cudaFree(m->dN); cudaFree(m->dcdf);
   cudaFree(m->dvcell_start); cudaFree(m->dvsorted); cudaFree(m->dnodes); cudaFree(m->dtri);
   delete m;
 }
@@ -474,6 +475,7 @@ extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, in
   MCK(dmalloc(&m->dvsorted, (size_t)nn, &acc));
   MCK(dmalloc(&m->dnodes, nodes.size(), &acc));
   MCK(dmalloc(&m->dtri, tri.size(), &acc));
+  MCK(dmalloc(&m->dcdf, (size_t)nF, &acc));
   m->bytes = acc;
   cudaStream_t st = 0;
   MCK(cudaMemcpyAsync(m->dV, m->hV.data(), sizeof(float) * 3 * nn, cudaMemcpyHostToDevice, st));
@@ -482,6 +484,21 @@ extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, in
   MCK(cudaMemcpyAsync(m->dfcs, fcs.data(), sizeof(int) * 3 * (size_t)nF, cudaMemcpyHostToDevice, st));
   MCK(cudaMemcpyAsync(m->dnodes, nodes.data(), sizeof(BVHNode) * nodes.size(), cudaMemcpyHostToDevice, st));
   MCK(cudaMemcpyAsync(m->dtri, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice, st));
+  {
+    std::vector<double> cdf(nF);
+    double accum = 0.0;
+    for (int f = 0; f < nF; ++f) {
+      const float* pa = &m->hV[3 * (size_t)m->hF[3 * f]];
+      const float* pb = &m->hV[3 * (size_t)m->hF[3 * f + 1]];
+      const float* pc = &m->hV[3 * (size_t)m->hF[3 * f + 2]];
+      double e1[3] = {(double)pb[0] - pa[0], (double)pb[1] - pa[1], (double)pb[2] - pa[2]};
+      double e2[3] = {(double)pc[0] - pa[0], (double)pc[1] - pa[1], (double)pc[2] - pa[2]};
+      double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+      accum += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+      cdf[f] = accum;
+    }
+    MCK(cudaMemcpy(m->dcdf, cdf.data(), sizeof(double) * nF, cudaMemcpyHostToDevice));
+  }
   k_stage_normals<<<cdiv(nn, 256), 256, 0, st>>>(m->dV, nn, m->dF, m->doff, m->dfcs, m->dN);
   LAUNCHED(1);
   MCK(cudaGetLastError());
@@ -677,8 +694,6 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   if (p->kproj != kKProj) return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: kproj must be 5");
   if (p->mode < 0 || p->mode > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: mode must be 0, 1 or 2");
   if (p->profile < 0 || p->profile > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: profile");
-  if ((long)max_cells > (long)kScanTile * kScanThreads * kScanItems)
-    return fail(CVT_ERR_CAPACITY, "cvt_engine_create: max_cells above the scan limit (16,777,216)");
   cvt_engine* e = new cvt_engine();
   e->p = *p;
   e->K = p->k;
@@ -762,7 +777,7 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   int s = -1;
   for (int k = 0; k < e->max_seg; ++k) if (!e->active[k] && !e->seg_mesh[k]) { s = k; break; }
   if (s < 0) return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: no free segment slot");
-  GridGeom g = surface_grid(mesh->lo, mesh->hi, mesh->area, n, (double)(e->K + 1), e->p.cell_factor, 8L * n + 64);
+  GridGeom g = surface_grid(mesh->lo, mesh->hi, mesh->area, n, (double)(e->K + 1), e->p.cell_factor, 4L * n + 64);
   int cells = g.ncell + 1;
   int base = e->site_alloc.take(n);
   if (base < 0) return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: site capacity exhausted");
@@ -778,6 +793,8 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   sd.iter = 0;
   // twice the (K+1)-th squared distance of a uniform planar density n/area
   sd.kth_est = (float)(2.0 * (e->K + 1) * (double)mesh->area / (M_PI * (double)n));
+  sd.stop_motion2 = -1.f;
+  sd.stop_iters = 0;
   MeshDev md = mesh->dev();
   static const int kStreak1[6] = {5, 10, 15, 20, 25, 25};  // main.cu:22, 543-553
   static const int kStreak2[6] = {5, 10, 15, 20, 25, 10};  // main.cu:39, 554-563
@@ -977,7 +994,7 @@ extern "C" cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream) 
     }
     launches += nl;
     e->parity ^= 1;
-    for (int k = 0; k < e->max_seg; ++k) if (e->active[k]) e->host_iters[k]++;
+    for (int k = 0; k < e->max_seg; ++k) if (e->active[k] == 1) e->host_iters[k]++;
   }
   e->last_launches = launches;
   return CVT_OK;
@@ -997,7 +1014,7 @@ extern "C" cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms,
     if (s != CVT_OK) break;
     LAUNCHED(nl);
     e->parity ^= 1;
-    for (int k = 0; k < e->max_seg; ++k) if (e->active[k]) e->host_iters[k]++;
+    for (int k = 0; k < e->max_seg; ++k) if (e->active[k] == 1) e->host_iters[k]++;
     CK(cudaEventSynchronize(ev[4]));
     for (int k = 0; k < 4; ++k) {
       float t = 0.f;
@@ -1089,7 +1106,7 @@ extern "C" cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n) {
 
 // capacity for one mesh + site set
 static void engine_caps(const cvt_mesh* m, int n, const cvt_params_t* p, int* cells) {
-  GridGeom g = surface_grid(m->lo, m->hi, m->area, n, (double)(p->k + 1), p->cell_factor, 8L * n + 64);
+  GridGeom g = surface_grid(m->lo, m->hi, m->area, n, (double)(p->k + 1), p->cell_factor, 4L * n + 64);
   *cells = g.ncell + 1;
 }
 
@@ -1313,3 +1330,77 @@ extern "C" cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int s, cvt_eval_t* o
 // allocation-free site KNN (scratch in a fixed device array)
 // ---------------------------------------------------------------------------
 #include "cvt_noalloc.cu"
+
+// ---------------------------------------------------------------------------
+// stop rules, progress polling, device site sampler
+// ---------------------------------------------------------------------------
+extern "C" cvt_status_t cvt_engine_set_stop(cvt_engine_t e, int s, float max_motion, int max_iters) {
+  if (!e || s < 0 || s >= e->max_seg || !e->seg_mesh[s] || max_iters < 0)
+    return fail(CVT_ERR_INVALID, "cvt_engine_set_stop: bad arguments");
+  const float m2 = max_motion >= 0.f ? max_motion * max_motion : -1.f;
+  e->segs[s].stop_motion2 = m2;
+  e->segs[s].stop_iters = max_iters;
+  char* base = reinterpret_cast<char*>(e->d_segs + s);
+  CK(cudaMemcpy(base + offsetof(SegDev, stop_motion2), &m2, sizeof(float), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(base + offsetof(SegDev, stop_iters), &max_iters, sizeof(int), cudaMemcpyHostToDevice));
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_poll(cvt_engine_t e, int* iters, int* state, int cap, void* stream) {
+  if (!e || cap < 0 || (cap > 0 && (!iters || !state))) return fail(CVT_ERR_INVALID, "cvt_engine_poll: bad arguments");
+  cudaStream_t st = S_(stream);
+  std::vector<SegDev> sd(e->max_seg);
+  std::vector<int> act(e->max_seg);
+  CK(cudaMemcpyAsync(sd.data(), e->d_segs, sizeof(SegDev) * e->max_seg, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(act.data(), e->d_active, sizeof(int) * e->max_seg, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  for (int k = 0; k < e->max_seg; ++k) {
+    if (!e->seg_mesh[k]) continue;
+    e->active[k] = act[k];
+    e->host_iters[k] = sd[k].iter;
+  }
+  for (int k = 0; k < cap && k < e->max_seg; ++k) {
+    iters[k] = e->seg_mesh[k] ? e->host_iters[k] : 0;
+    state[k] = e->seg_mesh[k] ? e->active[k] : 0;
+  }
+  return CVT_OK;
+}
+
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ double unit53(unsigned long long h) { return (double)(h >> 11) * 0x1.0p-53; }
+
+// area-uniform points: face by the area CDF, then the square-root
+// barycentric map; a counter-based hash of (seed, i) gives the three uniforms
+__global__ void k_sample_sites(const double* __restrict__ cdf, int nF, const float* __restrict__ V,
+                               const int* __restrict__ F, int n, unsigned long long seed, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned long long h0 = mix64(seed * 0x100000001b3ull + (unsigned long long)i * 3ull);
+  unsigned long long h1 = mix64(h0 + 1ull), h2 = mix64(h0 + 2ull);
+  const double total = cdf[nF - 1];
+  const double u = unit53(h0) * total;
+  int lo = 0, hi = nF - 1;
+  while (lo < hi) {
+    int mid = (lo + hi) >> 1;
+    if (cdf[mid] > u) hi = mid; else lo = mid + 1;
+  }
+  const double r1 = __dsqrt_rn(unit53(h1)), r2 = unit53(h2);
+  const int ia = F[3 * lo], ib = F[3 * lo + 1], ic = F[3 * lo + 2];
+  for (int a = 0; a < 3; ++a) {
+    const double pa = V[3 * ia + a], pb = V[3 * ib + a], pc = V[3 * ic + a];
+    out[3 * (size_t)i + a] = (float)((1.0 - r1) * pa + r1 * (1.0 - r2) * pb + r1 * r2 * pc);
+  }
+}
+
+extern "C" cvt_status_t cvt_mesh_sample_sites(cvt_mesh_t m, int n, unsigned long long seed, float* out, void* stream) {
+  if (!m || n < 0 || (n > 0 && !out)) return fail(CVT_ERR_INVALID, "cvt_mesh_sample_sites: bad arguments");
+  if (n == 0) return CVT_OK;
+  k_sample_sites<<<cdiv(n, 256), 256, 0, S_(stream)>>>(m->dcdf, m->nF, m->dV, m->dF, n, seed, out);
+  CKLAUNCH();
+  return CVT_OK;
+}

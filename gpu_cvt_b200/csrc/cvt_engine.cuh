@@ -52,6 +52,8 @@ struct SegDev {
   int ex_quirk;
   int iter;       // iterations completed (device-side count)
   float kth_est;  // first-iteration estimate of the (K+1)-th squared distance
+  float stop_motion2;  // stop once an iteration's max squared motion <= this (< 0: never)
+  int stop_iters;      // stop after this many iterations (0: never)
   float thr2_tier[6];
   int need_tier[6];
 };
@@ -64,7 +66,7 @@ template <> struct PT<PROF_FP64> { using T = double; using Q = double; using PP 
 template <class T> struct EngineArgs {
   const SegDev* segs;
   const GridGeom* geom;
-  const int* active;
+  const int* active;      // 0 free, 1 iterating, 2 stopped by its stop rule
   const MeshDev* meshes;
   const int* site_seg;
   T* S[2];
@@ -523,17 +525,22 @@ __global__ void __launch_bounds__(64) k_cell_overflow(EngineArgs<typename PT<PRO
 }
 
 // iteration bookkeeping: advance active segments, clear their next stats
-// slot, reset the overflow list
-__global__ void k_seg_advance(SegDev* segs, const int* active, int nseg, int* stats, int* ovf) {
+// slot, apply each segment's stop rule (a stopped segment is no longer
+// gridded or iterated: active = 2), reset the overflow list
+__global__ void k_seg_advance(SegDev* segs, int* active, int nseg, int* stats, int* ovf) {
   for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
-    if (!active[s]) continue;
+    if (active[s] != 1) continue;
     int it = segs[s].iter;
     int* cur = stats + ((size_t)s * kStatsRing + (it % kStatsRing)) * kStatsWords;
     cur[5] = it;
+    const float d2 = __uint_as_float((unsigned)cur[4]);
     int nx = it + 1;
     int* sl = stats + ((size_t)s * kStatsRing + (nx % kStatsRing)) * kStatsWords;
     for (int w = 0; w < kStatsWords; ++w) sl[w] = 0;
     segs[s].iter = nx;
+    const float lim = segs[s].stop_motion2;
+    const int cap = segs[s].stop_iters;
+    if ((lim >= 0.f && d2 <= lim) || (cap > 0 && nx >= cap)) active[s] = 2;
   }
   if (threadIdx.x == 0) ovf[0] = 0;
 }

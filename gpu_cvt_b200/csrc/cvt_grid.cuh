@@ -434,7 +434,7 @@ __device__ __forceinline__ typename KeyOps<T>::Key warp_nearest(const GridGeom& 
 struct SegGrid {           // the minimal per-point view the build needs
   const GridGeom* geom;    // one geometry per segment
   const int* seg_of;       // segment of each point (nullptr: all segment 0)
-  const int* active;       // per-segment active flag (nullptr: all active)
+  const int* active;       // per-segment state, 1 = iterating (nullptr: all)
 };
 
 template <class T>
@@ -443,7 +443,7 @@ __global__ void k_grid_count(int n, const T* __restrict__ P, SegGrid sg, int* __
   int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= n) return;
   int s = sg.seg_of ? sg.seg_of[g] : 0;
-  if (s < 0 || (sg.active && !sg.active[s])) { cellrank[g] = make_int2(-1, 0); return; }
+  if (s < 0 || (sg.active && sg.active[s] != 1)) { cellrank[g] = make_int2(-1, 0); return; }
   GridGeom G = sg.geom[s];
   int cell = grid_cell(G, ld3(P, g));
   int rank = atomicAdd(cell_count + cell, 1);
@@ -463,8 +463,8 @@ __global__ void k_grid_scatter(int n, const T* __restrict__ P, const int2* __res
   sorted[cell_start[cr.x] + cr.y] = o;
 }
 
-// Exclusive scan of n ints (n <= 4096 * 4096): block sums, scan of the block
-// sums, then a block-local rescan with the block offset.  out[n] = total.
+// Exclusive scan of n ints: block sums, scan of the block sums, then a
+// block-local rescan with the block offset.  out[n] = total.
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -508,21 +508,26 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(int n, const int* 
   if (threadIdx.x == 0) part[blockIdx.x] = total;
 }
 
+// one block scans the block sums tile by tile, carrying the running total
 __global__ void __launch_bounds__(kScanThreads) k_scan_partials(int nb, int* __restrict__ part) {
   __shared__ int sw[33];
-  int base = threadIdx.x * kScanItems;
-  int v[kScanItems];
-  int s = 0;
+  int carry = 0;
+  for (int tile = 0; tile < nb; tile += kScanTile) {
+    int base = tile + threadIdx.x * kScanItems;
+    int v[kScanItems];
+    int s = 0;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) { v[k] = (base + k < nb) ? part[base + k] : 0; s += v[k]; }
-  int total;
-  int off = block_exclusive_scan(s, sw, total);
+    for (int k = 0; k < kScanItems; ++k) { v[k] = (base + k < nb) ? part[base + k] : 0; s += v[k]; }
+    int total;
+    int off = block_exclusive_scan(s, sw, total) + carry;
 #pragma unroll
-  for (int k = 0; k < kScanItems; ++k) {
-    if (base + k < nb) part[base + k] = off;
-    off += v[k];
+    for (int k = 0; k < kScanItems; ++k) {
+      if (base + k < nb) part[base + k] = off;
+      off += v[k];
+    }
+    carry += total;
   }
-  if (threadIdx.x == 0) part[nb] = total;
+  if (threadIdx.x == 0) part[nb] = carry;
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_apply(int n, const int* __restrict__ in, const int* __restrict__ part,

@@ -72,6 +72,12 @@ class Mesh:
              C.byref(out), stream)
         return float(out.value)
 
+    def sample_sites(self, out_tensor, seed: int, stream=None) -> None:
+        """Fill a (n,3) float32 CUDA tensor with area-uniform points (device
+        sampler, counter hash of (seed, i))."""
+        call("cvt_mesh_sample_sites", self.handle, int(out_tensor.shape[0]), C.c_ulonglong(seed & (2**64 - 1)),
+             C.c_void_p(out_tensor.data_ptr()), stream)
+
     def close(self):
         if getattr(self, "handle", None):
             _lib.load().cvt_mesh_destroy(self.handle)
@@ -177,6 +183,18 @@ class Engine:
         d["dH_rel"] = d["dH"] / d["diag"] if d["diag"] > 0 else float("nan")
         return d
 
+    def set_stop(self, seg: int, max_motion: float, max_iters: int) -> None:
+        """Device-side stop rule: stop once no site moves more than max_motion
+        in an iteration (< 0: never), or after max_iters iterations (0: never)."""
+        call("cvt_engine_set_stop", self.handle, int(seg), float(max_motion), int(max_iters))
+
+    def poll(self, cap: int, stream=None):
+        """(iters, state) per segment slot; state 0 free, 1 iterating, 2 stopped."""
+        it = (C.c_int * cap)()
+        st = (C.c_int * cap)()
+        call("cvt_engine_poll", self.handle, it, st, int(cap), stream)
+        return list(it), list(st)
+
     def last_launches(self) -> int:
         v = C.c_longlong()
         call("cvt_engine_last_launches", self.handle, C.byref(v))
@@ -205,7 +223,7 @@ def grid_cells(mesh: Mesh, n_sites: int, k: int, cell_factor: float = 1.1) -> in
     h = cell_factor * np.sqrt((k + 1) / (np.pi * dens))
     h = max(h, emax / 2048.0)
     pad = 1e-4 * emax
-    cap = 8 * n_sites + 64
+    cap = 4 * n_sites + 64
     for _ in range(200):
         dims = [max(1, int(np.ceil((e + 2 * pad) / h))) for e in ext]
         prod = dims[0] * dims[1] * dims[2]

@@ -189,6 +189,11 @@ cvt_status_t cvt_mesh_info(cvt_mesh_t m, cvt_mesh_info_t* info);
 cvt_status_t cvt_mesh_device_arrays(cvt_mesh_t m, const float** V, const int** F, const float** N,
                                     const int** vf_off, const int** vf_faces);
 cvt_status_t cvt_mesh_destroy(cvt_mesh_t m);
+/* n area-uniform points on the mesh (device out, n*3 floats): a face drawn by
+ * area, then the square-root barycentric map, three uniforms per point from
+ * a counter hash of (seed, i).  New (the reference starts from the vertices,
+ * main.cu:493). */
+cvt_status_t cvt_mesh_sample_sites(cvt_mesh_t m, int n, unsigned long long seed, float* out, void* stream);
 
 /* ======================================================================
  * Engine: many (mesh, site set) segments iterated together; each Lloyd
@@ -257,6 +262,16 @@ typedef struct {
   float diag;  /* bbox diagonal of the segment's mesh */
 } cvt_eval_t;
 cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int seg_id, cvt_eval_t* out, void* stream);
+/* Stop rule of a segment, applied on the device after every iteration: the
+ * segment stops iterating once an iteration moves no site by more than
+ * max_motion (absolute; < 0: no motion rule) or after max_iters iterations
+ * (0: no cap).  The serving loop's "until max site motion < 1e-4 of the bbox
+ * diagonal, capped at 150 iterations". */
+cvt_status_t cvt_engine_set_stop(cvt_engine_t e, int seg_id, float max_motion, int max_iters);
+/* Progress of the first `cap` segment slots, read from the device
+ * (synchronous): iters[s] = iterations done, state[s] = 0 free, 1 iterating,
+ * 2 stopped by its stop rule. */
+cvt_status_t cvt_engine_poll(cvt_engine_t e, int* iters, int* state, int cap, void* stream);
 /* Kernel launches issued by the last cvt_engine_run (graph nodes included). */
 cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n);
 

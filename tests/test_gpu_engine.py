@@ -178,3 +178,51 @@ def test_engine_evaluate_matches_oracle_pipeline(eng, oracle, small_torus):
     assert abs(ev["Qavg"] - q["Qavg"]) < 1e-5
     e.close()
     M.close()
+
+
+def test_stop_rule_and_poll(eng, c1):
+    m, S0 = c1
+    M = eng.Mesh(m.V, m.F)
+    e = eng.Engine(eng.params(k=20, mode=0), 2, 2 * len(S0), 2 * eng.grid_cells(M, len(S0), 20))
+    g1, g2 = e.add(M, S0), e.add(M, S0)
+    e.set_stop(g1, -1.0, 7)                  # iteration cap
+    e.set_stop(g2, 1e9, 0)                   # first iteration already "converged"
+    e.run(12)
+    iters, state = e.poll(2)
+    assert state == [2, 2] and iters == [7, 1]
+    ref = run_engine(eng, m, S0, 20, 0, 7)[0]
+    assert np.array_equal(e.sites(g1), ref)
+    e.close()
+
+
+def test_device_sampler_on_surface(eng):
+    m = mg.icosphere(4)
+    M = eng.Mesh(m.V, m.F)
+    t = torch.empty((20000, 3), dtype=torch.float32, device="cuda")
+    M.sample_sites(t, 123)
+    S = t.cpu().numpy()
+    r = np.linalg.norm(S, axis=1)
+    assert r.max() <= 1.0 + 1e-6 and r.min() > 0.99
+    assert abs(S.mean(0)).max() < 0.02          # area-uniform on a sphere: centred
+    t2 = torch.empty_like(t)
+    M.sample_sites(t2, 123)
+    assert torch.equal(t, t2)
+
+
+def test_serving_results_equal_alone(eng):
+    """Continuous batching: every request's final sites equal the same request
+    served alone, first come first served."""
+    from gpu_cvt_b200 import server
+    meshes, reqs = server.request_stream(n_requests=10, rate=2000.0, site_lo=1000, site_hi=20000, n_meshes=3, seed=9)
+    srv = server.RemeshServer(meshes, k=24, mode=1, profile="mixed", hbm_budget=64 << 20, max_segments=8,
+                              max_iters=40, chunk=3, keep_results=True)
+    stats = srv.run(reqs)
+    srv.close()
+    import copy
+    alone = [copy.copy(r) for r in reqs]
+    for r in alone:
+        r.result = None
+    server.serve_plain(meshes, alone, k=24, mode=1, profile="mixed", max_iters=40, chunk=3, keep_results=True)
+    for a, b in zip(reqs, alone):
+        assert a.iters == b.iters and np.array_equal(a.result, b.result), a.rid
+    assert stats["requests"] == 10 and stats["latency_p99_s"] >= stats["latency_p50_s"]
