@@ -638,6 +638,7 @@ struct cvt_engine {
   std::vector<cvt_mesh_t> seg_mesh;
   std::vector<int> seg_cells;  // cells reserved (spatial + NaN bucket)
   std::vector<int> host_iters;
+  std::vector<int> seg_p0;  // global parity when the segment was placed
   RangeAlloc site_alloc, cell_alloc;
   int parity = 0;
   // device
@@ -707,6 +708,7 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   e->seg_mesh.assign(max_segments, nullptr);
   e->seg_cells.assign(max_segments, 0);
   e->host_iters.assign(max_segments, 0);
+  e->seg_p0.assign(max_segments, 0);
   e->site_alloc.init(max_sites);
   e->cell_alloc.init(max_cells);
   const size_t tsz = e->f64 ? sizeof(double) : sizeof(float);
@@ -809,6 +811,7 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   e->seg_mesh[s] = mesh;
   e->seg_cells[s] = cells;
   e->host_iters[s] = 0;
+  e->seg_p0[s] = e->parity;
   const size_t tsz = e->f64 ? sizeof(double) : sizeof(float);
   CK(cudaMemcpyAsync(e->d_segs + s, &e->segs[s], sizeof(SegDev), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(e->d_geom + s, &e->geom[s], sizeof(GridGeom), cudaMemcpyHostToDevice, st));
@@ -1027,16 +1030,33 @@ extern "C" cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms,
   return s;
 }
 
+// Ping-pong buffer holding a segment's current sites.  A segment stopped by
+// its stop rule keeps its sites where its last iteration wrote them, so the
+// buffer follows from the parity at placement and the iterations done, read
+// from the device.  Synchronous.
+static cvt_status_t seg_sites_buffer(cvt_engine* e, int s, cudaStream_t st, int* par) {
+  int it = 0;
+  CK(cudaMemcpyAsync(&it, reinterpret_cast<char*>(e->d_segs + s) + offsetof(SegDev, iter), sizeof(int),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  e->host_iters[s] = it;
+  *par = (e->seg_p0[s] + it) & 1;
+  return CVT_OK;
+}
+
 extern "C" cvt_status_t cvt_engine_get_sites(cvt_engine_t e, int s, float* out, int out_on_device, void* stream) {
   if (!e || !out || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_get_sites: bad arguments");
   cudaStream_t st = S_(stream);
   const SegDev& sd = e->segs[s];
   size_t cnt = 3 * (size_t)sd.n_sites;
+  int par = 0;
+  cvt_status_t ps = seg_sites_buffer(e, s, st, &par);
+  if (ps != CVT_OK) return ps;
   if (!e->f64) {
-    const float* src = (const float*)e->d_S[e->parity] + 3 * (size_t)sd.site_base;
+    const float* src = (const float*)e->d_S[par] + 3 * (size_t)sd.site_base;
     CK(cudaMemcpyAsync(out, src, sizeof(float) * cnt, out_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
   } else {
-    const double* src = (const double*)e->d_S[e->parity] + 3 * (size_t)sd.site_base;
+    const double* src = (const double*)e->d_S[par] + 3 * (size_t)sd.site_base;
     Scratch sc(st);
     float* tmp = out;
     if (!out_on_device) CK(sc.get(&tmp, cnt));
@@ -1053,7 +1073,10 @@ extern "C" cvt_status_t cvt_engine_get_sites_f64(cvt_engine_t e, int s, double* 
     return fail(CVT_ERR_INVALID, "cvt_engine_get_sites_f64: bad arguments (FP64 engines only)");
   cudaStream_t st = S_(stream);
   const SegDev& sd = e->segs[s];
-  const double* src = (const double*)e->d_S[e->parity] + 3 * (size_t)sd.site_base;
+  int par = 0;
+  cvt_status_t ps = seg_sites_buffer(e, s, st, &par);
+  if (ps != CVT_OK) return ps;
+  const double* src = (const double*)e->d_S[par] + 3 * (size_t)sd.site_base;
   CK(cudaMemcpyAsync(out, src, sizeof(double) * 3 * (size_t)sd.n_sites, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   return CVT_OK;
@@ -1270,16 +1293,19 @@ extern "C" cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int s, cvt_eval_t* o
   const SegDev& sd = e->segs[s];
   const int n = sd.n_sites;
   const cvt_mesh* m = e->seg_mesh[s];
+  int par = 0;
+  cvt_status_t ps = seg_sites_buffer(e, s, st, &par);
+  if (ps != CVT_OK) return ps;
   Scratch sc(st);
   float *Sf, *U, *V;
   CK(sc.get(&Sf, 3 * (size_t)n));
   CK(sc.get(&U, 3 * (size_t)n));
   CK(sc.get(&V, 3 * (size_t)n));
   if (e->f64)
-    k_eval_frames<double><<<cdiv(n, 128), 128, 0, st>>>((const double*)e->d_S[e->parity], sd.site_base, n, e->d_frozen,
+    k_eval_frames<double><<<cdiv(n, 128), 128, 0, st>>>((const double*)e->d_S[par], sd.site_base, n, e->d_frozen,
                                                          e->d_knnv, sd.mode, m->dev(), Sf, U, V);
   else
-    k_eval_frames<float><<<cdiv(n, 128), 128, 0, st>>>((const float*)e->d_S[e->parity], sd.site_base, n, e->d_frozen,
+    k_eval_frames<float><<<cdiv(n, 128), 128, 0, st>>>((const float*)e->d_S[par], sd.site_base, n, e->d_frozen,
                                                         e->d_knnv, sd.mode, m->dev(), Sf, U, V);
   CKLAUNCH();
   // R2 = longest bbox edge of the current sites (main.cu:899-909)

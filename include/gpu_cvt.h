@@ -235,7 +235,8 @@ cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, const float
 cvt_status_t cvt_engine_remove_segment(cvt_engine_t e, int seg_id);
 /* Run `iters` Lloyd iterations of every active segment (asynchronous). */
 cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream);
-/* Copy a segment's current sites out (n*3 floats; FP64 engines convert). */
+/* Copy a segment's current sites out (n*3 floats; FP64 engines convert).
+ * Synchronous (it reads the segment's iteration count from the device). */
 cvt_status_t cvt_engine_get_sites(cvt_engine_t e, int seg_id, float* out, int out_on_device, void* stream);
 /* FP64 engines: the double-precision sites (n*3 doubles, host). */
 cvt_status_t cvt_engine_get_sites_f64(cvt_engine_t e, int seg_id, double* out, void* stream);
