@@ -84,6 +84,7 @@ _SIGS = {
     "cvt_engine_poll": [vp, vp, vp, i32, vp],
     "cvt_mesh_sample_sites": [vp, i32, u64, vp, vp],
     "cvt_engine_evaluate": [vp, i32, vp, vp],
+    "cvt_engine_faces": [vp, i32, vp, i32, vp, vp, vp],
     "cvt_extract_faces": [vp, vp, vp, vp, i32, i32, f32, vp, i32, vp, vp],
     "cvt_quality": [vp, vp, i32, vp, vp],
     "cvt_remesh": [vp, i32, vp, i32, vp, i32, vp, i32, vp, vp],

@@ -1287,7 +1287,22 @@ __global__ void k_eval_frames(const T* __restrict__ S, int base, int n, const ui
   st3(Vv, i, fr.v);
 }
 
+static cvt_status_t engine_eval_impl(cvt_engine_t e, int s, cvt_eval_t* out, int* faces_host, int max_faces_host,
+                                     int* n_faces_host, void* stream);
+
 extern "C" cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int s, cvt_eval_t* out, void* stream) {
+  return engine_eval_impl(e, s, out, nullptr, 0, nullptr, stream);
+}
+
+extern "C" cvt_status_t cvt_engine_faces(cvt_engine_t e, int s, int* faces, int max_faces, int* n_faces, cvt_eval_t* out,
+                                         void* stream) {
+  if (!n_faces || max_faces < 0 || (max_faces > 0 && !faces)) return fail(CVT_ERR_INVALID, "cvt_engine_faces: bad arguments");
+  cvt_eval_t tmp;
+  return engine_eval_impl(e, s, out ? out : &tmp, faces, max_faces, n_faces, stream);
+}
+
+static cvt_status_t engine_eval_impl(cvt_engine_t e, int s, cvt_eval_t* out, int* faces_host, int max_faces_host,
+                                     int* n_faces_host, void* stream) {
   if (!e || !out || s < 0 || s >= e->max_seg || !e->seg_mesh[s]) return fail(CVT_ERR_INVALID, "cvt_engine_evaluate: bad segment");
   cudaStream_t st = S_(stream);
   const SegDev& sd = e->segs[s];
@@ -1344,6 +1359,14 @@ extern "C" cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int s, cvt_eval_t* o
   float dH = 0.f;
   r = cvt_hausdorff_to_mesh(const_cast<cvt_mesh*>(m), Sf, n, Fc, nf, &dH, stream);
   if (r != CVT_OK) return r;
+  if (n_faces_host) {
+    *n_faces_host = nf;
+    if (nf > max_faces_host) return fail(CVT_ERR_CAPACITY, "cvt_engine_faces: more faces than max_faces (count in *n_faces)");
+    if (nf > 0) {
+      CK(cudaMemcpyAsync(faces_host, Fc, sizeof(int) * 3 * (size_t)nf, cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+    }
+  }
   out->dH = dH;
   out->Qmin = q[0]; out->Qavg = q[1]; out->theta_min = q[2]; out->theta_min_avg = q[3];
   out->theta_lt_30_pct = q[4]; out->theta_gt_90_pct = q[5];

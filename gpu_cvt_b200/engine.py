@@ -195,6 +195,24 @@ class Engine:
         call("cvt_engine_poll", self.handle, it, st, int(cap), stream)
         return list(it), list(st)
 
+    def faces(self, seg: int, stream=None):
+        """(faces int32 (nF,3), evaluation dict) of the current sites."""
+        n = self.sizes[seg]
+        cap = 4 * n + 64
+        while True:
+            F = np.zeros((cap, 3), np.int32)
+            nf = C.c_int()
+            o = EvalOut()
+            st = _lib.load().cvt_engine_faces(self.handle, int(seg), _ptr(F), cap, C.byref(nf), C.byref(o), stream)
+            if st == 5 and nf.value > cap:
+                cap = nf.value
+                continue
+            if st != 0:
+                raise _lib.CvtError("cvt_engine_faces", st, _lib.last_error())
+            d = {f: getattr(o, f) for f, _ in EvalOut._fields_}
+            d["dH_rel"] = d["dH"] / d["diag"] if d["diag"] > 0 else float("nan")
+            return F[:nf.value].copy(), d
+
     def last_launches(self) -> int:
         v = C.c_longlong()
         call("cvt_engine_last_launches", self.handle, C.byref(v))

@@ -263,6 +263,11 @@ typedef struct {
   float diag;  /* bbox diagonal of the segment's mesh */
 } cvt_eval_t;
 cvt_status_t cvt_engine_evaluate(cvt_engine_t e, int seg_id, cvt_eval_t* out, void* stream);
+/* The same evaluation, also copying the dual triangles (host, max_faces*3
+ * ints; *n_faces gets the count, also on CVT_ERR_CAPACITY) -- the mesh that
+ * main.cu:982 writes as iter_%03d.obj.  `out` may be NULL. */
+cvt_status_t cvt_engine_faces(cvt_engine_t e, int seg_id, int* faces, int max_faces, int* n_faces, cvt_eval_t* out,
+                              void* stream);
 /* Stop rule of a segment, applied on the device after every iteration: the
  * segment stops iterating once an iteration moves no site by more than
  * max_motion (absolute; < 0: no motion rule) or after max_iters iterations

@@ -226,3 +226,24 @@ def test_serving_results_equal_alone(eng):
     for a, b in zip(reqs, alone):
         assert a.iters == b.iters and np.array_equal(a.result, b.result), a.rid
     assert stats["requests"] == 10 and stats["latency_p99_s"] >= stats["latency_p50_s"]
+
+
+def test_cli_driver_contract(tmp_path):
+    """gpu_cvt <mesh.obj> [mode] [iters]: the reference driver's outputs."""
+    from gpu_cvt_b200 import cli, meshgen as mg
+    m = mg.icosphere(4)
+    obj = tmp_path / "ball.obj"
+    mg.save_obj(str(obj), m.V, m.F)
+    assert cli.main([str(obj), "1", "12", "--k", "24", "--out-root", str(tmp_path)]) == 0
+    d = tmp_path / "experiments" / "output" / "freeze" / "ball"
+    rows = (d / "eval_iters.csv").read_text().strip().split("\n")
+    assert rows[0] == cli.EVAL_HEADER and len(rows) == 3          # iterations 0 and 10
+    assert len(rows[1].split(",")) == 28
+    for it in (0, 10):
+        V = mg.load_obj(str(d / f"iter_{it:03d}.obj"))
+        assert V.nV == m.nV and V.nF > m.nV
+        assert len((d / f"iter_{it:03d}_frozen.txt").read_text().split()) == m.nV
+    runs = (tmp_path / "experiments" / "runs.csv").read_text().strip().split("\n")
+    assert runs[0] == cli.RUNS_HEADER and runs[1].startswith("ball,freeze,")
+    dH = float(rows[2].split(",")[9])
+    assert 0 < dH < 0.05
