@@ -401,6 +401,23 @@ def run_serve(args):
     return 0
 
 
+def run_precision(args):
+    """1M sites on the jittered rounded box, K=32, 200
+    iterations in the FP32, mixed and FP64 profiles."""
+    import torch
+    from gpu_cvt_b200 import workloads
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    r = workloads.precision_study(iters=200, k=32, mode=1)
+    line = {"metric": METRIC, "value": r["mixed"]["sites_iters_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1,
+            "warmup": 1, "ms_per_step": r["mixed"]["ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "superellipsoid_1m", "mesh": r["mesh"], "sites": r["sites"], "k": 32,
+                       "iters": 200, "mode": 1, "profile": "mixed"},
+            "profiles": {p: r[p] for p in ("ref", "mixed", "fp64")}, "generation_s": r["generation_s"]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -410,7 +427,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
-    ap.add_argument("--workload", choices=["torus_100k", "batched", "serve"], default="torus_100k")
+    ap.add_argument("--workload", choices=["torus_100k", "batched", "serve", "superellipsoid_1m"],
+                    default="torus_100k")
     ap.add_argument("--meshes", type=int, default=256)
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--hbm-gb", type=int, default=4)
@@ -421,6 +439,8 @@ def main():
         return run_batched(args)
     if args.workload == "serve":
         return run_serve(args)
+    if args.workload == "superellipsoid_1m":
+        return run_precision(args)
     return run_ours(args)
 
 

@@ -114,3 +114,48 @@ def batched_vs_plain(n_meshes=256, iters=100, k=24, mode=0, profile="ref", seed=
             "batched_s": tb, "plain_loop_s": tp,
             "batched_sites_iters_per_s": n_tot * iters / tb, "plain_sites_iters_per_s": n_tot * iters / tp,
             "speedup": tp / tb, "identical_results": same, "mesh_generation_s": gen_s}
+
+
+def precision_study(iters=200, k=32, mode=1, n_sites=1_000_000, tris=2_000_000, seed=2):
+    """Rounded box |x|^8+|y|^8+|z|^8=1 (~2M triangles, 1% jittered by 1e-3),
+    1M area-uniform sites, K=32: the same run in the ref (FP32), mixed and
+    fp64 profiles; Hausdorff of each result and per-site drift against FP64."""
+    import torch
+    t0 = time.perf_counter()
+    m = mg.superellipsoid(8.0, tris, 0.01, 1e-3, seed=seed)
+    S0 = mg.sample_sites(m.V, m.F, n_sites, seed=seed)
+    gen_s = time.perf_counter() - t0
+    M = E.Mesh(m.V, m.F)
+    cells = E.grid_cells(M, n_sites, k)
+    out = {"mesh": f"superellipsoid p=8, {m.nF} triangles, 1% jittered by 1e-3 (seed {seed})",
+           "sites": n_sites, "k": k, "mode": mode, "iters": iters, "generation_s": gen_s}
+    sites = {}
+    for prof in ("ref", "mixed", "fp64"):
+        eng = E.Engine(E.params(k=k, mode=mode, profile=prof), 1, n_sites, cells)
+        g = eng.add(M, S0)
+        eng.run(1)                      # graph capture, first iteration
+        _sync()
+        eng.remove(g)
+        g = eng.add(M, S0)
+        st = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        eng.run(iters, C_stream(st))
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        ev = eng.evaluate(g)
+        sites[prof] = eng.sites_f64(g) if prof == "fp64" else eng.sites(g).astype(np.float64)
+        nfz = int(eng.state(g)["frozen"].sum())
+        eng.close()
+        out[prof] = {"ms": ms, "sites_iters_per_s": n_sites * iters / (ms / 1e3), "dH": ev["dH"],
+                     "dH_rel": ev["dH_rel"], "n_faces": ev["n_faces"], "Qavg": ev["Qavg"], "Qmin": ev["Qmin"],
+                     "frozen_end": nfz, "nan_sites": int(np.isnan(sites[prof]).any(axis=1).sum())}
+    for prof in ("ref", "mixed"):
+        d = np.linalg.norm(sites[prof] - sites["fp64"], axis=1) / M.diag
+        d = d[np.isfinite(d)]
+        out[prof]["drift_vs_fp64"] = {"max": float(d.max()), "mean": float(d.mean()),
+                                      "p99": float(np.percentile(d, 99))}
+        out[prof]["dH_minus_fp64_rel"] = (out[prof]["dH"] - out["fp64"]["dH"]) / M.diag
+    M.close()
+    return out
