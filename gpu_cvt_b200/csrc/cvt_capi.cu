@@ -335,10 +335,12 @@ struct cvt_mesh {
   GridGeom vg{};
   int* dvcell_start = nullptr;
   Pt4<float>* dvsorted = nullptr;
-  BVHNode* dnodes = nullptr;
+  BVHNode* dnodes = nullptr;  // built on first use (Hausdorff)
   int* dtri = nullptr;
   int nnodes = 0;
+  void* arena = nullptr;      // V, F, CSR, normals, vertex grid: one allocation
   size_t bytes = 0;
+  std::mutex lazy_mu;         // guards the first-use builds (BVH, area CDF)
   std::vector<float> hV;
   std::vector<int> hF;
   MeshDev dev() const {
@@ -351,16 +353,83 @@ struct cvt_mesh {
   }
 };
 
+// Many device arrays carved out of one cudaMalloc (256-byte aligned slices):
+// one allocator call and one free per object instead of one per array.
+struct Arena {
+  std::vector<std::pair<void**, size_t>> slots;
+  size_t size = 0;
+  template <class X> void add(X** p, size_t count) {
+    slots.push_back({reinterpret_cast<void**>(p), size});
+    size += (std::max<size_t>(count * sizeof(X), 16) + 255) & ~size_t(255);
+  }
+  cudaError_t commit(void** base) {
+    cudaError_t e = cudaMalloc(base, std::max<size_t>(size, 256));
+    if (e != cudaSuccess) { *base = nullptr; return e; }
+    for (auto& s : slots) *s.first = static_cast<char*>(*base) + s.second;
+    return cudaSuccess;
+  }
+};
+
 static void mesh_free(cvt_mesh* m) {
   if (!m) return;
-  cudaFree(m->dV); cudaFree(m->dF); cudaFree(m->doff); cudaFree(m->dfcs); cudaFree(m->dN); cudaFree(m->dcdf);
-  cudaFree(m->dvcell_start); cudaFree(m->dvsorted); cudaFree(m->dnodes); cudaFree(m->dtri);
+  cudaFree(m->arena); cudaFree(m->dcdf); cudaFree(m->dnodes); cudaFree(m->dtri);
   delete m;
 }
 
-template <class X> static cudaError_t dmalloc(X** p, size_t count, size_t* acc) {
-  *acc += std::max<size_t>(count * sizeof(X), 16);
-  return cudaMalloc((void**)p, std::max<size_t>(count * sizeof(X), 16));
+// BVH of the mesh (evaluate.cuh:114-201), built on the host and uploaded the
+// first time a Hausdorff distance needs it.
+static cvt_status_t mesh_ensure_bvh(cvt_mesh* m) {
+  std::lock_guard<std::mutex> lk(m->lazy_mu);
+  if (m->dnodes) return CVT_OK;
+  std::vector<BVHNode> nodes;
+  std::vector<int> tri;
+  build_bvh_host(m->hV.data(), m->hF.data(), m->nF, 8, nodes, tri);
+  BVHNode* dn = nullptr;
+  int* dt = nullptr;
+  cudaError_t e = cudaMalloc(&dn, sizeof(BVHNode) * std::max<size_t>(nodes.size(), 1));
+  if (e == cudaSuccess) e = cudaMalloc(&dt, sizeof(int) * std::max<size_t>(tri.size(), 1));
+  if (e == cudaSuccess) e = cudaMemcpy(dn, nodes.data(), sizeof(BVHNode) * nodes.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dt, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(dn); cudaFree(dt);
+    return fail(e == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,
+                std::string("mesh BVH: ") + cudaGetErrorString(e));
+  }
+  m->nnodes = (int)nodes.size();
+  m->dtri = dt;
+  m->bytes += sizeof(BVHNode) * nodes.size() + sizeof(int) * tri.size();
+  m->dnodes = dn;
+  return CVT_OK;
+}
+
+// Face-area prefix sums (FP64) for the site sampler, built on first use.
+static cvt_status_t mesh_ensure_cdf(cvt_mesh* m) {
+  std::lock_guard<std::mutex> lk(m->lazy_mu);
+  if (m->dcdf) return CVT_OK;
+  const int nF = m->nF;
+  std::vector<double> cdf(nF);
+  double accum = 0.0;
+  for (int f = 0; f < nF; ++f) {
+    const float* pa = &m->hV[3 * (size_t)m->hF[3 * f]];
+    const float* pb = &m->hV[3 * (size_t)m->hF[3 * f + 1]];
+    const float* pc = &m->hV[3 * (size_t)m->hF[3 * f + 2]];
+    double e1[3] = {(double)pb[0] - pa[0], (double)pb[1] - pa[1], (double)pb[2] - pa[2]};
+    double e2[3] = {(double)pc[0] - pa[0], (double)pc[1] - pa[1], (double)pc[2] - pa[2]};
+    double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
+    accum += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
+    cdf[f] = accum;
+  }
+  double* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(double) * std::max(nF, 1));
+  if (e == cudaSuccess) e = cudaMemcpy(d, cdf.data(), sizeof(double) * nF, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return fail(e == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,
+                std::string("mesh area CDF: ") + cudaGetErrorString(e));
+  }
+  m->bytes += sizeof(double) * nF;
+  m->dcdf = d;
+  return CVT_OK;
 }
 
 // Uniform grid for surface points: cell edge = factor * radius expected to
@@ -450,13 +519,8 @@ extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, in
     for (int f = 0; f < nF; ++f)
       for (int k = 0; k < 3; ++k) fcs[cur[m->hF[3 * f + k]]++] = f;
   }
-  std::vector<BVHNode> nodes;
-  std::vector<int> tri;
-  build_bvh_host(m->hV.data(), m->hF.data(), nF, 8, nodes, tri);
-  m->nnodes = (int)nodes.size();
   m->vg = surface_grid(m->lo, m->hi, area, nn, 6.0, g_vcell_factor, 4L * nn + 64);
   cudaError_t e = cudaSuccess;
-  size_t acc = 0;
 #define MCK(x)                                                                              \
   do {                                                                                      \
     e = (x);                                                                                \
@@ -466,39 +530,21 @@ extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, in
                   std::string("cvt_mesh_create: ") + cudaGetErrorString(e));                \
     }                                                                                       \
   } while (0)
-  MCK(dmalloc(&m->dV, 3 * (size_t)nn, &acc));
-  MCK(dmalloc(&m->dF, 3 * (size_t)nF, &acc));
-  MCK(dmalloc(&m->doff, (size_t)nn + 1, &acc));
-  MCK(dmalloc(&m->dfcs, 3 * (size_t)nF, &acc));
-  MCK(dmalloc(&m->dN, 3 * (size_t)nn, &acc));
-  MCK(dmalloc(&m->dvcell_start, (size_t)m->vg.ncell + 2, &acc));
-  MCK(dmalloc(&m->dvsorted, (size_t)nn, &acc));
-  MCK(dmalloc(&m->dnodes, nodes.size(), &acc));
-  MCK(dmalloc(&m->dtri, tri.size(), &acc));
-  MCK(dmalloc(&m->dcdf, (size_t)nF, &acc));
-  m->bytes = acc;
+  Arena ar;
+  ar.add(&m->dV, 3 * (size_t)nn);
+  ar.add(&m->dF, 3 * (size_t)nF);
+  ar.add(&m->doff, (size_t)nn + 1);
+  ar.add(&m->dfcs, 3 * (size_t)nF);
+  ar.add(&m->dN, 3 * (size_t)nn);
+  ar.add(&m->dvcell_start, (size_t)m->vg.ncell + 2);
+  ar.add(&m->dvsorted, (size_t)nn);
+  MCK(ar.commit(&m->arena));
+  m->bytes = ar.size;
   cudaStream_t st = 0;
   MCK(cudaMemcpyAsync(m->dV, m->hV.data(), sizeof(float) * 3 * nn, cudaMemcpyHostToDevice, st));
   MCK(cudaMemcpyAsync(m->dF, m->hF.data(), sizeof(int) * 3 * (size_t)nF, cudaMemcpyHostToDevice, st));
   MCK(cudaMemcpyAsync(m->doff, off.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice, st));
   MCK(cudaMemcpyAsync(m->dfcs, fcs.data(), sizeof(int) * 3 * (size_t)nF, cudaMemcpyHostToDevice, st));
-  MCK(cudaMemcpyAsync(m->dnodes, nodes.data(), sizeof(BVHNode) * nodes.size(), cudaMemcpyHostToDevice, st));
-  MCK(cudaMemcpyAsync(m->dtri, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice, st));
-  {
-    std::vector<double> cdf(nF);
-    double accum = 0.0;
-    for (int f = 0; f < nF; ++f) {
-      const float* pa = &m->hV[3 * (size_t)m->hF[3 * f]];
-      const float* pb = &m->hV[3 * (size_t)m->hF[3 * f + 1]];
-      const float* pc = &m->hV[3 * (size_t)m->hF[3 * f + 2]];
-      double e1[3] = {(double)pb[0] - pa[0], (double)pb[1] - pa[1], (double)pb[2] - pa[2]};
-      double e2[3] = {(double)pc[0] - pa[0], (double)pc[1] - pa[1], (double)pc[2] - pa[2]};
-      double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
-      accum += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
-      cdf[f] = accum;
-    }
-    MCK(cudaMemcpy(m->dcdf, cdf.data(), sizeof(double) * nF, cudaMemcpyHostToDevice));
-  }
   k_stage_normals<<<cdiv(nn, 256), 256, 0, st>>>(m->dV, nn, m->dF, m->doff, m->dfcs, m->dN);
   LAUNCHED(1);
   MCK(cudaGetLastError());
@@ -550,6 +596,8 @@ extern "C" cvt_status_t cvt_hausdorff_to_mesh(cvt_mesh_t ref, const float* Vc, i
   cudaStream_t st = S_(stream);
   long nP = (long)nVc + 4L * nFc;
   if (nP == 0) { *out = 0.f; return CVT_OK; }
+  cvt_status_t ls = mesh_ensure_bvh(ref);
+  if (ls != CVT_OK) return ls;
   Scratch sc(st);
   unsigned* bits;
   int* ovf;
@@ -641,7 +689,9 @@ struct cvt_engine {
   std::vector<int> seg_p0;  // global parity when the segment was placed
   RangeAlloc site_alloc, cell_alloc;
   int parity = 0;
-  // device
+  // device: every array below is a slice of one allocation
+  void* arena = nullptr;
+  size_t bytes = 0;
   SegDev* d_segs = nullptr;
   GridGeom* d_geom = nullptr;
   int* d_active = nullptr;
@@ -673,15 +723,9 @@ struct cvt_engine {
 
 static void engine_free(cvt_engine* e) {
   if (!e) return;
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < 2; ++k)
     if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
-    cudaFree(e->d_S[k]);
-  }
-  cudaFree(e->d_knn); cudaFree(e->d_same); cudaFree(e->d_kth); cudaFree(e->d_act); cudaFree(e->d_act_count);
-  cudaFree(e->d_segs); cudaFree(e->d_geom); cudaFree(e->d_active); cudaFree(e->d_meshes); cudaFree(e->d_site_seg);
-  cudaFree(e->d_knnv); cudaFree(e->d_nnv); cudaFree(e->d_frozen); cudaFree(e->d_streak); cudaFree(e->d_tier);
-  cudaFree(e->d_cellrank); cudaFree(e->d_sorted); cudaFree(e->d_cell_count); cudaFree(e->d_cell_start);
-  cudaFree(e->d_part); cudaFree(e->d_stats); cudaFree(e->d_ovf);
+  cudaFree(e->arena);
   delete e;
 }
 
@@ -724,38 +768,33 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
     }                                                                                        \
   } while (0)
   const size_t ns = (size_t)max_sites;
-  ECK(cudaMalloc(&e->d_segs, sizeof(SegDev) * max_segments));
-  ECK(cudaMalloc(&e->d_geom, sizeof(GridGeom) * max_segments));
-  ECK(cudaMalloc(&e->d_active, sizeof(int) * max_segments));
-  ECK(cudaMalloc(&e->d_meshes, sizeof(MeshDev) * max_segments));
-  ECK(cudaMalloc(&e->d_site_seg, sizeof(int) * ns));
-  for (int k = 0; k < 2; ++k) ECK(cudaMalloc(&e->d_S[k], tsz * 3 * ns));
-  ECK(cudaMalloc(&e->d_knn, sizeof(uint32_t) * e->K * ns));
-  ECK(cudaMalloc(&e->d_same, ns));
-  ECK(cudaMalloc(&e->d_kth, sizeof(float) * ns));
-  ECK(cudaMalloc(&e->d_act, sizeof(int) * ns));
-  ECK(cudaMalloc(&e->d_act_count, sizeof(int)));
-  ECK(cudaMalloc(&e->d_knnv, sizeof(int) * kKProj * ns));
-  ECK(cudaMalloc(&e->d_nnv, sizeof(int) * ns));
-  ECK(cudaMalloc(&e->d_frozen, ns));
-  ECK(cudaMalloc(&e->d_streak, ns));
-  ECK(cudaMalloc(&e->d_tier, ns));
-  ECK(cudaMalloc(&e->d_cellrank, sizeof(int2) * ns));
-  ECK(cudaMalloc(&e->d_sorted, psz * ns));
-  ECK(cudaMalloc(&e->d_cell_count, sizeof(int) * (size_t)max_cells));
-  ECK(cudaMalloc(&e->d_cell_start, sizeof(int) * ((size_t)max_cells + 1)));
-  ECK(cudaMalloc(&e->d_part, sizeof(int) * ((size_t)scan_blocks(max_cells) + 2)));
-  ECK(cudaMalloc(&e->d_stats, sizeof(int) * (size_t)max_segments * kStatsRing * kStatsWords));
-  ECK(cudaMalloc(&e->d_ovf, sizeof(int) * (ns + 1)));
-  ECK(cudaMemset(e->d_active, 0, sizeof(int) * max_segments));
-  ECK(cudaMemset(e->d_segs, 0, sizeof(SegDev) * max_segments));
-  ECK(cudaMemset(e->d_geom, 0, sizeof(GridGeom) * max_segments));
-  ECK(cudaMemset(e->d_meshes, 0, sizeof(MeshDev) * max_segments));
-  ECK(cudaMemset(e->d_stats, 0, sizeof(int) * (size_t)max_segments * kStatsRing * kStatsWords));
-  ECK(cudaMemset(e->d_ovf, 0, sizeof(int)));
-  for (int k = 0; k < 2; ++k) ECK(cudaMemset(e->d_S[k], 0, tsz * 3 * ns));
-  ECK(cudaMemset(e->d_knn, 0, sizeof(uint32_t) * e->K * ns));
-  ECK(cudaMemset(e->d_same, 0, ns));
+  Arena ar;
+  ar.add(&e->d_segs, max_segments);
+  ar.add(&e->d_geom, max_segments);
+  ar.add(&e->d_active, max_segments);
+  ar.add(&e->d_meshes, max_segments);
+  ar.add(&e->d_site_seg, ns);
+  for (int k = 0; k < 2; ++k) ar.add(reinterpret_cast<char**>(&e->d_S[k]), tsz * 3 * ns);
+  ar.add(&e->d_knn, (size_t)e->K * ns);
+  ar.add(&e->d_same, ns);
+  ar.add(&e->d_kth, ns);
+  ar.add(&e->d_act, ns);
+  ar.add(&e->d_act_count, 1);
+  ar.add(&e->d_knnv, (size_t)kKProj * ns);
+  ar.add(&e->d_nnv, ns);
+  ar.add(&e->d_frozen, ns);
+  ar.add(&e->d_streak, ns);
+  ar.add(&e->d_tier, ns);
+  ar.add(&e->d_cellrank, ns);
+  ar.add(reinterpret_cast<char**>(&e->d_sorted), psz * ns);
+  ar.add(&e->d_cell_count, (size_t)max_cells);
+  ar.add(&e->d_cell_start, (size_t)max_cells + 1);
+  ar.add(&e->d_part, (size_t)scan_blocks(max_cells) + 2);
+  ar.add(&e->d_stats, (size_t)max_segments * kStatsRing * kStatsWords);
+  ar.add(&e->d_ovf, ns + 1);
+  ECK(ar.commit(&e->arena));
+  e->bytes = ar.size;
+  ECK(cudaMemset(e->arena, 0, ar.size));
   k_fill_int<<<cdiv((long)ns, 256), 256>>>(e->d_site_seg, (int)ns, -1);
   LAUNCHED(1);
   ECK(cudaGetLastError());
@@ -1150,13 +1189,15 @@ extern "C" cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF,
   if (s == CVT_OK) s = cvt_engine_run(e, iters, nullptr);
   if (s == CVT_OK) s = cvt_engine_get_sites(e, seg, sites_out, 0, nullptr);
   if (s == CVT_OK && counts) {
-    int lo = std::max(0, iters - kStatsRing);
-    for (int it = 0; it < iters && s == CVT_OK; ++it) {
-      if (it < lo) { for (int a = 0; a < 4; ++a) counts[4 * it + a] = -1; continue; }
-      cvt_iter_stats_t t;
-      s = cvt_engine_get_stats(e, seg, it, &t, nullptr);
-      counts[4 * it + 0] = t.same; counts[4 * it + 1] = t.low; counts[4 * it + 2] = t.both; counts[4 * it + 3] = t.newly_frozen;
-    }
+    // the segment's whole statistics ring in one copy
+    std::vector<int> ring((size_t)kStatsRing * kStatsWords);
+    cudaError_t ce = cudaMemcpy(ring.data(), e->d_stats + (size_t)seg * kStatsRing * kStatsWords,
+                                sizeof(int) * ring.size(), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) s = fail(CVT_ERR_CUDA, std::string("cvt_remesh: ") + cudaGetErrorString(ce));
+    const int lo = std::max(0, iters - kStatsRing);
+    for (int it = 0; it < iters && s == CVT_OK; ++it)
+      for (int a = 0; a < 4; ++a)
+        counts[4 * it + a] = it < lo ? -1 : ring[(size_t)(it % kStatsRing) * kStatsWords + a];
   }
   cvt_engine_destroy(e);
   cvt_mesh_destroy(m);
@@ -1449,6 +1490,8 @@ __global__ void k_sample_sites(const double* __restrict__ cdf, int nF, const flo
 extern "C" cvt_status_t cvt_mesh_sample_sites(cvt_mesh_t m, int n, unsigned long long seed, float* out, void* stream) {
   if (!m || n < 0 || (n > 0 && !out)) return fail(CVT_ERR_INVALID, "cvt_mesh_sample_sites: bad arguments");
   if (n == 0) return CVT_OK;
+  cvt_status_t ls = mesh_ensure_cdf(m);
+  if (ls != CVT_OK) return ls;
   k_sample_sites<<<cdiv(n, 256), 256, 0, S_(stream)>>>(m->dcdf, m->nF, m->dV, m->dF, n, seed, out);
   CKLAUNCH();
   return CVT_OK;

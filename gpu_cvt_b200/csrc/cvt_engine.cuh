@@ -29,6 +29,8 @@ constexpr int kKProj = 5;         // KPROJ (main.cu:394)
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
 constexpr int kKnnBlock = 128;    // threads per block of the site KNN kernel
 constexpr int kKnnBuf = 64;       // parked candidates per thread (shared memory)
+constexpr int kCellMinBlocks = 6;  // resident blocks per SM asked of k_site_cell (caps registers near 80;
+                                   // its two polygon buffers take 32 KB per block)
 
 struct MeshDev {
   const float* V;
@@ -100,15 +102,22 @@ template <class PP> struct PolyRef {
 
 // Sutherland-Hodgman clip by a*x + b*y - c <= eps (2dClip.cuh:11-53).  Stops
 // with ovf = true before writing vertex `cap` (buffer full); keeps the
-// reference's 64-vertex cap (2dClip.cuh:47-50) for larger buffers.
+// reference's 64-vertex cap (2dClip.cuh:47-50) for larger buffers.  r2 returns
+// the largest squared vertex radius of the output (NaN if any vertex is NaN).
 template <class PP, class Q>
 __device__ __forceinline__ int clip_poly(const PolyRef<PP>& in, int n, const PolyRef<PP>& out, Q a, Q b, Q c,
-                                         Q eps, int cap, bool& ovf) {
+                                         Q eps, int cap, bool& ovf, Q& r2) {
+  r2 = (Q)0;
   if (n <= 0) return 0;
   auto f = [&](V2<PP> p) -> Q { return fmaT(a, (Q)p.x, fmaT(b, (Q)p.y, -c)); };
   auto isect = [&](V2<PP> s, V2<PP> e, Q fs, Q fe) -> V2<PP> {
     Q t = divT(fs, (fs - fe) + (Q)1e-30);
     return {(PP)fmaT(t, (Q)e.x - (Q)s.x, (Q)s.x), (PP)fmaT(t, (Q)e.y - (Q)s.y, (Q)s.y)};
+  };
+  auto put = [&](int k, V2<PP> v) {
+    out.set(k, v);
+    const Q q = fmaT((Q)v.y, (Q)v.y, (Q)v.x * (Q)v.x);
+    r2 = (q > r2 || q != q) ? q : r2;
   };
   V2<PP> s = in.get(n - 1);
   Q fs = f(s);
@@ -121,13 +130,13 @@ __device__ __forceinline__ int clip_poly(const PolyRef<PP>& in, int n, const Pol
     if (ins_e) {
       if (!ins_s) {
         if (m >= cap) { ovf = true; return m; }
-        out.set(m++, isect(s, e, fs, fe));
+        put(m++, isect(s, e, fs, fe));
       }
       if (m >= cap) { ovf = true; return m; }
-      out.set(m++, e);
+      put(m++, e);
     } else if (ins_s) {
       if (m >= cap) { ovf = true; return m; }
-      out.set(m++, isect(s, e, fs, fe));
+      put(m++, isect(s, e, fs, fe));
     }
     s = e; fs = fe; ins_s = ins_e;
     if (m >= 64) { m = 64; break; }
@@ -135,25 +144,54 @@ __device__ __forceinline__ int clip_poly(const PolyRef<PP>& in, int n, const Pol
   return m;
 }
 
+// True when the half-plane a*x + b*y <= c holds, as the clip's predicate
+// computes it, at every point within sqrt(r2) of the origin: then clipping
+// by it returns the polygon unchanged (same vertices, same order) and can be
+// skipped.  By Cauchy-Schwarz a*x + b*y <= sqrt((a^2+b^2) r2); the 1e-4
+// relative margin covers the rounding of this test (a few ulp) and of the
+// predicate fma(a, x, fma(b, y, -c)) (< 2 ulp of c), so the skip is exact.
+// c > 1e-18 keeps the products away from underflow.  NaN fails the test.
+template <class Q>
+__device__ __forceinline__ bool halfplane_contains_disk(Q a, Q b, Q c, Q r2) {
+  return c > (Q)1e-18 && fmaT(a, a, b * b) * r2 * (Q)1.0001 < c * c;
+}
+
 // Clip the square [-R,R]^2 by the bisectors of the listed neighbours; returns
 // the vertex count (polygon in `cur` on return) or -1 on buffer overflow.
+//
+// Security radius: a bisector whose half-plane contains the disk around the
+// site that holds the current polygon cannot cut it and is skipped
+// (halfplane_contains_disk).  When the row is this iteration's K-nearest list
+// of the same positions (ascending distance), every later neighbour j has
+// |d_j| >= |d_t|; the tangent-plane normal of its bisector is at most |d_j|
+// long and its offset is |d_j|^2/2, so once |d_t|^2 > 4 r2 (with a 1e-3
+// margin for the distance keys' rounding) none of the remaining bisectors can
+// cut the polygon and the loop ends.  Both shortcuts only leave out clips
+// that would return their input unchanged: the result is the same bit for
+// bit as clipping by all K bisectors.
 template <int PROF>
 __device__ __forceinline__ int clip_cell(const typename PT<PROF>::T* __restrict__ S, int site_base, int n_sites,
                                          V3<typename PT<PROF>::T> si, const uint32_t* __restrict__ row, int K,
                                          const Frame<typename PT<PROF>::T>& fr, float R,
                                          PolyRef<typename PT<PROF>::PP>& cur, PolyRef<typename PT<PROF>::PP>& nxt,
-                                         int cap) {
+                                         int cap, bool row_sorted) {
   using T = typename PT<PROF>::T;
   using Q = typename PT<PROF>::Q;
   using PP = typename PT<PROF>::PP;
   const PP r = (PP)R;
   cur.set(0, {-r, -r}); cur.set(1, {r, -r}); cur.set(2, {r, r}); cur.set(3, {-r, r});
   int n = 4;
+  Q r2 = (Q)2 * (Q)r * (Q)r * (Q)1.0001;
   bool ovf = false;
   // the next neighbour's position is loaded while the current one clips
   uint32_t jn = __ldg(row);
   V3<T> sn = jn < (uint32_t)n_sites ? ld3(S, (long)site_base + jn) : si;
+  // Every lane runs all K trips; a finished lane only skips their bodies.  A
+  // data-dependent `break` lets lanes leave at different trips, and the warp
+  // then runs the rest of the site's work in fragments (measured 2x slower).
+  bool done = false;
   for (int t = 0; t < K; ++t) {
+    if (done) continue;
     const uint32_t j = jn;
     const V3<T> sj = sn;
     if (t + 1 < K) {
@@ -170,10 +208,14 @@ __device__ __forceinline__ int clip_cell(const typename PT<PROF>::T* __restrict_
       V3<T> d = sub3(sj, si);
       a = (Q)dot3(d, fr.u); b = (Q)dot3(d, fr.v); c = (Q)((T)0.5 * dot3(d, d));
     }
-    n = clip_poly<PP, Q>(cur, n, nxt, a, b, c, (Q)1e-12, cap, ovf);
-    if (ovf) return -1;
+    if (halfplane_contains_disk(a, b, c, r2)) {
+      done = row_sorted && c > (Q)1e-18 && (Q)2.002 * r2 < c;
+      continue;
+    }
+    n = clip_poly<PP, Q>(cur, n, nxt, a, b, c, (Q)1e-12, cap, ovf, r2);
+    if (ovf) { n = -1; done = true; continue; }
     PolyRef<PP> tmp = cur; cur = nxt; nxt = tmp;
-    if (n == 0) break;
+    if (n == 0) done = true;
   }
   return n;
 }
@@ -386,7 +428,7 @@ __device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>
 
   // clip + centroid
   PolyRef<PP> cur = A, nxt = B;
-  const int np = clip_cell<PROF>(S, sd.site_base, sd.n_sites, si, row, K, fr, md.R, cur, nxt, cap);
+  const int np = clip_cell<PROF>(S, sd.site_base, sd.n_sites, si, row, K, fr, md.R, cur, nxt, cap, !fz);
   if (np < 0) return false;
   const V2<PP> c2 = poly_centroid<PP>(cur, np, PROF == PROF_MIXED);
   V3<T> cent;
@@ -487,7 +529,7 @@ __device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, cons
 }
 
 template <int PROF, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK) k_site_cell(EngineArgs<typename PT<PROF>::T> a, int parity) {
+__global__ void __launch_bounds__(BLOCK, kCellMinBlocks) k_site_cell(EngineArgs<typename PT<PROF>::T> a, int parity) {
   using PP = typename PT<PROF>::PP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V2<PP>* sm = reinterpret_cast<V2<PP>*>(smem_raw);

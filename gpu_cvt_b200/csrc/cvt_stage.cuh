@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(BLOCK) k_stage_clip(const float* __restrict__ 
   V3<float> si = ld3(S, i);
   Frame<float> fr{ld3(U, i), ld3(Vv, i)};
   PolyRef<PP> cur = A, nxt = B;
-  int np = clip_cell<PROF>(S, 0, n, si, knn + (size_t)i * K, K, fr, R, cur, nxt, CAP);
+  int np = clip_cell<PROF>(S, 0, n, si, knn + (size_t)i * K, K, fr, R, cur, nxt, CAP, false);
   if (np < 0) {
     int k = atomicAdd(ovf, 1);
     ovf[1 + k] = i;
@@ -224,7 +224,7 @@ __global__ void __launch_bounds__(64) k_stage_clip_fallback(const float* __restr
     V3<float> si = ld3(S, i);
     Frame<float> fr{ld3(U, i), ld3(Vv, i)};
     PolyRef<PP> cur{buf[0], 1}, nxt{buf[1], 1};
-    int np = clip_cell<PROF>(S, 0, n, si, knn + (size_t)i * K, K, fr, R, cur, nxt, kFallbackCap);
+    int np = clip_cell<PROF>(S, 0, n, si, knn + (size_t)i * K, K, fr, R, cur, nxt, kFallbackCap, false);
     V2<PP> c2 = poly_centroid<PP>(cur, np, PROF == PROF_MIXED);
     V3<float> c;
     if (!(finiteT(c2.x) && finiteT(c2.y))) c = {NAN, NAN, NAN};

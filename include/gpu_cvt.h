@@ -175,11 +175,15 @@ typedef struct {
   float area;
   float bbox_lo[3], bbox_hi[3];
   float diag;          /* bbox diagonal */
-  size_t device_bytes; /* HBM held by the mesh */
+  size_t device_bytes; /* HBM held by the mesh (grows when the BVH or the
+                          sampler's area table is first built) */
 } cvt_mesh_info_t;
 
 /* Host arrays in; the mesh is compacted, uploaded and preprocessed (vertex
- * normals, vertex->face CSR, vertex grid, BVH) and stays resident. */
+ * normals, vertex->face CSR, vertex grid) and stays resident.  The BVH is
+ * built on the first Hausdorff distance against the mesh, the area table on
+ * the first cvt_mesh_sample_sites; both are then kept (first use is
+ * thread-safe). */
 cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, int nF, cvt_mesh_t* out);
 /* Cell edge of the vertex grid of meshes created afterwards, in units of the
  * radius expected to hold 6 vertices (default 1.5; a tuning knob only). */
