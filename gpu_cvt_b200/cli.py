@@ -11,8 +11,10 @@ samples.  Outputs, under experiments/output/<gpucvt|freeze|freeze_tiered>/<mesh>
 * eval_iters.csv  -- every DUMP_STRIDE=10 iterations: quality, one-sided
                      Hausdorff, per-stage milliseconds, freeze counts
                      (the reference's 28 columns, evaluate.cuh:468-550)
-* iter_%03d.obj, iter_%03d_frozen.txt -- the dual-triangle mesh and the
-                     frozen mask at those iterations
+* iter_%03d.obj, iter_%03d_sites.xyz, iter_%03d_frozen.txt -- the
+                     dual-triangle mesh, the sites ("x y z" lines,
+                     buildmesh.cuh:203-207) and the frozen mask at those
+                     iterations
 and one row appended to experiments/runs.csv (main.cu:342-368).  The stdout
 lines follow main.cu's.
 
@@ -122,6 +124,8 @@ def main(argv=None) -> int:
             last_nf = F.shape[0]
             path = os.path.join(out_dir, f"iter_{it:03d}.obj")
             mg.save_obj(path, S, F)
+            with open(os.path.join(out_dir, f"iter_{it:03d}_sites.xyz"), "w") as fh:   # write_pts_cpu
+                fh.write("".join(f"{_g(x)} {_g(y)} {_g(z)}\n" for x, y, z in S))
             with open(os.path.join(out_dir, f"iter_{it:03d}_frozen.txt"), "w") as fh:
                 fh.write("\n".join(str(int(x)) for x in state["frozen"]) + "\n")
             print(f"iter {it} V {n} faces {last_nf} wrote {path}")

@@ -10,10 +10,13 @@
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_reduce.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cub/device/device_select.cuh>
 
 #include "../../include/gpu_cvt.h"
 #include "cvt_eval.cuh"
+#include "cvt_ingest.cuh"
 #include "cvt_stage.cuh"
 
 using namespace cvt;
@@ -335,18 +338,20 @@ struct cvt_mesh {
   GridGeom vg{};
   int* dvcell_start = nullptr;
   Pt4<float>* dvsorted = nullptr;
+  float4* dring = nullptr;    // one-ring records (3 per CSR entry)
+  float* dunref = nullptr;    // input vertices no face uses (Hausdorff probes only)
+  int n_unref = 0;
   BVHNode* dnodes = nullptr;  // built on first use (Hausdorff)
   int* dtri = nullptr;
   int nnodes = 0;
-  void* arena = nullptr;      // V, F, CSR, normals, vertex grid: one allocation
+  void* arena = nullptr;      // V, F, CSR, normals, ring records, unreferenced vertices
+  void* arena_grid = nullptr; // vertex grid (sized once the area is known)
   size_t bytes = 0;
   std::mutex lazy_mu;         // guards the first-use builds (BVH, area CDF)
-  std::vector<float> hV;
-  std::vector<int> hF;
   MeshDev dev() const {
     MeshDev m;
     m.V = dV; m.F = dF; m.vf_off = doff; m.vf_faces = dfcs; m.N = dN;
-    m.vcell_start = dvcell_start; m.vsorted = dvsorted; m.vg = vg;
+    m.vcell_start = dvcell_start; m.vsorted = dvsorted; m.ring = dring; m.vg = vg;
     m.nV = nV; m.nF = nF; m.R = R;
     m.thr2 = ((0.01f * R) * 0.01f) * R;
     return m;
@@ -372,32 +377,108 @@ struct Arena {
 
 static void mesh_free(cvt_mesh* m) {
   if (!m) return;
-  cudaFree(m->arena); cudaFree(m->dcdf); cudaFree(m->dnodes); cudaFree(m->dtri);
+  cudaFree(m->arena); cudaFree(m->arena_grid); cudaFree(m->dcdf); cudaFree(m->dnodes); cudaFree(m->dtri);
   delete m;
 }
 
-// BVH of the mesh (evaluate.cuh:114-201), built on the host and uploaded the
-// first time a Hausdorff distance needs it.
+// Subtree node count of the median-split BVH for n triangles (shape only).
+static int bvh_subtree_nodes(int n, int leaf, std::vector<std::pair<int, int>>& memo) {
+  if (n <= leaf) return 1;
+  for (auto& kv : memo) if (kv.first == n) return kv.second;
+  const int c = 1 + bvh_subtree_nodes(n / 2, leaf, memo) + bvh_subtree_nodes(n - n / 2, leaf, memo);
+  memo.push_back({n, c});
+  return c;
+}
+
+// BVH of the mesh (evaluate.cuh:114-201, leaf 8), built on the device level
+// by level (cvt_ingest.cuh) the first time a Hausdorff distance needs it.
 static cvt_status_t mesh_ensure_bvh(cvt_mesh* m) {
   std::lock_guard<std::mutex> lk(m->lazy_mu);
   if (m->dnodes) return CVT_OK;
-  std::vector<BVHNode> nodes;
-  std::vector<int> tri;
-  build_bvh_host(m->hV.data(), m->hF.data(), m->nF, 8, nodes, tri);
+  constexpr int leaf = 8;
+  const int nF = m->nF;
+  cudaStream_t st = 0;
+  std::vector<std::pair<int, int>> memo;
+  const int n_nodes = bvh_subtree_nodes(nF, leaf, memo);
   BVHNode* dn = nullptr;
   int* dt = nullptr;
-  cudaError_t e = cudaMalloc(&dn, sizeof(BVHNode) * std::max<size_t>(nodes.size(), 1));
-  if (e == cudaSuccess) e = cudaMalloc(&dt, sizeof(int) * std::max<size_t>(tri.size(), 1));
-  if (e == cudaSuccess) e = cudaMemcpy(dn, nodes.data(), sizeof(BVHNode) * nodes.size(), cudaMemcpyHostToDevice);
-  if (e == cudaSuccess) e = cudaMemcpy(dt, tri.data(), sizeof(int) * tri.size(), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) {
+  cudaError_t e = cudaMalloc(&dn, sizeof(BVHNode) * (size_t)n_nodes);
+  if (e == cudaSuccess) e = cudaMalloc(&dt, sizeof(int) * (size_t)nF);
+  auto bail = [&](cudaError_t err) {
     cudaFree(dn); cudaFree(dt);
-    return fail(e == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,
-                std::string("mesh BVH: ") + cudaGetErrorString(e));
+    return fail(err == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,
+                std::string("mesh BVH: ") + cudaGetErrorString(err));
+  };
+  if (e != cudaSuccess) return bail(e);
+  {
+    Scratch sc(st);
+    float* tinfo;
+    int *ids2, *acc, *axis;
+    unsigned long long *keys, *keys2;
+    BvhSeg* dseg;
+    // a split segment has more than `leaf` triangles, so both halves hold at
+    // least leaf/2: the frontier never has more than nF/(leaf/2) + 1 segments
+    const size_t max_seg = (size_t)nF / (leaf / 2) + 2;
+    if ((e = sc.get(&tinfo, 9 * (size_t)nF)) != cudaSuccess || (e = sc.get(&ids2, (size_t)nF)) != cudaSuccess ||
+        (e = sc.get(&keys, (size_t)nF)) != cudaSuccess || (e = sc.get(&keys2, (size_t)nF)) != cudaSuccess ||
+        (e = sc.get(&acc, 12 * max_seg)) != cudaSuccess || (e = sc.get(&axis, max_seg)) != cudaSuccess ||
+        (e = sc.get(&dseg, max_seg)) != cudaSuccess)
+      return bail(e);
+    k_tri_info<<<cdiv(nF, 256), 256, 0, st>>>(m->dV, m->dF, nF, tinfo);
+    k_iota<<<cdiv(nF, 256), 256, 0, st>>>(dt, nF);
+    LAUNCHED(2);
+    size_t tb = 0;
+    if ((e = cub::DeviceRadixSort::SortPairs(nullptr, tb, keys, keys2, dt, ids2, nF, 0, 64, st)) != cudaSuccess)
+      return bail(e);
+    void* tmp;
+    if ((e = sc.get(reinterpret_cast<char**>(&tmp), tb)) != cudaSuccess) return bail(e);
+    std::vector<BvhSeg> segs{{0, nF, 0, -1, -1}};
+    int* cur = dt;
+    int* alt = ids2;
+    while (true) {
+      bool split = false;
+      for (auto& g : segs)
+        if (g.node >= 0 && g.count > leaf) {
+          g.left = g.node + 1;
+          g.right = g.node + 1 + bvh_subtree_nodes(g.count / 2, leaf, memo);
+          split = true;
+        }
+      const int nseg = (int)segs.size();
+      if ((e = cudaMemcpyAsync(dseg, segs.data(), sizeof(BvhSeg) * nseg, cudaMemcpyHostToDevice, st)) != cudaSuccess)
+        return bail(e);
+      k_seg_acc_init<<<cdiv(nseg, 256), 256, 0, st>>>(nseg, acc);
+      k_seg_reduce<<<cdiv(nF, 256), 256, 0, st>>>(cur, nF, dseg, nseg, tinfo, acc);
+      k_seg_emit<<<cdiv(nseg, 256), 256, 0, st>>>(dseg, nseg, acc, leaf, dn, axis);
+      LAUNCHED(3);
+      if (!split) break;
+      k_seg_keys<<<cdiv(nF, 256), 256, 0, st>>>(cur, nF, dseg, nseg, axis, tinfo, keys);
+      LAUNCHED(1);
+      int sbits = 1;
+      while (sbits < 31 && (1LL << sbits) < (long long)nseg) ++sbits;
+      if ((e = cub::DeviceRadixSort::SortPairs(tmp, tb, keys, keys2, cur, alt, nF, 0, 32 + sbits, st)) != cudaSuccess)
+        return bail(e);
+      std::swap(cur, alt);
+      std::vector<BvhSeg> next;
+      next.reserve(2 * segs.size());
+      for (const auto& g : segs) {
+        if (g.node >= 0 && g.count > leaf) {
+          next.push_back({g.start, g.count / 2, g.left, -1, -1});
+          next.push_back({g.start + g.count / 2, g.count - g.count / 2, g.right, -1, -1});
+        } else {
+          next.push_back({g.start, g.count, -1, -1, -1});
+        }
+      }
+      // (a pageable upload has left the host buffer when cudaMemcpyAsync
+      // returns; the device copy is reused in stream order)
+      segs.swap(next);
+    }
+    if (cur != dt && (e = cudaMemcpyAsync(dt, cur, sizeof(int) * (size_t)nF, cudaMemcpyDeviceToDevice, st)) != cudaSuccess)
+      return bail(e);
+    if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaStreamSynchronize(st)) != cudaSuccess) return bail(e);
   }
-  m->nnodes = (int)nodes.size();
+  m->nnodes = n_nodes;
   m->dtri = dt;
-  m->bytes += sizeof(BVHNode) * nodes.size() + sizeof(int) * tri.size();
+  m->bytes += sizeof(BVHNode) * (size_t)n_nodes + sizeof(int) * (size_t)nF;
   m->dnodes = dn;
   return CVT_OK;
 }
@@ -407,21 +488,23 @@ static cvt_status_t mesh_ensure_cdf(cvt_mesh* m) {
   std::lock_guard<std::mutex> lk(m->lazy_mu);
   if (m->dcdf) return CVT_OK;
   const int nF = m->nF;
-  std::vector<double> cdf(nF);
-  double accum = 0.0;
-  for (int f = 0; f < nF; ++f) {
-    const float* pa = &m->hV[3 * (size_t)m->hF[3 * f]];
-    const float* pb = &m->hV[3 * (size_t)m->hF[3 * f + 1]];
-    const float* pc = &m->hV[3 * (size_t)m->hF[3 * f + 2]];
-    double e1[3] = {(double)pb[0] - pa[0], (double)pb[1] - pa[1], (double)pb[2] - pa[2]};
-    double e2[3] = {(double)pc[0] - pa[0], (double)pc[1] - pa[1], (double)pc[2] - pa[2]};
-    double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
-    accum += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
-    cdf[f] = accum;
-  }
+  cudaStream_t st = 0;
   double* d = nullptr;
   cudaError_t e = cudaMalloc(&d, sizeof(double) * std::max(nF, 1));
-  if (e == cudaSuccess) e = cudaMemcpy(d, cdf.data(), sizeof(double) * nF, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    Scratch sc(st);
+    double* fa;
+    size_t tb = 0;
+    void* tmp;
+    if ((e = sc.get(&fa, (size_t)nF)) == cudaSuccess &&
+        (e = cub::DeviceScan::InclusiveSum(nullptr, tb, fa, d, nF, st)) == cudaSuccess &&
+        (e = sc.get(reinterpret_cast<char**>(&tmp), tb)) == cudaSuccess) {
+      k_face_area<<<cdiv(nF, 256), 256, 0, st>>>(m->dV, m->dF, nF, fa);
+      LAUNCHED(1);
+      if ((e = cudaGetLastError()) == cudaSuccess) e = cub::DeviceScan::InclusiveSum(tmp, tb, fa, d, nF, st);
+    }
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     cudaFree(d);
     return fail(e == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,
@@ -465,61 +548,13 @@ static float g_vcell_factor = 1.5f;
 
 extern "C" void cvt_set_vertex_cell_factor(float f) { if (f > 0.f) g_vcell_factor = f; }
 
+// The device does the ingest (cvt_ingest.cuh): upload, validation, bounds,
+// compaction, areas and the face CSR; the host reads back five scalars to
+// size the resident arrays and the vertex grid.
 extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, int nF, cvt_mesh_t* out) {
   if (!out || !V || !F || nV <= 0 || nF <= 0) return fail(CVT_ERR_INVALID, "cvt_mesh_create: empty mesh or null pointer");
-  for (long k = 0; k < 3L * nF; ++k)
-    if (F[k] < 0 || F[k] >= nV) return fail(CVT_ERR_INVALID, "cvt_mesh_create: face index out of range");
   cvt_mesh* m = new cvt_mesh();
-  // R over every input vertex (main.cu:169-227)
-  float bmin[3] = {1e30f, 1e30f, 1e30f}, bmax[3] = {-1e30f, -1e30f, -1e30f};
-  for (int i = 0; i < nV; ++i)
-    for (int a = 0; a < 3; ++a) {
-      bmin[a] = std::fmin(bmin[a], V[3 * i + a]);
-      bmax[a] = std::fmax(bmax[a], V[3 * i + a]);
-    }
-  m->R = std::fmax(bmax[0] - bmin[0], std::fmax(bmax[1] - bmin[1], bmax[2] - bmin[2]));
-  // compaction (main.cu:230-257)
-  std::vector<int> remap(nV, -1);
-  std::vector<unsigned char> used(nV, 0);
-  for (long k = 0; k < 3L * nF; ++k) used[F[k]] = 1;
-  int nn = 0;
-  for (int i = 0; i < nV; ++i) if (used[i]) remap[i] = nn++;
-  m->nV = nn;
-  m->nF = nF;
-  m->hV.resize(3 * (size_t)nn);
-  for (int i = 0; i < nV; ++i)
-    if (remap[i] >= 0) for (int a = 0; a < 3; ++a) m->hV[3 * (size_t)remap[i] + a] = V[3 * i + a];
-  m->hF.resize(3 * (size_t)nF);
-  for (long k = 0; k < 3L * nF; ++k) m->hF[k] = remap[F[k]];
-  double area = 0.0;
-  for (int a = 0; a < 3; ++a) { m->lo[a] = 1e30f; m->hi[a] = -1e30f; }
-  for (int i = 0; i < nn; ++i)
-    for (int a = 0; a < 3; ++a) {
-      m->lo[a] = std::fmin(m->lo[a], m->hV[3 * i + a]);
-      m->hi[a] = std::fmax(m->hi[a], m->hV[3 * i + a]);
-    }
-  for (int f = 0; f < nF; ++f) {
-    const float* a = &m->hV[3 * (size_t)m->hF[3 * f]];
-    const float* b = &m->hV[3 * (size_t)m->hF[3 * f + 1]];
-    const float* c = &m->hV[3 * (size_t)m->hF[3 * f + 2]];
-    double e1[3] = {(double)b[0] - a[0], (double)b[1] - a[1], (double)b[2] - a[2]};
-    double e2[3] = {(double)c[0] - a[0], (double)c[1] - a[1], (double)c[2] - a[2]};
-    double cx = e1[1] * e2[2] - e1[2] * e2[1], cy = e1[2] * e2[0] - e1[0] * e2[2], cz = e1[0] * e2[1] - e1[1] * e2[0];
-    area += 0.5 * std::sqrt(cx * cx + cy * cy + cz * cz);
-  }
-  m->area = (float)area;
-  double dx = (double)m->hi[0] - m->lo[0], dy = (double)m->hi[1] - m->lo[1], dz = (double)m->hi[2] - m->lo[2];
-  m->diag = (float)std::sqrt(dx * dx + dy * dy + dz * dz);
-  // vertex -> face CSR in face order (main.cu:259-285)
-  std::vector<int> off(nn + 1, 0), fcs(3 * (size_t)nF);
-  for (long k = 0; k < 3L * nF; ++k) off[m->hF[k] + 1]++;
-  for (int v = 0; v < nn; ++v) off[v + 1] += off[v];
-  {
-    std::vector<int> cur(off.begin(), off.end() - 1);
-    for (int f = 0; f < nF; ++f)
-      for (int k = 0; k < 3; ++k) fcs[cur[m->hF[3 * f + k]]++] = f;
-  }
-  m->vg = surface_grid(m->lo, m->hi, area, nn, 6.0, g_vcell_factor, 4L * nn + 64);
+  cudaStream_t st = 0;
   cudaError_t e = cudaSuccess;
 #define MCK(x)                                                                              \
   do {                                                                                      \
@@ -530,28 +565,115 @@ extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, in
                   std::string("cvt_mesh_create: ") + cudaGetErrorString(e));                \
     }                                                                                       \
   } while (0)
+  const long n3 = 3L * nF;
+  Scratch sc(st);
+  float* rV;
+  int *rF, *used, *remap, *info;   // info: bad, bounds[12]
+  double *farea, *area_sum;
+  MCK(sc.get(&rV, 3 * (size_t)nV));
+  MCK(sc.get(&rF, (size_t)n3));
+  MCK(sc.get(&used, (size_t)nV));
+  MCK(sc.get(&remap, (size_t)nV));
+  MCK(sc.get(&info, 13));
+  MCK(sc.get(&farea, (size_t)nF));
+  MCK(sc.get(&area_sum, 1));
+  MCK(cudaMemcpyAsync(rV, V, sizeof(float) * 3 * (size_t)nV, cudaMemcpyHostToDevice, st));
+  MCK(cudaMemcpyAsync(rF, F, sizeof(int) * (size_t)n3, cudaMemcpyHostToDevice, st));
+  MCK(cudaMemsetAsync(used, 0, sizeof(int) * (size_t)nV, st));
+  MCK(cudaMemsetAsync(info, 0, sizeof(int), st));
+  k_ingest_bounds_init<<<1, 32, 0, st>>>(info + 1);
+  k_ingest_mark<<<cdiv(n3, 256), 256, 0, st>>>(rF, n3, nV, used, info);
+  k_ingest_bounds<<<cdiv(nV, 256), 256, 0, st>>>(rV, nV, used, info + 1, info);
+  LAUNCHED(3);
+  MCK(cudaGetLastError());
+  {
+    size_t tb = 0;
+    MCK(cub::DeviceScan::ExclusiveSum(nullptr, tb, used, remap, nV, st));
+    void* tmp;
+    MCK(sc.get(reinterpret_cast<char**>(&tmp), tb));
+    MCK(cub::DeviceScan::ExclusiveSum(tmp, tb, used, remap, nV, st));
+  }
+  int h[15];
+  MCK(cudaMemcpyAsync(h, info, sizeof(int) * 13, cudaMemcpyDeviceToHost, st));
+  MCK(cudaMemcpyAsync(h + 13, remap + nV - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaMemcpyAsync(h + 14, used + nV - 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+  MCK(cudaStreamSynchronize(st));
+  if (h[0] & 1) { mesh_free(m); return fail(CVT_ERR_INVALID, "cvt_mesh_create: face index out of range"); }
+  if (h[0] & 2) { mesh_free(m); return fail(CVT_ERR_INVALID, "cvt_mesh_create: non-finite coordinate in a face's vertex"); }
+  auto ord2f = [](int o) { int b = o >= 0 ? o : o ^ 0x7fffffff; float f; std::memcpy(&f, &b, 4); return f; };
+  // R over every input vertex (main.cu:169-227)
+  float bmin[3], bmax[3];
+  for (int a = 0; a < 3; ++a) {
+    bmin[a] = ord2f(h[1 + a]); bmax[a] = ord2f(h[4 + a]);
+    m->lo[a] = ord2f(h[7 + a]); m->hi[a] = ord2f(h[10 + a]);
+  }
+  m->R = std::fmax(bmax[0] - bmin[0], std::fmax(bmax[1] - bmin[1], bmax[2] - bmin[2]));
+  const int nn = h[13] + h[14];
+  m->nV = nn;
+  m->nF = nF;
+  m->n_unref = nV - nn;
+  double dx = (double)m->hi[0] - m->lo[0], dy = (double)m->hi[1] - m->lo[1], dz = (double)m->hi[2] - m->lo[2];
+  m->diag = (float)std::sqrt(dx * dx + dy * dy + dz * dz);
   Arena ar;
   ar.add(&m->dV, 3 * (size_t)nn);
-  ar.add(&m->dF, 3 * (size_t)nF);
+  ar.add(&m->dF, (size_t)n3);
   ar.add(&m->doff, (size_t)nn + 1);
-  ar.add(&m->dfcs, 3 * (size_t)nF);
+  ar.add(&m->dfcs, (size_t)n3);
   ar.add(&m->dN, 3 * (size_t)nn);
-  ar.add(&m->dvcell_start, (size_t)m->vg.ncell + 2);
-  ar.add(&m->dvsorted, (size_t)nn);
+  ar.add(&m->dring, 9 * (size_t)nF);
+  ar.add(&m->dunref, 3 * (size_t)m->n_unref);
+  // the vertex grid's cell array is sized after the area is known
   MCK(ar.commit(&m->arena));
   m->bytes = ar.size;
-  cudaStream_t st = 0;
-  MCK(cudaMemcpyAsync(m->dV, m->hV.data(), sizeof(float) * 3 * nn, cudaMemcpyHostToDevice, st));
-  MCK(cudaMemcpyAsync(m->dF, m->hF.data(), sizeof(int) * 3 * (size_t)nF, cudaMemcpyHostToDevice, st));
-  MCK(cudaMemcpyAsync(m->doff, off.data(), sizeof(int) * (nn + 1), cudaMemcpyHostToDevice, st));
-  MCK(cudaMemcpyAsync(m->dfcs, fcs.data(), sizeof(int) * 3 * (size_t)nF, cudaMemcpyHostToDevice, st));
+  unsigned long long *keys, *keys2;
+  int* vcount;
+  MCK(sc.get(&keys, (size_t)n3));
+  MCK(sc.get(&keys2, (size_t)n3));
+  MCK(sc.get(&vcount, (size_t)nn + 1));
+  MCK(cudaMemsetAsync(vcount, 0, sizeof(int) * ((size_t)nn + 1), st));
+  k_ingest_compact<<<cdiv(nV, 256), 256, 0, st>>>(rV, nV, used, remap, m->dV, m->dunref);
+  k_ingest_faces<<<cdiv(n3, 256), 256, 0, st>>>(rF, n3, remap, m->dF, keys, vcount);
+  k_face_area<<<cdiv(nF, 256), 256, 0, st>>>(m->dV, m->dF, nF, farea);
+  LAUNCHED(3);
+  MCK(cudaGetLastError());
+  {
+    // vertex -> face CSR in face order (main.cu:259-285): sort (vertex, face)
+    int vbits = 1;
+    while (vbits < 32 && (1LL << vbits) <= (long long)nn) ++vbits;
+    size_t tb_sort = 0, tb_scan = 0, tb_sum = 0;
+    MCK(cub::DeviceRadixSort::SortKeys(nullptr, tb_sort, keys, keys2, (int)n3, 0, 32 + vbits, st));
+    MCK(cub::DeviceScan::ExclusiveSum(nullptr, tb_scan, vcount, m->doff, nn + 1, st));
+    MCK(cub::DeviceReduce::Sum(nullptr, tb_sum, farea, area_sum, nF, st));
+    void* tmp;
+    MCK(sc.get(reinterpret_cast<char**>(&tmp), std::max(tb_sort, std::max(tb_scan, tb_sum))));
+    MCK(cub::DeviceRadixSort::SortKeys(tmp, tb_sort, keys, keys2, (int)n3, 0, 32 + vbits, st));
+    k_keys_low32<<<cdiv(n3, 256), 256, 0, st>>>(keys2, n3, m->dfcs);
+    LAUNCHED(1);
+    MCK(cub::DeviceScan::ExclusiveSum(tmp, tb_scan, vcount, m->doff, nn + 1, st));
+    MCK(cub::DeviceReduce::Sum(tmp, tb_sum, farea, area_sum, nF, st));
+  }
+  double area = 0.0;
+  MCK(cudaMemcpyAsync(&area, area_sum, sizeof(double), cudaMemcpyDeviceToHost, st));
+  MCK(cudaStreamSynchronize(st));
+  m->area = (float)area;
+  m->vg = surface_grid(m->lo, m->hi, area, nn, 6.0, g_vcell_factor, 4L * nn + 64);
+  {
+    Arena ag;
+    ag.add(&m->dvcell_start, (size_t)m->vg.ncell + 2);
+    ag.add(&m->dvsorted, (size_t)nn);
+    MCK(ag.commit(&m->arena_grid));
+    m->bytes += ag.size;
+  }
   k_stage_normals<<<cdiv(nn, 256), 256, 0, st>>>(m->dV, nn, m->dF, m->doff, m->dfcs, m->dN);
   LAUNCHED(1);
   MCK(cudaGetLastError());
+  k_build_ring_records<<<cdiv(n3, 256), 256, 0, st>>>(m->dV, m->dF, nF, m->dfcs, n3, m->dring);
+  LAUNCHED(1);
+  MCK(cudaGetLastError());
   {
-    Scratch sc(st);
+    Scratch sg(st);
     PointGrid pg;
-    cvt_status_t s = build_point_grid(sc, m->dV, nn, 0.f, &m->vg, pg);
+    cvt_status_t s = build_point_grid(sg, m->dV, nn, 0.f, &m->vg, pg);
     if (s != CVT_OK) { mesh_free(m); return s; }
     MCK(cudaMemcpyAsync(m->dvcell_start, pg.cell_start, sizeof(int) * (m->vg.ncell + 2), cudaMemcpyDeviceToDevice, st));
     MCK(cudaMemcpyAsync(m->dvsorted, pg.sorted, sizeof(Pt4<float>) * nn, cudaMemcpyDeviceToDevice, st));
@@ -616,6 +738,66 @@ extern "C" cvt_status_t cvt_hausdorff_to_mesh(cvt_mesh_t ref, const float* Vc, i
   float d2;
   std::memcpy(&d2, &hb, sizeof(float));
   *out = std::sqrt(d2);
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_mesh_get_bvh(cvt_mesh_t m, void* nodes, int nodes_cap, int* tri, int tri_cap, int* n_nodes) {
+  if (!m || !n_nodes) return fail(CVT_ERR_INVALID, "cvt_mesh_get_bvh: null");
+  cvt_status_t ls = mesh_ensure_bvh(m);
+  if (ls != CVT_OK) return ls;
+  *n_nodes = m->nnodes;
+  if (nodes) {
+    if (nodes_cap < m->nnodes) return fail(CVT_ERR_CAPACITY, "cvt_mesh_get_bvh: node buffer too small");
+    CK(cudaMemcpy(nodes, m->dnodes, sizeof(BVHNode) * (size_t)m->nnodes, cudaMemcpyDeviceToHost));
+  }
+  if (tri) {
+    if (tri_cap < m->nF) return fail(CVT_ERR_CAPACITY, "cvt_mesh_get_bvh: triangle buffer too small");
+    CK(cudaMemcpy(tri, m->dtri, sizeof(int) * (size_t)m->nF, cudaMemcpyDeviceToHost));
+  }
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_hausdorff_meshes(cvt_mesh_t a, cvt_mesh_t b, float* out, float* a_to_b, float* b_to_a,
+                                             void* stream) {
+  if (!a || !b || !out) return fail(CVT_ERR_INVALID, "cvt_hausdorff_meshes: bad arguments");
+  cvt_status_t ls = mesh_ensure_bvh(a);
+  if (ls == CVT_OK) ls = mesh_ensure_bvh(b);
+  if (ls != CVT_OK) return ls;
+  cudaStream_t st = S_(stream);
+  Scratch sc(st);
+  unsigned* bits;
+  int* ovf;
+  CK(sc.get(&bits, 2));
+  CK(sc.get(&ovf, 1));
+  CK(cudaMemsetAsync(bits, 0, 2 * sizeof(unsigned), st));
+  CK(cudaMemsetAsync(ovf, 0, sizeof(int), st));
+  // probes of `from` (every input vertex, then per face the centroid and the
+  // three edge midpoints) against the BVH of `to`, max into *dst
+  auto side = [&](const cvt_mesh* from, const cvt_mesh* to, unsigned* dst) -> cudaError_t {
+    const long nP = (long)from->nV + 4L * from->nF;
+    k_hausdorff<<<cdiv(nP, 128), 128, 0, st>>>(from->dV, from->nV, from->dF, nP, to->dnodes, to->dtri, to->dV,
+                                               to->dF, dst, ovf);
+    LAUNCHED(1);
+    if (from->n_unref) {
+      k_hausdorff<<<cdiv(from->n_unref, 128), 128, 0, st>>>(from->dunref, from->n_unref, nullptr, from->n_unref,
+                                                             to->dnodes, to->dtri, to->dV, to->dF, dst, ovf);
+      LAUNCHED(1);
+    }
+    return cudaGetLastError();
+  };
+  CK(side(a, b, bits));
+  CK(side(b, a, bits + 1));
+  unsigned hb[2] = {0, 0};
+  int ho = 0;
+  CK(cudaMemcpyAsync(hb, bits, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(&ho, ovf, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (ho) return fail(CVT_ERR_CAPACITY, "cvt_hausdorff_meshes: BVH deeper than the traversal stack");
+  float d2[2];
+  std::memcpy(d2, hb, sizeof(d2));
+  if (a_to_b) *a_to_b = std::sqrt(d2[0]);
+  if (b_to_a) *b_to_a = std::sqrt(d2[1]);
+  *out = std::sqrt(std::max(d2[0], d2[1]));
   return CVT_OK;
 }
 

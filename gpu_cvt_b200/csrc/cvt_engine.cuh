@@ -40,6 +40,7 @@ struct MeshDev {
   const float* N;
   const int* vcell_start;
   const Pt4<float>* vsorted;
+  const float4* ring;  // one-ring records, 3 per CSR entry (k_build_ring_records)
   GridGeom vg;
   int nV, nF;
   float R;     // clip square half-size: longest input bbox edge (main.cu:421)
@@ -461,9 +462,9 @@ __device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>
   if (PROF == PROF_MIXED && !finite3(cent)) {
     sn = si;
   } else if (PROF == PROF_REF) {
-    sn = project_onering<T, float>(cent, md.V, md.nV, md.F, md.nF, md.vf_off, md.vf_faces, knnv, kKProj);
+    sn = project_onering_rec<T, float>(cent, md.ring, md.nV, md.vf_off, knnv, kKProj);
   } else {
-    sn = project_onering<T, double>(cent, md.V, md.nV, md.F, md.nF, md.vf_off, md.vf_faces, knnv, kKProj);
+    sn = project_onering_rec<T, double>(cent, md.ring, md.nV, md.vf_off, knnv, kKProj);
   }
   st3(a.S[parity ^ 1], g, sn);
 

@@ -1,4 +1,4 @@
-// Evaluation: BVH over the reference surface and the one-sided Hausdorff
+// Evaluation: BVH traversal over the reference surface and the one-sided Hausdorff
 // distance of a candidate mesh (evaluate.cuh:15-383), plus the dual-triangle
 // extraction that produces the candidate mesh from the sites
 // (near_project.cuh:201-352, buildmesh.cuh:11-241, main.cu:928-974).
@@ -15,80 +15,9 @@ struct BVHNode {
   int left, right, triStart, triCount;
 };
 
-// Host build with the reference's rule: bounds from the triangle boxes,
-// leaf <= leaf_size triangles, otherwise split the centroid-sorted list
-// (stable sort along the longest centroid-extent axis) at its middle;
-// nodes numbered in pre-order (evaluate.cuh:114-201).
-struct BvhBuilder {
-  const std::vector<float>& info;  // per triangle: bmin(3) bmax(3) ctr(3)
-  std::vector<BVHNode>& nodes;
-  std::vector<int>& tri;
-  int leaf;
-  int rec(std::vector<int>& tids) {
-    BVHNode nd{};
-    for (int a = 0; a < 3; ++a) { nd.bmin[a] = 1e30f; nd.bmax[a] = -1e30f; }
-    for (int t : tids)
-      for (int a = 0; a < 3; ++a) {
-        nd.bmin[a] = std::min(nd.bmin[a], info[9 * t + a]);
-        nd.bmax[a] = std::max(nd.bmax[a], info[9 * t + 3 + a]);
-      }
-    nd.left = nd.right = -1;
-    nd.triStart = -1;
-    nd.triCount = 0;
-    int me = (int)nodes.size();
-    nodes.push_back(nd);
-    if ((int)tids.size() <= leaf) {
-      nodes[me].triStart = (int)tri.size();
-      nodes[me].triCount = (int)tids.size();
-      tri.insert(tri.end(), tids.begin(), tids.end());
-      return me;
-    }
-    float cmin[3] = {1e30f, 1e30f, 1e30f}, cmax[3] = {-1e30f, -1e30f, -1e30f};
-    for (int t : tids)
-      for (int a = 0; a < 3; ++a) {
-        cmin[a] = std::min(cmin[a], info[9 * t + 6 + a]);
-        cmax[a] = std::max(cmax[a], info[9 * t + 6 + a]);
-      }
-    float ex = cmax[0] - cmin[0], ey = cmax[1] - cmin[1], ez = cmax[2] - cmin[2];
-    int axis = (ex >= ey && ex >= ez) ? 0 : (ey >= ez ? 1 : 2);
-    std::stable_sort(tids.begin(), tids.end(),
-                     [&](int a, int b) { return info[9 * a + 6 + axis] < info[9 * b + 6 + axis]; });
-    size_t mid = tids.size() / 2;
-    std::vector<int> L(tids.begin(), tids.begin() + mid), R(tids.begin() + mid, tids.end());
-    std::vector<int>().swap(tids);
-    int l = rec(L);
-    int r = rec(R);
-    nodes[me].left = l;
-    nodes[me].right = r;
-    return me;
-  }
-};
-
-inline void build_bvh_host(const float* V, const int* F, int nF, int leaf, std::vector<BVHNode>& nodes,
-                           std::vector<int>& tri) {
-  std::vector<float> info((size_t)9 * nF);
-  const float third = 1.0f / 3.0f;
-  for (int i = 0; i < nF; ++i) {
-    const float* a = V + 3 * F[3 * i];
-    const float* b = V + 3 * F[3 * i + 1];
-    const float* c = V + 3 * F[3 * i + 2];
-    float* o = &info[(size_t)9 * i];
-    for (int k = 0; k < 3; ++k) {
-      o[k] = std::min(a[k], std::min(b[k], c[k]));
-      o[3 + k] = std::max(a[k], std::max(b[k], c[k]));
-      o[6 + k] = (a[k] + (b[k] + c[k])) * third;
-    }
-  }
-  nodes.clear();
-  tri.clear();
-  nodes.reserve(2 * (size_t)nF / 4 + 16);
-  tri.reserve(nF);
-  if (nF == 0) return;
-  std::vector<int> tids(nF);
-  for (int i = 0; i < nF; ++i) tids[i] = i;
-  BvhBuilder b{info, nodes, tri, leaf};
-  b.rec(tids);
-}
+// The tree is the reference's (bounds from the triangle boxes, leaf <= 8
+// triangles, otherwise the centroid-sorted list split at its middle, nodes in
+// pre-order, evaluate.cuh:114-201); it is built on the device, cvt_ingest.cuh.
 
 // Per-probe closest squared distance to the BVH surface.  Near-first
 // traversal: of two children the nearer box is visited first, which only

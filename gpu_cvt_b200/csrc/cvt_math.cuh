@@ -195,6 +195,60 @@ __device__ __forceinline__ V3<T> project_onering(V3<T> c, const float* __restric
   return cvt3<T>(bp);
 }
 
+// One-ring records: for every vertex->face CSR entry (same order as the CSR),
+// the face's three corner positions and vertex ids in three 16-byte words,
+//   r0 = {A.x, A.y, A.z, B.x}, r1 = {B.y, B.z, C.x, C.y}, r2 = {C.z, ia, ib, ic}
+// (ids as int bits), so a projection reads one offset and then independent
+// 16-byte loads instead of the chain CSR entry -> face -> corners.
+__global__ void k_build_ring_records(const float* __restrict__ V, const int* __restrict__ F, int nF,
+                                     const int* __restrict__ fcs, long n_entries, float4* __restrict__ rec) {
+  const long ii = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ii >= n_entries) return;
+  const int fi = fcs[ii];
+  int ia = -1, ib = -1, ic = -1;
+  float a[3] = {0.f, 0.f, 0.f}, b[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
+  if ((unsigned)fi < (unsigned)nF) {
+    ia = F[3 * fi]; ib = F[3 * fi + 1]; ic = F[3 * fi + 2];
+    for (int k = 0; k < 3; ++k) { a[k] = V[3 * ia + k]; b[k] = V[3 * ib + k]; c[k] = V[3 * ic + k]; }
+  }
+  rec[3 * ii] = make_float4(a[0], a[1], a[2], b[0]);
+  rec[3 * ii + 1] = make_float4(b[1], b[2], c[0], c[1]);
+  rec[3 * ii + 2] = make_float4(c[2], __int_as_float(ia), __int_as_float(ib), __int_as_float(ic));
+}
+
+// project_onering over the one-ring records: the same faces in the same
+// order, the same arithmetic, so the same result bit for bit.
+template <class T, class Q>
+__device__ __forceinline__ V3<T> project_onering_rec(V3<T> c, const float4* __restrict__ rec, int nV,
+                                                     const int* __restrict__ off, const int* knnv, int kproj) {
+  V3<Q> cq = cvt3<Q>(c), bp = cq;
+  Q best = (Q)1e30;
+  for (int t = 0; t < kproj; ++t) {
+    int v = knnv[t];
+    if ((unsigned)v >= (unsigned)nV) continue;
+    int beg = __ldg(off + v), end = __ldg(off + v + 1);
+    for (int ii = beg; ii < end; ++ii) {
+      const float4 r0 = __ldg(rec + 3 * ii), r1 = __ldg(rec + 3 * ii + 1), r2 = __ldg(rec + 3 * ii + 2);
+      const int ia = __float_as_int(r2.y), ib = __float_as_int(r2.z), ic = __float_as_int(r2.w);
+      if (ia < 0) continue;
+      bool seen = false;
+      for (int s = 0; s < t; ++s) {
+        const int w = knnv[s];
+        seen = seen || w == ia || w == ib || w == ic;
+      }
+      if (seen) continue;
+      V3<Q> A = {(Q)r0.x, (Q)r0.y, (Q)r0.z};
+      V3<Q> B = {(Q)r0.w, (Q)r1.x, (Q)r1.y};
+      V3<Q> C = {(Q)r1.z, (Q)r1.w, (Q)r2.x};
+      V3<Q> p = closest_point_tri(cq, A, B, C);
+      V3<Q> dd = sub3(p, cq);
+      Q d2 = dot3(dd, dd);
+      if (d2 < best) { best = d2; bp = p; }
+    }
+  }
+  return cvt3<T>(bp);
+}
+
 // --------------------------------------------------------------------------
 // evaluation primitives (evaluate.cuh:44-104)
 // --------------------------------------------------------------------------

@@ -72,6 +72,25 @@ class Mesh:
              C.byref(out), stream)
         return float(out.value)
 
+    def bvh(self):
+        """(nodes structured array, face ids) of the evaluation BVH."""
+        n = C.c_int()
+        call("cvt_mesh_get_bvh", self.handle, None, 0, None, 0, C.byref(n))
+        dt = np.dtype([("bmin", np.float32, 3), ("bmax", np.float32, 3), ("left", np.int32),
+                       ("right", np.int32), ("triStart", np.int32), ("triCount", np.int32)])
+        nodes = np.zeros(n.value, dt)
+        tri = np.zeros(self.nF, np.int32)
+        call("cvt_mesh_get_bvh", self.handle, nodes.ctypes.data_as(C.c_void_p), n.value,
+             tri.ctypes.data_as(C.c_void_p), self.nF, C.byref(n))
+        return nodes, tri
+
+    def hausdorff(self, other: "Mesh", stream=None) -> dict:
+        """Symmetric Hausdorff distance to another mesh (scripts/evaluate.py
+        hausdorff_bvh): {"dH": max of both sides, "self_to_other", "other_to_self"}."""
+        out, ab, ba = C.c_float(), C.c_float(), C.c_float()
+        call("cvt_hausdorff_meshes", self.handle, other.handle, C.byref(out), C.byref(ab), C.byref(ba), stream)
+        return {"dH": float(out.value), "self_to_other": float(ab.value), "other_to_self": float(ba.value)}
+
     def sample_sites(self, out_tensor, seed: int, stream=None) -> None:
         """Fill a (n,3) float32 CUDA tensor with area-uniform points (device
         sampler, counter hash of (seed, i))."""

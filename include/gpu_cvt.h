@@ -193,6 +193,19 @@ cvt_status_t cvt_mesh_info(cvt_mesh_t m, cvt_mesh_info_t* info);
 cvt_status_t cvt_mesh_device_arrays(cvt_mesh_t m, const float** V, const int** F, const float** N,
                                     const int** vf_off, const int** vf_faces);
 cvt_status_t cvt_mesh_destroy(cvt_mesh_t m);
+/* The evaluation BVH (built on first use): n_nodes 40-byte nodes {float
+ * bmin[3], bmax[3]; int left, right, triStart, triCount} in pre-order and the
+ * nF face ids the leaves index (evaluate.cuh:15-22,114-201).  nodes / tri
+ * may be NULL (count only); otherwise host buffers of nodes_cap / tri_cap
+ * entries.  Synchronous. */
+cvt_status_t cvt_mesh_get_bvh(cvt_mesh_t m, void* nodes, int nodes_cap, int* tri, int tri_cap, int* n_nodes);
+/* Symmetric Hausdorff distance between two meshes (scripts/evaluate.py:
+ * 271-290, hausdorff_bvh): each mesh's probes -- every input vertex (also
+ * those no face uses), every face centroid and edge midpoint -- against the
+ * other's BVH, FP32 as the GPU evaluator (evaluate.cuh:291-357).  *out =
+ * max of the two sides; a_to_b / b_to_a (may be NULL) are the one-sided
+ * distances.  Synchronous. */
+cvt_status_t cvt_hausdorff_meshes(cvt_mesh_t a, cvt_mesh_t b, float* out, float* a_to_b, float* b_to_a, void* stream);
 /* n area-uniform points on the mesh (device out, n*3 floats): a face drawn by
  * area, then the square-root barycentric map, three uniforms per point from
  * a counter hash of (seed, i).  New (the reference starts from the vertices,

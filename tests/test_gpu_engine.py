@@ -243,6 +243,8 @@ def test_cli_driver_contract(tmp_path):
         V = mg.load_obj(str(d / f"iter_{it:03d}.obj"))
         assert V.nV == m.nV and V.nF > m.nV
         assert len((d / f"iter_{it:03d}_frozen.txt").read_text().split()) == m.nV
+        xyz = np.loadtxt(d / f"iter_{it:03d}_sites.xyz")
+        assert xyz.shape == (m.nV, 3) and np.allclose(xyz, V.V, atol=1e-5)
     runs = (tmp_path / "experiments" / "runs.csv").read_text().strip().split("\n")
     assert runs[0] == cli.RUNS_HEADER and runs[1].startswith("ball,freeze,")
     dH = float(rows[2].split(",")[9])

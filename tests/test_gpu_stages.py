@@ -238,6 +238,26 @@ def test_hausdorff(oracle):
     mesh.close()
 
 
+def test_hausdorff_symmetric(oracle):
+    """Both sides of scripts/evaluate.py's hausdorff_bvh, including probes at
+    input vertices that no face uses."""
+    from gpu_cvt_b200.engine import Mesh
+    ref = mg.icosphere(4)
+    c = mg.icosphere(3)
+    Vc = (c.V * np.float32(1.02)).astype(np.float32)
+    Vc[::7] *= np.float32(0.97)
+    Vc = np.vstack([Vc, np.array([[0.0, 0.0, 1.6]], np.float32)])   # unreferenced vertex
+    A, B = Mesh(Vc, c.F), Mesh(ref.V, ref.F)
+    got = A.hausdorff(B)
+    ab = oracle.hausdorff_one_sided(Vc, c.F, ref.V, ref.F)
+    ba = oracle.hausdorff_one_sided(ref.V, ref.F, Vc, c.F)
+    assert abs(got["self_to_other"] - ab) <= 1e-6 * ab
+    assert abs(got["other_to_self"] - ba) <= 1e-6 * ba
+    assert got["dH"] == max(got["self_to_other"], got["other_to_self"])
+    assert abs(got["self_to_other"] - 0.6) < 1e-5       # the lone vertex sets this side
+    A.close(); B.close()
+
+
 def test_extract_faces_and_quality(st, oracle):
     m = mg.icosphere(4)
     S = mg.sample_sites(m.V, m.F, 1500, seed=2)
@@ -253,3 +273,75 @@ def test_extract_faces_and_quality(st, oracle):
     qo = oracle.quality(S, Fo)
     for k in qo:
         assert abs(q[k] - qo[k]) <= 1e-4 * max(1.0, abs(qo[k])), k
+
+
+def _d2h(ptr, n, dtype):
+    from cuda.bindings import runtime as rt
+    out = np.empty(n, dtype)
+    err, = rt.cudaMemcpy(out.ctypes.data, ptr, out.nbytes, rt.cudaMemcpyKind.cudaMemcpyDeviceToHost)
+    assert int(err) == 0
+    return out
+
+
+def test_mesh_ingest_on_device(oracle):
+    """cvt_mesh_create does compaction, the face CSR and the bounds on the
+    device: the same arrays as the host restatement (main.cu:230-285)."""
+    from gpu_cvt_b200.engine import Mesh
+    from gpu_cvt_b200._lib import CvtError
+    rng = np.random.default_rng(5)
+    m = mg.icosphere(3)
+    # unreferenced vertices interleaved, faces shuffled
+    extra = rng.normal(size=(7, 3)).astype(np.float32) * 3
+    perm = rng.permutation(m.nV + 7)
+    Vall = np.vstack([m.V, extra])[perm]
+    inv = np.argsort(perm)
+    F = inv[m.F][rng.permutation(m.nF)].astype(np.int32)
+    M = Mesh(Vall, F)
+    Vc, Fc = mg.compact_mesh(Vall, F)
+    assert (M.nV, M.nF) == (Vc.shape[0], F.shape[0])
+    pV, pF, pN, poff, pfcs = M.device_arrays()
+    assert np.array_equal(_d2h(pV, Vc.size, np.float32).reshape(-1, 3), Vc)
+    assert np.array_equal(_d2h(pF, F.size, np.int32).reshape(-1, 3), Fc)
+    off, fcs = oracle.build_vf(M.nV, Fc)
+    assert np.array_equal(_d2h(poff, M.nV + 1, np.int32), off)
+    assert np.array_equal(_d2h(pfcs, 3 * M.nF, np.int32), fcs)
+    assert np.array_equal(_d2h(pN, Vc.size, np.float32).reshape(-1, 3), oracle.vertex_normals(Vc, Fc))
+    R = float(np.max(Vall.max(0) - Vall.min(0)))
+    assert M.R == np.float32(R)
+    a = Vc[Fc[:, 1]].astype(np.float64) - Vc[Fc[:, 0]]
+    b = Vc[Fc[:, 2]].astype(np.float64) - Vc[Fc[:, 0]]
+    area = 0.5 * np.linalg.norm(np.cross(a, b), axis=1).sum()
+    assert abs(M.area - area) <= 1e-6 * area
+    M.close()
+    bad = F.copy()
+    bad[3, 1] = Vall.shape[0]
+    with pytest.raises(CvtError):
+        Mesh(Vall, bad)
+    Vn = Vall.copy()
+    Vn[F[0, 0], 2] = np.nan
+    with pytest.raises(CvtError):
+        Mesh(Vn, F)
+    unused = int(np.setdiff1d(np.arange(Vall.shape[0]), F.ravel())[0])
+    Vn = Vall.copy()
+    Vn[unused] = np.nan          # no face uses it: accepted
+    Mesh(Vn, F).close()
+
+
+@pytest.mark.parametrize("name", ["icosphere", "torus", "superquadric"])
+def test_bvh_matches_recursive_build(oracle, name):
+    """The device's level-by-level build gives the reference's recursive
+    median-split tree node for node (evaluate.cuh:114-201)."""
+    from gpu_cvt_b200.engine import Mesh
+    if name == "icosphere":
+        m = mg.icosphere(4)
+    elif name == "torus":
+        m = mg.torus(1.0, 0.3, 120, 60, noise_sigma=0.002, seed=1)
+    else:
+        m = mg.superquadric(8.0, 30_000, jitter_frac=0.01, jitter=1e-3, seed=2)
+    M = Mesh(m.V, m.F)
+    nodes, tri = M.bvh()
+    en, et = oracle.bvh_build(m.V, m.F)
+    assert nodes.shape == en.shape and np.array_equal(tri, et)
+    for f in en.dtype.names:
+        assert np.array_equal(nodes[f], en[f]), f
+    M.close()
