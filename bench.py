@@ -120,17 +120,24 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-# algorithmic bytes per site and launch (fp32 positions, uint32 ids)
+# algorithmic bytes per site and launch (fp32 positions, uint32 ids; the
+# mesh arrays are gathered from L2 and not counted, like the neighbours'
+# positions, which are the sites' own positions read again)
 def knn_bytes_per_site(K):
     # own position 12 + neighbour ids written 4K + frame vertex id 4
     return 12 + 4 * K + 4
 
 
-def cell_bytes_per_site(K):
-    # position 12 + neighbour ids read 4K + frame vertex 4 + flags read 4
-    # (frozen, streak, tier, same) + vertex ids 20 + new position 12 + flags
-    # written 2
-    return 12 + 4 * K + 4 + 4 + 20 + 12 + 2
+def clip_bytes_per_site(K):
+    # position 12 + neighbour ids read 4K + frame vertex id 4 + its normal 12
+    # + frozen flag 1 + centroid written 12
+    return 12 + 4 * K + 4 + 12 + 1 + 12
+
+
+def proj_bytes_per_site(K):
+    # centroid 12 + position 12 + vertex ids written 20 + new position 12 +
+    # flags read 4 (frozen, same, streak, tier) and written 2
+    return 12 + 12 + 20 + 12 + 4 + 2
 
 
 def traffic_from_profiles(kernel_key):
@@ -294,14 +301,20 @@ def run_ours(args):
     reset()
     prof = eng.profile(iters, sp)
     K = p["k"]
-    groups = {"k_site_knn": (prof["knn"], knn_bytes_per_site(K)), "k_site_cell": (prof["cell"], cell_bytes_per_site(K))}
+    # the KNN kernel runs for the sites not yet frozen at the start of each
+    # iteration (frozen counts from the engine's per-iteration statistics)
+    newly = np.array([eng.stats(state["seg"], i)["newly_frozen"] for i in range(iters)], np.float64)
+    active_mean = float(np.mean(n - np.concatenate([[0.0], np.cumsum(newly)[:-1]])))
+    groups = {"k_site_knn": (prof["knn"], active_mean * knn_bytes_per_site(K)),
+              "k_site_clip": (prof["clip"], n * clip_bytes_per_site(K)),
+              "k_site_proj": (prof["proj"], n * proj_bytes_per_site(K))}
     dom = max(groups, key=lambda g: groups[g][0])
-    ms, bps = groups[dom]
+    ms, alg_bytes = groups[dom]
     peak, peak_kind = measured_peaks()
-    achieved = n * bps / (ms * 1e-3) / 1e9
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
     tr = traffic_from_profiles(dom)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": tr, "kernel": dom, "algorithmic_bytes_per_launch": n * bps,
+                "traffic": tr, "kernel": dom, "algorithmic_bytes_per_launch": alg_bytes,
                 "ms_per_launch": ms, "peak_source": peak_kind,
                 "stage_ms_per_iter": {k: round(v, 5) for k, v in prof.items()}}
 

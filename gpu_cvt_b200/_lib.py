@@ -64,6 +64,7 @@ _SIGS = {
     "cvt_hausdorff_to_mesh": [vp, vp, i32, vp, i32, vp, vp],
     "cvt_hausdorff_meshes": [vp, vp, vp, vp, vp, vp],
     "cvt_mesh_get_bvh": [vp, vp, i32, vp, i32, vp],
+    "cvt_release_cached_memory": [],
     "cvt_mesh_create": [vp, i32, vp, i32, vp],
     "cvt_set_vertex_cell_factor": [f32],
     "cvt_mesh_info": [vp, vp],

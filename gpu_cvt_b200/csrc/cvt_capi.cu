@@ -67,6 +67,65 @@ extern "C" const char* cvt_last_error(void) { return g_last_error.c_str(); }
 extern "C" int cvt_version(void) { return 1; }
 extern "C" unsigned long long cvt_launch_count(void) { return g_launches.load(); }
 
+// Device memory: one stream-ordered pool per device, owned by the library,
+// that keeps what is freed for the next allocation instead of handing it back
+// to the driver (release threshold = unlimited).  Meshes, engines and call
+// temporaries come and go without allocator calls into the driver once the
+// pool has grown to the working set; cvt_release_cached_memory trims it.
+static std::mutex g_pool_mu;
+static std::vector<cudaMemPool_t> g_pools;
+
+static cudaError_t lib_pool(cudaMemPool_t* out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  if ((int)g_pools.size() <= dev) g_pools.resize(dev + 1, nullptr);
+  if (!g_pools[dev]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+    uint64_t keep = ~0ull;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+      cudaMemPoolDestroy(pool);
+      return e;
+    }
+    g_pools[dev] = pool;
+  }
+  *out = g_pools[dev];
+  return cudaSuccess;
+}
+
+static cudaError_t dev_alloc(void** p, size_t bytes, cudaStream_t st) {
+  cudaMemPool_t pool;
+  cudaError_t e = lib_pool(&pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, std::max<size_t>(bytes, 16), pool, st);
+}
+
+// long-lived objects: allocated and freed on the legacy stream, then waited for
+static cudaError_t dev_alloc_sync(void** p, size_t bytes) {
+  cudaError_t e = dev_alloc(p, bytes, 0);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+  return e;
+}
+static void dev_free_sync(void* p) {
+  if (p) { cudaFreeAsync(p, 0); cudaStreamSynchronize(0); }
+}
+
+extern "C" cvt_status_t cvt_release_cached_memory(void) {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (cudaMemPool_t pool : g_pools)
+    if (pool) {
+      cudaError_t e = cudaMemPoolTrimTo(pool, 0);
+      if (e != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("cvt_release_cached_memory: ") + cudaGetErrorString(e));
+    }
+  return CVT_OK;
+}
+
 // stream-ordered scratch
 struct Scratch {
   cudaStream_t st;
@@ -74,7 +133,7 @@ struct Scratch {
   explicit Scratch(cudaStream_t s) : st(s) {}
   template <class X> cudaError_t get(X** p, size_t count) {
     void* q = nullptr;
-    cudaError_t e = cudaMallocAsync(&q, std::max<size_t>(count * sizeof(X), 16), st);
+    cudaError_t e = dev_alloc(&q, count * sizeof(X), st);
     if (e == cudaSuccess) { ptrs.push_back(q); *p = reinterpret_cast<X*>(q); }
     return e;
   }
@@ -368,7 +427,7 @@ struct Arena {
     size += (std::max<size_t>(count * sizeof(X), 16) + 255) & ~size_t(255);
   }
   cudaError_t commit(void** base) {
-    cudaError_t e = cudaMalloc(base, std::max<size_t>(size, 256));
+    cudaError_t e = dev_alloc_sync(base, std::max<size_t>(size, 256));
     if (e != cudaSuccess) { *base = nullptr; return e; }
     for (auto& s : slots) *s.first = static_cast<char*>(*base) + s.second;
     return cudaSuccess;
@@ -377,7 +436,8 @@ struct Arena {
 
 static void mesh_free(cvt_mesh* m) {
   if (!m) return;
-  cudaFree(m->arena); cudaFree(m->arena_grid); cudaFree(m->dcdf); cudaFree(m->dnodes); cudaFree(m->dtri);
+  dev_free_sync(m->arena); dev_free_sync(m->arena_grid); dev_free_sync(m->dcdf); dev_free_sync(m->dnodes);
+  dev_free_sync(m->dtri);
   delete m;
 }
 
@@ -402,10 +462,10 @@ static cvt_status_t mesh_ensure_bvh(cvt_mesh* m) {
   const int n_nodes = bvh_subtree_nodes(nF, leaf, memo);
   BVHNode* dn = nullptr;
   int* dt = nullptr;
-  cudaError_t e = cudaMalloc(&dn, sizeof(BVHNode) * (size_t)n_nodes);
-  if (e == cudaSuccess) e = cudaMalloc(&dt, sizeof(int) * (size_t)nF);
+  cudaError_t e = dev_alloc_sync(reinterpret_cast<void**>(&dn), sizeof(BVHNode) * (size_t)n_nodes);
+  if (e == cudaSuccess) e = dev_alloc_sync(reinterpret_cast<void**>(&dt), sizeof(int) * (size_t)nF);
   auto bail = [&](cudaError_t err) {
-    cudaFree(dn); cudaFree(dt);
+    dev_free_sync(dn); dev_free_sync(dt);
     return fail(err == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,
                 std::string("mesh BVH: ") + cudaGetErrorString(err));
   };
@@ -490,7 +550,7 @@ static cvt_status_t mesh_ensure_cdf(cvt_mesh* m) {
   const int nF = m->nF;
   cudaStream_t st = 0;
   double* d = nullptr;
-  cudaError_t e = cudaMalloc(&d, sizeof(double) * std::max(nF, 1));
+  cudaError_t e = dev_alloc_sync(reinterpret_cast<void**>(&d), sizeof(double) * std::max(nF, 1));
   if (e == cudaSuccess) {
     Scratch sc(st);
     double* fa;
@@ -506,7 +566,7 @@ static cvt_status_t mesh_ensure_cdf(cvt_mesh* m) {
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
-    cudaFree(d);
+    dev_free_sync(d);
     return fail(e == cudaErrorMemoryAllocation ? CVT_ERR_OOM : CVT_ERR_CUDA,
                 std::string("mesh area CDF: ") + cudaGetErrorString(e));
   }
@@ -544,7 +604,7 @@ static GridGeom surface_grid(const float lo[3], const float hi[3], double area, 
   return g;
 }
 
-static float g_vcell_factor = 1.5f;
+static float g_vcell_factor = 1.25f;   // swept 0.8-2.0 on the torus and rounded-box workloads
 
 extern "C" void cvt_set_vertex_cell_factor(float f) { if (f > 0.f) g_vcell_factor = f; }
 
@@ -897,6 +957,8 @@ struct cvt_engine {
   int* d_part = nullptr;
   int* d_stats = nullptr;
   int* d_ovf = nullptr;
+  int* d_far = nullptr;
+  void* d_cent = nullptr;
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   int graph_nodes = 0;
@@ -907,7 +969,7 @@ static void engine_free(cvt_engine* e) {
   if (!e) return;
   for (int k = 0; k < 2; ++k)
     if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
-  cudaFree(e->arena);
+  dev_free_sync(e->arena);
   delete e;
 }
 
@@ -974,6 +1036,8 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   ar.add(&e->d_part, (size_t)scan_blocks(max_cells) + 2);
   ar.add(&e->d_stats, (size_t)max_segments * kStatsRing * kStatsWords);
   ar.add(&e->d_ovf, ns + 1);
+  ar.add(&e->d_far, ns + 1);
+  ar.add(reinterpret_cast<char**>(&e->d_cent), tsz * 3 * ns);
   ECK(ar.commit(&e->arena));
   e->bytes = ar.size;
   ECK(cudaMemset(e->arena, 0, ar.size));
@@ -1098,7 +1162,7 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   a.knnv = e->d_knnv; a.nnv = e->d_nnv;
   a.frozen = e->d_frozen; a.streak = e->d_streak; a.tier = e->d_tier;
   a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
-  a.stats = e->d_stats; a.ovf = e->d_ovf; a.cent_dbg = nullptr; a.K = e->K;
+  a.stats = e->d_stats; a.ovf = e->d_ovf; a.far = e->d_far; a.cent = (T*)e->d_cent; a.K = e->K;
   return a;
 }
 
@@ -1108,8 +1172,9 @@ static void launch_site_knn(const EngineArgs<T>& a, int nsites, int, cudaStream_
   k_site_knn<T, KK><<<cdiv((long)nsites * 32, kKnnBlock), kKnnBlock, 0, st>>>(a);
 }
 
-// ev (optional, 5 events): recorded before the grid build, after it, after
-// the KNN kernel, after the cell kernel and after the bookkeeping kernels
+// ev (optional, 6 events): recorded before the grid build, after it, after
+// the KNN kernel, after the clip kernels, after the projection kernels and
+// after the bookkeeping kernel
 template <int PROF>
 static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t st, int* nlaunch, cudaEvent_t* ev) {
   using T = typename PT<PROF>::T;
@@ -1145,14 +1210,17 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   if (ev) CK(cudaEventRecord(ev[2], st));
   constexpr int BLK = sizeof(PP) == 8 ? kCellBlockD : kCellBlockF;
   const size_t smem = 2 * kCellCap * BLK * sizeof(V2<PP>);
-  k_site_cell<PROF, BLK, kCellCap><<<cdiv(ns, BLK), BLK, smem, st>>>(a, parity);
-  L++;
+  k_site_clip<PROF, BLK, kCellCap><<<cdiv(ns, BLK), BLK, smem, st>>>(a, parity);
+  k_clip_overflow<PROF><<<148, 64, 0, st>>>(a, parity);
+  L += 2;
   if (ev) CK(cudaEventRecord(ev[3], st));
-  k_cell_overflow<PROF><<<148, 64, 0, st>>>(a, parity);
-  L++;
-  k_seg_advance<<<1, 256, 0, st>>>(e->d_segs, e->d_active, e->max_seg, e->d_stats, e->d_ovf);
-  L++;
+  k_site_proj<PROF><<<cdiv(ns, 128), 128, 0, st>>>(a, parity);
+  k_site_far<PROF><<<148, 128, 0, st>>>(a, parity);
+  L += 2;
   if (ev) CK(cudaEventRecord(ev[4], st));
+  k_seg_advance<<<1, 256, 0, st>>>(e->d_segs, e->d_active, e->max_seg, e->d_stats, e->d_ovf, e->d_far);
+  L++;
+  if (ev) CK(cudaEventRecord(ev[5], st));
   CK(cudaGetLastError());
   *nlaunch = L;
   return CVT_OK;
@@ -1173,12 +1241,14 @@ static cvt_status_t set_smem_attrs(cvt_engine* e) {
   if (done[pr]) return CVT_OK;
   const int smemF = 2 * kCellCap * kCellBlockF * (int)sizeof(V2<float>);
   const int smemD = 2 * kCellCap * kCellBlockD * (int)sizeof(V2<double>);
-  if (pr == CVT_PROFILE_REF)
-    CK(cudaFuncSetAttribute(k_site_cell<PROF_REF, kCellBlockF, kCellCap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemF));
-  else if (pr == CVT_PROFILE_MIXED)
-    CK(cudaFuncSetAttribute(k_site_cell<PROF_MIXED, kCellBlockF, kCellCap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemF));
-  else
-    CK(cudaFuncSetAttribute(k_site_cell<PROF_FP64, kCellBlockD, kCellCap>, cudaFuncAttributeMaxDynamicSharedMemorySize, smemD));
+  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  if (pr == CVT_PROFILE_REF) {
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_REF, kCellBlockF, kCellCap>, attr, smemF));
+  } else if (pr == CVT_PROFILE_MIXED) {
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_MIXED, kCellBlockF, kCellCap>, attr, smemF));
+  } else {
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_FP64, kCellBlockD, kCellCap>, attr, smemD));
+  }
   done[pr] = true;
   return CVT_OK;
 }
@@ -1229,9 +1299,9 @@ extern "C" cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms,
   cudaStream_t st = S_(stream);
   cvt_status_t s = set_smem_attrs(e);
   if (s != CVT_OK) return s;
-  cudaEvent_t ev[5];
-  for (int k = 0; k < 5; ++k) CK(cudaEventCreate(&ev[k]));
-  double acc[4] = {0, 0, 0, 0};
+  cudaEvent_t ev[6];
+  for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
+  double acc[5] = {0, 0, 0, 0, 0};
   for (int it = 0; it < iters; ++it) {
     int nl = 0;
     s = enqueue_iteration(e, e->parity, st, &nl, ev);
@@ -1239,15 +1309,15 @@ extern "C" cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms,
     LAUNCHED(nl);
     e->parity ^= 1;
     for (int k = 0; k < e->max_seg; ++k) if (e->active[k] == 1) e->host_iters[k]++;
-    CK(cudaEventSynchronize(ev[4]));
-    for (int k = 0; k < 4; ++k) {
+    CK(cudaEventSynchronize(ev[5]));
+    for (int k = 0; k < 5; ++k) {
       float t = 0.f;
       CK(cudaEventElapsedTime(&t, ev[k], ev[k + 1]));
       acc[k] += t;
     }
   }
-  for (int k = 0; k < 5; ++k) cudaEventDestroy(ev[k]);
-  for (int k = 0; k < 4; ++k) ms[k] = (float)(acc[k] / iters);
+  for (int k = 0; k < 6; ++k) cudaEventDestroy(ev[k]);
+  for (int k = 0; k < 5; ++k) ms[k] = (float)(acc[k] / iters);
   return s;
 }
 

@@ -6,15 +6,19 @@
 //                (site_knn.cuh:79), restore the previous list for frozen
 //                sites (main.cu:678), nearest mesh vertex for the frame
 //                (main.cu:685-700)
-//   k_site_cell  per site: frame (site_normals.cuh:69), tangent-plane clip
-//                and centroid (2dClip.cuh:82), centroid -> 5 nearest
+//   k_site_clip  per site (one thread): frame (site_normals.cuh:69),
+//                tangent-plane clip and centroid (2dClip.cuh:82)
+//   k_clip_overflow  the same for the rare cells whose polygon outgrows
+//                the shared-memory buffer (exact 64-vertex cap)
+//   k_site_proj  per site (one thread): centroid -> 5 nearest
 //                vertices (main.cu:719-735, frozen sites keep theirs),
 //                one-ring projection (near_project.cuh:149), freeze test
 //                and apply (freezetest.cuh:155-212, 270-327, 451-466),
 //                tier assignment on the segment's first iteration
 //                (main.cu:640-667)
-//   k_cell_overflow  the same for the rare cells whose polygon
-//                outgrows the shared-memory buffer (exact 64-vertex cap)
+//   k_site_far   the sites whose centroid lies so far off the surface that
+//                the vertex grid search gave up: exact brute-force 5-NN by
+//                a block, then the rest of the step
 //   k_seg_advance  per-segment iteration counters / statistics slots
 // All sizes come from device memory, so the whole iteration is captured once
 // in a CUDA graph and relaunched while segments come and go.
@@ -29,7 +33,7 @@ constexpr int kKProj = 5;         // KPROJ (main.cu:394)
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
 constexpr int kKnnBlock = 128;    // threads per block of the site KNN kernel
 constexpr int kKnnBuf = 64;       // parked candidates per thread (shared memory)
-constexpr int kCellMinBlocks = 6;  // resident blocks per SM asked of k_site_cell (caps registers near 80;
+constexpr int kCellMinBlocks = 6;  // resident blocks per SM asked of k_site_clip (caps registers near 80;
                                    // its two polygon buffers take 32 KB per block)
 
 struct MeshDev {
@@ -88,7 +92,8 @@ template <class T> struct EngineArgs {
   int total_cells;
   int* stats;
   int* ovf;  // [0] = count, [1 + k] = overflowed site
-  T* cent_dbg;
+  int* far;  // [0] = count, [1 + k] = site whose vertex search was deferred
+  T* cent;   // centroid per site (3 values), k_site_clip -> k_site_proj
   int K;
 };
 
@@ -405,31 +410,28 @@ struct SiteOut {
   float disp2;
 };
 
+// Frame, clip and centroid of site g into a.cent; false when the polygon
+// outgrew the buffers (the site is then redone by k_clip_overflow).
 template <int PROF>
-__device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g,
+__device__ __forceinline__ bool site_clip(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g,
                                           PolyRef<typename PT<PROF>::PP> A, PolyRef<typename PT<PROF>::PP> B,
-                                          int cap, SiteOut& o) {
+                                          int cap) {
   using T = typename PT<PROF>::T;
   using PP = typename PT<PROF>::PP;
   const int s = __ldg(a.site_seg + g);
   const SegDev& sd = a.segs[s];
   const MeshDev& md = a.meshes[sd.mesh];
-  const int K = a.K;
   const T* __restrict__ S = a.S[parity];
-  const uint32_t* row = a.knn + (size_t)g * K;
-  const int i = g - sd.site_base;
   const bool fz = sd.mode != 0 && a.frozen[g];
   const V3<T> si = ld3(S, g);
-
   // frame from the nearest vertex normal (frozen sites: their kept vertex list)
   const int nn = fz ? a.knnv[(size_t)g * kKProj] : a.nnv[g];
   Frame<T> fr;
   if (nn < 0) fr = {{(T)1, (T)0, (T)0}, {(T)0, (T)1, (T)0}};
   else fr = frame_from_normal(V3<T>{(T)__ldg(md.N + 3 * nn), (T)__ldg(md.N + 3 * nn + 1), (T)__ldg(md.N + 3 * nn + 2)});
-
-  // clip + centroid
   PolyRef<PP> cur = A, nxt = B;
-  const int np = clip_cell<PROF>(S, sd.site_base, sd.n_sites, si, row, K, fr, md.R, cur, nxt, cap, !fz);
+  const int np = clip_cell<PROF>(S, sd.site_base, sd.n_sites, si, a.knn + (size_t)g * a.K, a.K, fr, md.R, cur, nxt,
+                                 cap, !fz);
   if (np < 0) return false;
   const V2<PP> c2 = poly_centroid<PP>(cur, np, PROF == PROF_MIXED);
   V3<T> cent;
@@ -440,22 +442,51 @@ __device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>
     cent = {si.x + fmaT(fr.u.x, cx, fr.v.x * cy), si.y + fmaT(fr.u.y, cx, fr.v.y * cy),
             si.z + fmaT(fr.u.z, cx, fr.v.z * cy)};
   }
-  if (a.cent_dbg) st3(a.cent_dbg, g, cent);
+  st3(a.cent, g, cent);
+  return true;
+}
 
-  // centroid -> nearest mesh vertices (frozen sites keep theirs)
-  int* kv = a.knnv + (size_t)g * kKProj;
-  int knnv[kKProj];
-  if (!fz) {
-    TopK<T, kKProj> top;
-    const int skip = (sd.mode == 0 && sd.ex_quirk) ? i : -1;
-    grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, cent, top,
-                               [skip](uint32_t id) { return (int)id != skip; });
-#pragma unroll
-    for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
-  } else {
-#pragma unroll
-    for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];
+template <int PROF, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK, kCellMinBlocks) k_site_clip(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  using PP = typename PT<PROF>::PP;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  V2<PP>* sm = reinterpret_cast<V2<PP>*>(smem_raw);
+  PolyRef<PP> A{sm + threadIdx.x, BLOCK}, B{sm + CAP * BLOCK + threadIdx.x, BLOCK};
+  const int t = blockIdx.x * BLOCK + threadIdx.x;
+  const int n_grid = __ldg(a.cell_start + a.total_cells);
+  if (t < n_grid) {
+    const int g = (int)a.sorted[t].id;
+    if (!site_clip<PROF>(a, parity, g, A, B, CAP)) {
+      const int k = atomicAdd(a.ovf, 1);
+      a.ovf[1 + k] = g;
+    }
   }
+}
+
+template <int PROF>
+__global__ void __launch_bounds__(64) k_clip_overflow(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  using PP = typename PT<PROF>::PP;
+  V2<PP> buf[2][kFallbackCap];
+  const int n = *(volatile int*)a.ovf;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
+    site_clip<PROF>(a, parity, a.ovf[1 + k], PolyRef<PP>{buf[0], 1}, PolyRef<PP>{buf[1], 1}, kFallbackCap);
+}
+
+// Projection, tiers and the freeze test of site g, given the centroid in
+// a.cent and its 5 nearest vertices knnv.
+template <int PROF>
+__device__ __forceinline__ void site_finish(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g,
+                                            const int (&knnv)[kKProj], SiteOut& o) {
+  using T = typename PT<PROF>::T;
+  const int s = __ldg(a.site_seg + g);
+  const SegDev& sd = a.segs[s];
+  const MeshDev& md = a.meshes[sd.mesh];
+  const int K = a.K;
+  const uint32_t* row = a.knn + (size_t)g * K;
+  const int i = g - sd.site_base;
+  const bool fz = sd.mode != 0 && a.frozen[g];
+  const V3<T> si = ld3(a.S[parity], g);
+  const V3<T> cent = ld3((const T*)a.cent, g);
 
   // projection
   V3<T> sn;
@@ -504,7 +535,51 @@ __device__ __forceinline__ bool site_step(const EngineArgs<typename PT<PROF>::T>
       if (cand && !a.frozen[g]) { a.frozen[g] = 1; o.newly = 1; }
     }
   }
+}
+
+// Rings the per-thread centroid -> vertex search may visit before the site
+// is handed to k_site_far (a centroid far off the surface, e.g. of a cell
+// that the neighbours leave almost unbounded in the first iteration).
+constexpr int kVertexRingLimit = 4;
+
+// Everything after the centroid; false when the 5-NN search was deferred
+// (the site is then listed in a.far and finished by k_site_far).
+template <int PROF>
+__device__ __forceinline__ bool site_proj(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g, SiteOut& o) {
+  using T = typename PT<PROF>::T;
+  const int s = __ldg(a.site_seg + g);
+  const SegDev& sd = a.segs[s];
+  const MeshDev& md = a.meshes[sd.mesh];
+  const bool fz = sd.mode != 0 && a.frozen[g];
+  // centroid -> nearest mesh vertices (frozen sites keep theirs)
+  int* kv = a.knnv + (size_t)g * kKProj;
+  int knnv[kKProj];
+  if (!fz) {
+    const int skip = (sd.mode == 0 && sd.ex_quirk) ? g - sd.site_base : -1;
+    TopK<T, kKProj> top;
+    if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, ld3((const T*)a.cent, g), top,
+                                    [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
+      const int k = atomicAdd(a.far, 1);
+      a.far[1 + k] = g;
+      return false;
+    }
+#pragma unroll
+    for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];
+  }
+  site_finish<PROF>(a, parity, g, knnv, o);
   return true;
+}
+
+__device__ __forceinline__ void stats_atomic(int* stats, const SegDev* segs, const SiteOut& o) {
+  int* sl = stats + ((size_t)o.seg * kStatsRing + (segs[o.seg].iter % kStatsRing)) * kStatsWords;
+  if (o.same) atomicAdd(sl + 0, 1);
+  if (o.low) atomicAdd(sl + 1, 1);
+  if (o.both) atomicAdd(sl + 2, 1);
+  if (o.newly) atomicAdd(sl + 3, 1);
+  atomicMax(reinterpret_cast<unsigned*>(sl + 4), __float_as_uint(o.disp2));
 }
 
 __device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, const SiteOut& o) {
@@ -529,48 +604,61 @@ __device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, cons
   }
 }
 
-template <int PROF, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK, kCellMinBlocks) k_site_cell(EngineArgs<typename PT<PROF>::T> a, int parity) {
-  using PP = typename PT<PROF>::PP;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  V2<PP>* sm = reinterpret_cast<V2<PP>*>(smem_raw);
-  PolyRef<PP> A{sm + threadIdx.x, BLOCK}, B{sm + CAP * BLOCK + threadIdx.x, BLOCK};
-  const int t = blockIdx.x * BLOCK + threadIdx.x;
+template <int PROF>
+__global__ void __launch_bounds__(128) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  const int t = blockIdx.x * 128 + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   SiteOut o{-1, 0, 0, 0, 0, 0.f};
-  if (t < n_grid) {
-    const int g = (int)a.sorted[t].id;
-    if (!site_step<PROF>(a, parity, g, A, B, CAP, o)) {
-      o = SiteOut{-1, 0, 0, 0, 0, 0.f};
-      int k = atomicAdd(a.ovf, 1);
-      a.ovf[1 + k] = g;
-    }
-  }
+  if (t < n_grid) site_proj<PROF>(a, parity, (int)a.sorted[t].id, o);
   stats_flush(a.stats, a.segs, o);
 }
 
+// Deferred sites (a.far): one block per site finds the 5 nearest mesh
+// vertices of the centroid by scanning all of them (each thread every 128th
+// vertex, then a merge of the 128 lists by thread 0; exact, the keys are
+// unique), then thread 0 finishes the site.
 template <int PROF>
-__global__ void __launch_bounds__(64) k_cell_overflow(EngineArgs<typename PT<PROF>::T> a, int parity) {
-  using PP = typename PT<PROF>::PP;
-  V2<PP> buf[2][kFallbackCap];
-  const int n = *(volatile int*)a.ovf;
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int g = a.ovf[1 + k];
-    SiteOut o{-1, 0, 0, 0, 0, 0.f};
-    site_step<PROF>(a, parity, g, PolyRef<PP>{buf[0], 1}, PolyRef<PP>{buf[1], 1}, kFallbackCap, o);
-    int* sl = a.stats + ((size_t)o.seg * kStatsRing + (a.segs[o.seg].iter % kStatsRing)) * kStatsWords;
-    if (o.same) atomicAdd(sl + 0, 1);
-    if (o.low) atomicAdd(sl + 1, 1);
-    if (o.both) atomicAdd(sl + 2, 1);
-    if (o.newly) atomicAdd(sl + 3, 1);
-    atomicMax(reinterpret_cast<unsigned*>(sl + 4), __float_as_uint(o.disp2));
+__global__ void __launch_bounds__(128) k_site_far(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  using T = typename PT<PROF>::T;
+  using Key = typename KeyOps<T>::Key;
+  __shared__ Key keys[128 * kKProj];
+  const int n = *(volatile int*)a.far;
+  for (int k = blockIdx.x; k < n; k += gridDim.x) {
+    const int g = a.far[1 + k];
+    const int s = __ldg(a.site_seg + g);
+    const SegDev& sd = a.segs[s];
+    const MeshDev& md = a.meshes[sd.mesh];
+    const int skip = (sd.mode == 0 && sd.ex_quirk) ? g - sd.site_base : -1;
+    const V3<T> q = ld3((const T*)a.cent, g);
+    TopK<T, kKProj> top;
+    for (int v = threadIdx.x; v < md.nV; v += 128) {
+      if (v == skip) continue;
+      const V3<T> p{(T)__ldg(md.V + 3 * v), (T)__ldg(md.V + 3 * v + 1), (T)__ldg(md.V + 3 * v + 2)};
+      const T d = dist2(p, q);
+      if (d <= top.worst_d()) top.insert(KeyOps<T>::make(d, (uint32_t)v));
+    }
+#pragma unroll
+    for (int j = 0; j < kKProj; ++j) keys[threadIdx.x * kKProj + j] = top.k[j];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      TopK<T, kKProj> all;
+      for (int j = 0; j < 128 * kKProj; ++j) all.insert(keys[j]);
+      int knnv[kKProj];
+      int* kv = a.knnv + (size_t)g * kKProj;
+#pragma unroll
+      for (int j = 0; j < kKProj; ++j) { knnv[j] = (int)KeyOps<T>::idx(all.k[j]); kv[j] = knnv[j]; }
+      SiteOut o{-1, 0, 0, 0, 0, 0.f};
+      site_finish<PROF>(a, parity, g, knnv, o);
+      stats_atomic(a.stats, a.segs, o);
+    }
+    __syncthreads();
   }
 }
 
 // iteration bookkeeping: advance active segments, clear their next stats
 // slot, apply each segment's stop rule (a stopped segment is no longer
 // gridded or iterated: active = 2), reset the overflow list
-__global__ void k_seg_advance(SegDev* segs, int* active, int nseg, int* stats, int* ovf) {
+__global__ void k_seg_advance(SegDev* segs, int* active, int nseg, int* stats, int* ovf, int* far) {
   for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
     if (active[s] != 1) continue;
     int it = segs[s].iter;
@@ -585,7 +673,7 @@ __global__ void k_seg_advance(SegDev* segs, int* active, int nseg, int* stats, i
     const int cap = segs[s].stop_iters;
     if ((lim >= 0.f && d2 <= lim) || (cap > 0 && nx >= cap)) active[s] = 2;
   }
-  if (threadIdx.x == 0) ovf[0] = 0;
+  if (threadIdx.x == 0) { ovf[0] = 0; far[0] = 0; }
 }
 
 }  // namespace cvt

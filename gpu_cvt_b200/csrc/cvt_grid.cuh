@@ -97,11 +97,14 @@ template <class T, int KK> struct TopK {
 
 // Exact KK-nearest search of q among the points of one grid.  accept(id)
 // filters candidates (used for the vertex-index exclusion quirk).
+// With rlim > 0 the search gives up (returns false, top incomplete) when it
+// has not finished after rlim rings: a query far from every point would
+// otherwise visit the whole grid, one cell at a time.
 template <class T, class PT, int KK, class Accept>
-__device__ __forceinline__ void grid_knn(const GridGeom& g, const int* __restrict__ cell_start,
+__device__ __forceinline__ bool grid_knn(const GridGeom& g, const int* __restrict__ cell_start,
                                          const Pt4<PT>* __restrict__ pts, V3<T> q, TopK<T, KK>& top,
-                                         Accept accept) {
-  if (!finite3(q)) return;
+                                         Accept accept, int rlim = 0) {
+  if (!finite3(q)) return true;
   const int cx = grid_coord(g, q.x, 0), cy = grid_coord(g, q.y, 1), cz = grid_coord(g, q.z, 2);
   const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
   const float slack = 1e-3f * g.h;
@@ -141,7 +144,9 @@ __device__ __forceinline__ void grid_knn(const GridGeom& g, const int* __restric
     if (isinf(m)) break;
     m -= slack;
     if (top.full() && m > 0.f && (double)top.worst_d() < (double)m * (double)m) break;
+    if (r == rlim) return false;
   }
+  return true;
 }
 
 // Same search with buffered insertion.  Candidates with d <= thr are parked

@@ -188,10 +188,13 @@ class Engine:
         return v.value
 
     def profile(self, iters: int, stream=None):
-        """Per-kernel-group ms per iteration: grid, knn, cell, tail."""
-        ms = (C.c_float * 4)()
+        """Per-kernel-group ms per iteration: grid, knn, clip, proj, tail, and
+        cell = clip + proj."""
+        ms = (C.c_float * 5)()
         call("cvt_engine_profile", self.handle, int(iters), ms, stream)
-        return dict(zip(("grid", "knn", "cell", "tail"), [float(x) for x in ms]))
+        d = dict(zip(("grid", "knn", "clip", "proj", "tail"), [float(x) for x in ms]))
+        d["cell"] = d["clip"] + d["proj"]
+        return d
 
     def evaluate(self, seg: int, stream=None) -> dict:
         """Dual-triangle mesh of the current sites: quality and one-sided

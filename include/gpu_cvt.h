@@ -166,6 +166,12 @@ cvt_status_t cvt_extract_faces(const float* S, const float* U, const float* V, c
  * theta_lt_30_pct, theta_gt_90_pct.  Synchronous. */
 cvt_status_t cvt_quality(const float* V, const int* F, int nF, float* out, void* stream);
 
+/* Device memory of meshes, engines and call temporaries comes from one
+ * stream-ordered pool per device that keeps freed memory for reuse, so calls
+ * after the first allocate nothing from the driver.  This hands the cached,
+ * unused part back (e.g. before another library needs the HBM). */
+cvt_status_t cvt_release_cached_memory(void);
+
 /* ======================================================================
  * Resident meshes (main.cu:421-542: load, compact, normals, VF CSR, BVH)
  * ==================================================================== */
@@ -186,7 +192,7 @@ typedef struct {
  * thread-safe). */
 cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, int nF, cvt_mesh_t* out);
 /* Cell edge of the vertex grid of meshes created afterwards, in units of the
- * radius expected to hold 6 vertices (default 1.5; a tuning knob only). */
+ * radius expected to hold 6 vertices (default 1.25; a tuning knob only). */
 void cvt_set_vertex_cell_factor(float f);
 cvt_status_t cvt_mesh_info(cvt_mesh_t m, cvt_mesh_info_t* info);
 /* Device views of the compacted mesh (valid until cvt_mesh_destroy). */
@@ -267,8 +273,9 @@ cvt_status_t cvt_engine_get_stats(cvt_engine_t e, int seg_id, int iter, cvt_iter
 /* Iterations the segment has completed (host-side count). */
 cvt_status_t cvt_engine_segment_iters(cvt_engine_t e, int seg_id, int* iters);
 /* Run `iters` iterations without a graph, timing each kernel group with CUDA
- * events on `stream`; ms[4] = average ms per iteration of {grid build, site
- * KNN kernel, per-site cell kernel, fallback + bookkeeping}.  Synchronous. */
+ * events on `stream`; ms[5] = average ms per iteration of {grid build, site
+ * KNN kernel, clip kernel (+ overflow fallback), projection kernel (+ far
+ * fallback), bookkeeping}.  Synchronous. */
 cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms, void* stream);
 /* The evaluation of main.cu:883-1040 for one segment: frames of the current
  * sites, dual triangles with the last iteration's neighbour lists, quality,

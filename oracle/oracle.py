@@ -18,6 +18,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 
 P_REF, P_MIXED, P_FP64 = 0, 1, 2
+PROFILES = {"ref": P_REF, "mixed": P_MIXED, "fp64": P_FP64}
 
 
 def build(force: bool = False) -> str:

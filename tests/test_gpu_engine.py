@@ -84,6 +84,28 @@ def test_mixed_profile_bitexact(eng, oracle, small_torus):
     assert np.array_equal(S, r["S"]) and np.array_equal(counts, r["counts"])
 
 
+@pytest.mark.parametrize("mode,profile", [(0, "ref"), (1, "mixed")])
+def test_far_centroids_bitexact(eng, oracle, mode, profile):
+    """Sites cut off from the rest (a cap of 300 plus three lone sites) get
+    cells that reach the clip square, so their centroids lie far off the
+    sphere; the per-thread vertex search gives up on them and the deferred
+    brute-force path finishes them, with the oracle's result."""
+    m = mg.icosphere(5)
+    S = mg.sample_sites(m.V, m.F, 3000, seed=3)
+    lone = np.array([[1, 0, 0], [0, -1, 0], [-0.6, 0.6, -0.52915]], np.float32)
+    lone /= np.linalg.norm(lone, axis=1, keepdims=True)
+    S0 = np.vstack([S[S[:, 2] > 0.6][:300], lone]).astype(np.float32)
+    r1 = oracle.lloyd_run(m.V, m.F, S0, 20, mode, 1, profile=oracle.PROFILES[profile])
+    c = r1["cent"][-3:].astype(np.float64)
+    far = np.sqrt(((c[:, None, :] - m.V[None, :, :].astype(np.float64)) ** 2).sum(-1)).min(1)
+    assert far.min() > 0.25          # several vertex-grid cells (about 0.06) away
+    S, st, counts = run_engine(eng, m, S0, 20, mode, 6, profile=profile)
+    r = oracle.lloyd_run(m.V, m.F, S0, 20, mode, 6, profile=oracle.PROFILES[profile])
+    assert np.array_equal(S, r["S"])
+    assert np.array_equal(st["knnv"], r["knnv"])
+    assert np.array_equal(counts, r["counts"])
+
+
 def test_fp64_profile_matches_fp64_oracle(eng, oracle, c1):
     m, S0 = c1
     S, st, counts = run_engine(eng, m, S0, 20, 0, 10, profile="fp64")

@@ -345,3 +345,18 @@ def test_bvh_matches_recursive_build(oracle, name):
     for f in en.dtype.names:
         assert np.array_equal(nodes[f], en[f]), f
     M.close()
+
+
+def test_memory_pool_reuse_and_release():
+    """Meshes and engines freed go back to the library's pool and are reused;
+    cvt_release_cached_memory hands the unused part back; work continues."""
+    from gpu_cvt_b200 import engine as E
+    from gpu_cvt_b200._lib import call
+    m = mg.icosphere(3)
+    S0 = mg.sample_sites(m.V, m.F, 500, seed=2)
+    out = []
+    for rep in range(3):
+        out.append(E.remesh(m.V, m.F, S0, k=20, mode=0, iters=5))
+        if rep == 1:
+            call("cvt_release_cached_memory")
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[1], out[2])
