@@ -1183,11 +1183,11 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   const int ns = e->max_sites;
   int L = 0;
   if (ev) CK(cudaEventRecord(ev[0], st));
-  CK(cudaMemsetAsync(e->d_cell_count, 0, sizeof(int) * e->max_cells, st));
+  // d_cell_count is all zero here: set at creation, cleared by the scan
   k_grid_count<T><<<cdiv(ns, 256), 256, 0, st>>>(ns, (const T*)e->d_S[parity], SegGrid{e->d_geom, e->d_site_seg, e->d_active},
                                                  e->d_cell_count, e->d_cellrank);
   L++;
-  launch_exclusive_scan(e->max_cells, e->d_cell_count, e->d_part, e->d_cell_start, st);
+  launch_exclusive_scan(e->max_cells, e->d_cell_count, e->d_part, e->d_cell_start, st, true);
   L += 3;
   k_grid_scatter<T><<<cdiv(ns, 256), 256, 0, st>>>(ns, (const T*)e->d_S[parity], e->d_cellrank, e->d_cell_start,
                                                    (Pt4<T>*)e->d_sorted);

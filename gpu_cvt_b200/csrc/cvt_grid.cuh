@@ -535,14 +535,21 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_partials(int nb, int* __r
   if (threadIdx.x == 0) part[nb] = carry;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_apply(int n, const int* __restrict__ in, const int* __restrict__ part,
-                                                             int* __restrict__ out) {
+// clear_in: the input is zeroed once read (the engine's cell counts are then
+// ready for the next iteration's counting without a memset)
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(int n, int* __restrict__ in, const int* __restrict__ part,
+                                                             int* __restrict__ out, int clear_in) {
   __shared__ int sw[33];
   int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
   int v[kScanItems];
   int s = 0;
 #pragma unroll
   for (int k = 0; k < kScanItems; ++k) { v[k] = (base + k < n) ? in[base + k] : 0; s += v[k]; }
+  if (clear_in) {
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k)
+      if (base + k < n) in[base + k] = 0;
+  }
   int total;
   int off = block_exclusive_scan(s, sw, total) + part[blockIdx.x];
 #pragma unroll
@@ -556,12 +563,12 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(int n, const int* _
 inline int scan_blocks(int n) { return (n + kScanTile - 1) / kScanTile; }
 
 // part must hold scan_blocks(n) + 1 ints
-inline void launch_exclusive_scan(int n, const int* in, int* part, int* out, cudaStream_t st) {
+inline void launch_exclusive_scan(int n, int* in, int* part, int* out, cudaStream_t st, bool clear_in = false) {
   int nb = scan_blocks(n);
   if (nb < 1) nb = 1;
   k_scan_reduce<<<nb, kScanThreads, 0, st>>>(n, in, part);
   k_scan_partials<<<1, kScanThreads, 0, st>>>(nb, part);
-  k_scan_apply<<<nb, kScanThreads, 0, st>>>(n, in, part, out);
+  k_scan_apply<<<nb, kScanThreads, 0, st>>>(n, in, part, out, clear_in ? 1 : 0);
 }
 
 }  // namespace cvt
