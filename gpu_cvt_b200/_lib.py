@@ -29,7 +29,8 @@ class MeshInfo(C.Structure):
 
 class Params(C.Structure):
     _fields_ = [("k", i32), ("mode", i32), ("profile", i32), ("kproj", i32), ("ex_quirk", i32),
-                ("cell_factor", f32), ("use_graph", i32)]
+                ("cell_factor", f32), ("use_graph", i32), ("knn_block", i32), ("clip_block", i32),
+                ("proj_block", i32)]
 
 
 class EvalOut(C.Structure):
@@ -65,6 +66,7 @@ _SIGS = {
     "cvt_hausdorff_meshes": [vp, vp, vp, vp, vp, vp],
     "cvt_mesh_get_bvh": [vp, vp, i32, vp, i32, vp],
     "cvt_release_cached_memory": [],
+    "cvt_autotune": [vp, vp, i32, i32, vp, vp],
     "cvt_mesh_create": [vp, i32, vp, i32, vp],
     "cvt_set_vertex_cell_factor": [f32],
     "cvt_mesh_info": [vp, vp],

@@ -873,6 +873,28 @@ extern "C" void cvt_params_default(cvt_params_t* p) {
   p->ex_quirk = 1;
   p->cell_factor = 1.1f;
   p->use_graph = 1;
+  p->knn_block = p->clip_block = p->proj_block = 0;
+}
+
+// launch shapes the tiles may take (cvt_params_t knn_block / clip_block /
+// proj_block); 0 in the params selects the first
+static const int kKnnBlocks[] = {128, 64, 256};
+static const int kClipBlocksF[] = {128, 64};
+static const int kClipBlocksD[] = {64, 32};
+static const int kProjBlocks[] = {128, 64, 256};
+
+static bool in_set(int v, const int* set, int n) {
+  for (int i = 0; i < n; ++i) if (set[i] == v) return true;
+  return false;
+}
+// fill 0 fields with the defaults; false if a field holds an unsupported shape
+static bool resolve_tiles(cvt_params_t* p) {
+  const bool f64 = p->profile == CVT_PROFILE_FP64;
+  const int* clip = f64 ? kClipBlocksD : kClipBlocksF;
+  if (p->knn_block == 0) p->knn_block = kKnnBlocks[0];
+  if (p->clip_block == 0) p->clip_block = clip[0];
+  if (p->proj_block == 0) p->proj_block = kProjBlocks[0];
+  return in_set(p->knn_block, kKnnBlocks, 3) && in_set(p->clip_block, clip, 2) && in_set(p->proj_block, kProjBlocks, 3);
 }
 
 // first-fit interval allocator over [0, cap)
@@ -983,8 +1005,12 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   if (p->kproj != kKProj) return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: kproj must be 5");
   if (p->mode < 0 || p->mode > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: mode must be 0, 1 or 2");
   if (p->profile < 0 || p->profile > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: profile");
+  cvt_params_t q = *p;
+  if (!resolve_tiles(&q))
+    return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: knn_block / proj_block must be 64, 128 or 256, clip_block "
+                                     "64 or 128 (FP64 profile: 32 or 64)");
   cvt_engine* e = new cvt_engine();
-  e->p = *p;
+  e->p = q;
   e->K = p->k;
   e->f64 = p->profile == CVT_PROFILE_FP64;
   e->max_seg = max_segments;
@@ -1150,8 +1176,6 @@ extern "C" cvt_status_t cvt_engine_remove_segment(cvt_engine_t e, int s) {
   return CVT_OK;
 }
 
-constexpr int kCellBlockF = 128;
-constexpr int kCellBlockD = 64;
 constexpr int kCellCap = 16;
 
 template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
@@ -1167,10 +1191,34 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
 }
 
 template <class T, int KK>
-static void launch_site_knn(const EngineArgs<T>& a, int nsites, int, cudaStream_t st) {
+static void launch_site_knn(const EngineArgs<T>& a, int nsites, int bs, cudaStream_t st) {
   // one warp per site
-  k_site_knn<T, KK><<<cdiv((long)nsites * 32, kKnnBlock), kKnnBlock, 0, st>>>(a);
+  const int nb = cdiv((long)nsites * 32, bs);
+  if (bs == 64) k_site_knn<T, KK, 64><<<nb, 64, 0, st>>>(a);
+  else if (bs == 256) k_site_knn<T, KK, 256><<<nb, 256, 0, st>>>(a);
+  else k_site_knn<T, KK, 128><<<nb, 128, 0, st>>>(a);
 }
+
+template <int PROF>
+static void launch_site_clip(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, cudaStream_t st) {
+  using PP = typename PT<PROF>::PP;
+  const size_t smem = 2 * kCellCap * (size_t)bs * sizeof(V2<PP>);
+  if (sizeof(PP) == 8) {
+    if (bs == 32) k_site_clip<PROF, 32, kCellCap><<<cdiv(ns, 32), 32, smem, st>>>(a, parity);
+    else k_site_clip<PROF, 64, kCellCap><<<cdiv(ns, 64), 64, smem, st>>>(a, parity);
+  } else {
+    if (bs == 64) k_site_clip<PROF, 64, kCellCap><<<cdiv(ns, 64), 64, smem, st>>>(a, parity);
+    else k_site_clip<PROF, 128, kCellCap><<<cdiv(ns, 128), 128, smem, st>>>(a, parity);
+  }
+}
+
+template <int PROF>
+static void launch_site_proj(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, cudaStream_t st) {
+  if (bs == 64) k_site_proj<PROF, 64><<<cdiv(ns, 64), 64, 0, st>>>(a, parity);
+  else if (bs == 256) k_site_proj<PROF, 256><<<cdiv(ns, 256), 256, 0, st>>>(a, parity);
+  else k_site_proj<PROF, 128><<<cdiv(ns, 128), 128, 0, st>>>(a, parity);
+}
+
 
 // ev (optional, 6 events): recorded before the grid build, after it, after
 // the KNN kernel, after the clip kernels, after the projection kernels and
@@ -1199,22 +1247,20 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   L++;
   if (ev) CK(cudaEventRecord(ev[1], st));
   switch (e->K) {
-    case 8: launch_site_knn<T, 9>(a, ns, parity, st); break;
-    case 12: launch_site_knn<T, 13>(a, ns, parity, st); break;
-    case 16: launch_site_knn<T, 17>(a, ns, parity, st); break;
-    case 20: launch_site_knn<T, 21>(a, ns, parity, st); break;
-    case 24: launch_site_knn<T, 25>(a, ns, parity, st); break;
-    default: launch_site_knn<T, 33>(a, ns, parity, st); break;
+    case 8: launch_site_knn<T, 9>(a, ns, e->p.knn_block, st); break;
+    case 12: launch_site_knn<T, 13>(a, ns, e->p.knn_block, st); break;
+    case 16: launch_site_knn<T, 17>(a, ns, e->p.knn_block, st); break;
+    case 20: launch_site_knn<T, 21>(a, ns, e->p.knn_block, st); break;
+    case 24: launch_site_knn<T, 25>(a, ns, e->p.knn_block, st); break;
+    default: launch_site_knn<T, 33>(a, ns, e->p.knn_block, st); break;
   }
   L++;
   if (ev) CK(cudaEventRecord(ev[2], st));
-  constexpr int BLK = sizeof(PP) == 8 ? kCellBlockD : kCellBlockF;
-  const size_t smem = 2 * kCellCap * BLK * sizeof(V2<PP>);
-  k_site_clip<PROF, BLK, kCellCap><<<cdiv(ns, BLK), BLK, smem, st>>>(a, parity);
+  launch_site_clip<PROF>(a, parity, ns, e->p.clip_block, st);
   k_clip_overflow<PROF><<<148, 64, 0, st>>>(a, parity);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[3], st));
-  k_site_proj<PROF><<<cdiv(ns, 128), 128, 0, st>>>(a, parity);
+  launch_site_proj<PROF>(a, parity, ns, e->p.proj_block, st);
   k_site_far<PROF><<<148, 128, 0, st>>>(a, parity);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[4], st));
@@ -1239,15 +1285,18 @@ static cvt_status_t set_smem_attrs(cvt_engine* e) {
   static bool done[3] = {false, false, false};
   int pr = e->p.profile;
   if (done[pr]) return CVT_OK;
-  const int smemF = 2 * kCellCap * kCellBlockF * (int)sizeof(V2<float>);
-  const int smemD = 2 * kCellCap * kCellBlockD * (int)sizeof(V2<double>);
   const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
+  const int f128 = 2 * kCellCap * 128 * (int)sizeof(V2<float>), f64 = f128 / 2;
+  const int d64 = 2 * kCellCap * 64 * (int)sizeof(V2<double>), d32 = d64 / 2;
   if (pr == CVT_PROFILE_REF) {
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_REF, kCellBlockF, kCellCap>, attr, smemF));
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_REF, 128, kCellCap>, attr, f128));
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_REF, 64, kCellCap>, attr, f64));
   } else if (pr == CVT_PROFILE_MIXED) {
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_MIXED, kCellBlockF, kCellCap>, attr, smemF));
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_MIXED, 128, kCellCap>, attr, f128));
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_MIXED, 64, kCellCap>, attr, f64));
   } else {
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_FP64, kCellBlockD, kCellCap>, attr, smemD));
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_FP64, 64, kCellCap>, attr, d64));
+    CK(cudaFuncSetAttribute(k_site_clip<PROF_FP64, 32, kCellCap>, attr, d32));
   }
   done[pr] = true;
   return CVT_OK;
@@ -1422,6 +1471,51 @@ extern "C" cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n) {
 static void engine_caps(const cvt_mesh* m, int n, const cvt_params_t* p, int* cells) {
   GridGeom g = surface_grid(m->lo, m->hi, m->area, n, (double)(p->k + 1), p->cell_factor, 4L * n + 64);
   *cells = g.ncell + 1;
+}
+
+// Three timed passes over the same fresh copy of the sites: pass r runs
+// knn/proj candidate r and clip candidate min(r, 1) (candidate 0 = default).  The kernels are timed
+// separately by cvt_engine_profile, so one pass measures one candidate of
+// each; results do not depend on the shapes.
+extern "C" cvt_status_t cvt_autotune(cvt_mesh_t mesh, const float* sites, int n_sites, int iters, cvt_params_t* p,
+                                     float* ms_out) {
+  if (!mesh || !sites || n_sites < 1 || iters < 2 || !p) return fail(CVT_ERR_INVALID, "cvt_autotune: bad arguments");
+  cvt_params_t q = *p;
+  if (!resolve_tiles(&q)) return fail(CVT_ERR_UNSUPPORTED, "cvt_autotune: unsupported launch shape in params");
+  const int* clip = q.profile == CVT_PROFILE_FP64 ? kClipBlocksD : kClipBlocksF;
+  int cells = 0;
+  engine_caps(mesh, n_sites, &q, &cells);
+  cvt_engine_t e = nullptr;
+  cvt_status_t s = cvt_engine_create(&q, 1, n_sites, cells, &e);
+  if (s != CVT_OK) return s;
+  // pass 0 runs the default shapes; another shape replaces a default only
+  // when it is more than 3 % faster (closer calls are within the noise of a
+  // few iterations and the default is the one measured over whole runs)
+  float best[3] = {1e30f, 1e30f, 1e30f};
+  int pick[3] = {q.knn_block, q.clip_block, q.proj_block};
+  auto better = [](float t, float cur, bool first) { return first ? true : t < 0.97f * cur; };
+  for (int r = 0; r < 3 && s == CVT_OK; ++r) {
+    e->p.knn_block = kKnnBlocks[r];
+    e->p.clip_block = clip[r < 2 ? r : 1];
+    e->p.proj_block = kProjBlocks[r];
+    int seg = -1;
+    s = cvt_engine_add_segment(e, mesh, sites, n_sites, 0, &seg, nullptr);
+    float ms[5], warm[5];
+    if (s == CVT_OK) s = cvt_engine_profile(e, 1, warm, nullptr);   // first launches of these shapes
+    if (s == CVT_OK) s = cvt_engine_profile(e, iters, ms, nullptr);
+    if (s == CVT_OK) s = cvt_engine_remove_segment(e, seg);
+    if (s != CVT_OK) break;
+    if (better(ms[1], best[0], r == 0)) { best[0] = ms[1]; pick[0] = e->p.knn_block; }
+    if (r < 2 && better(ms[2], best[1], r == 0)) { best[1] = ms[2]; pick[1] = e->p.clip_block; }
+    if (better(ms[3], best[2], r == 0)) { best[2] = ms[3]; pick[2] = e->p.proj_block; }
+  }
+  cvt_engine_destroy(e);
+  if (s != CVT_OK) return s;
+  p->knn_block = pick[0];
+  p->clip_block = pick[1];
+  p->proj_block = pick[2];
+  if (ms_out) for (int k = 0; k < 3; ++k) ms_out[k] = best[k];
+  return CVT_OK;
 }
 
 extern "C" cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF, const float* sites_in, int n_sites,

@@ -31,10 +31,12 @@ constexpr int kStatsRing = 256;   // iterations of per-segment statistics kept
 constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter, -, -
 constexpr int kKProj = 5;         // KPROJ (main.cu:394)
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
-constexpr int kKnnBlock = 128;    // threads per block of the site KNN kernel
 constexpr int kKnnBuf = 64;       // parked candidates per thread (shared memory)
-constexpr int kCellMinBlocks = 6;  // resident blocks per SM asked of k_site_clip (caps registers near 80;
-                                   // its two polygon buffers take 32 KB per block)
+// threads per SM that k_site_clip's launch bounds ask to keep resident: it
+// caps registers near 80 (6 blocks of 128 with 32 KB of polygon buffers each
+// for FP32 polygons, 6 of 64 for FP64 ones) whatever the block size
+constexpr int kClipThreadsF = 768;
+constexpr int kClipThreadsD = 384;
 
 struct MeshDev {
   const float* V;
@@ -344,8 +346,8 @@ __global__ void k_active_list(EngineArgs<T> a) {
 // list row is read (for the freeze test's equality) and written coalesced.
 // Sets same[g] (new list == stored list), kth[g] and the frame vertex nnv[g].
 // ---------------------------------------------------------------------------
-template <class T, int KK>
-__global__ void __launch_bounds__(kKnnBlock) k_site_knn(EngineArgs<T> a) {
+template <class T, int KK, int BS>
+__global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
   using O = KeyOps<T>;
   const int lane = threadIdx.x & 31;
   const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
@@ -450,7 +452,8 @@ __device__ __forceinline__ bool site_clip(const EngineArgs<typename PT<PROF>::T>
 }
 
 template <int PROF, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK, kCellMinBlocks) k_site_clip(EngineArgs<typename PT<PROF>::T> a, int parity) {
+__global__ void __launch_bounds__(BLOCK, (sizeof(typename PT<PROF>::PP) == 8 ? kClipThreadsD : kClipThreadsF) / BLOCK)
+    k_site_clip(EngineArgs<typename PT<PROF>::T> a, int parity) {
   using PP = typename PT<PROF>::PP;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   V2<PP>* sm = reinterpret_cast<V2<PP>*>(smem_raw);
@@ -607,9 +610,9 @@ __device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, cons
   }
 }
 
-template <int PROF>
-__global__ void __launch_bounds__(128) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
-  const int t = blockIdx.x * 128 + threadIdx.x;
+template <int PROF, int BS>
+__global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  const int t = blockIdx.x * BS + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   SiteOut o{-1, 0, 0, 0, 0, 0.f};
   if (t < n_grid) site_proj<PROF>(a, parity, (int)a.sorted[t].id, o);

@@ -25,7 +25,8 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1, use_graph=True) -> Params:
+def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1, use_graph=True,
+           knn_block=0, clip_block=0, proj_block=0) -> Params:
     p = Params()
     _lib.load().cvt_params_default(C.byref(p))
     p.k = int(k)
@@ -35,6 +36,7 @@ def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1,
     p.ex_quirk = int(bool(ex_quirk))
     p.cell_factor = float(cell_factor)
     p.use_graph = int(bool(use_graph))
+    p.knn_block, p.clip_block, p.proj_block = int(knn_block), int(clip_block), int(proj_block)
     return p
 
 
@@ -273,14 +275,31 @@ def grid_cells(mesh: Mesh, n_sites: int, k: int, cell_factor: float = 1.1) -> in
     return int(prod) + 1
 
 
-def remesh(V, F, sites, k=24, mode=0, profile="ref", iters=50, ex_quirk=True, cell_factor=1.1, with_counts=False):
-    """One-call remesh through ``cvt_remesh`` (host arrays in and out)."""
+def autotune(mesh: Mesh, sites, prm: Params, iters: int = 4):
+    """Launch-shape autotuner (``cvt_autotune``): returns (tuned copy of the
+    params, per-iteration ms of the chosen KNN, clip and projection shapes)."""
+    S = np.ascontiguousarray(sites, np.float32)
+    q = Params()
+    C.memmove(C.byref(q), C.byref(prm), C.sizeof(Params))
+    ms = (C.c_float * 3)()
+    call("cvt_autotune", mesh.handle, _ptr(S), S.shape[0], int(iters), C.byref(q), ms)
+    return q, {"knn": float(ms[0]), "clip": float(ms[1]), "proj": float(ms[2])}
+
+
+def tiles(prm: Params) -> dict:
+    return {"knn_block": prm.knn_block, "clip_block": prm.clip_block, "proj_block": prm.proj_block}
+
+
+def remesh(V, F, sites, k=24, mode=0, profile="ref", iters=50, ex_quirk=True, cell_factor=1.1, with_counts=False,
+           prm: Params | None = None):
+    """One-call remesh through ``cvt_remesh`` (host arrays in and out); prm,
+    when given, replaces the parameters built from the keywords."""
     V = np.ascontiguousarray(V, np.float32)
     F = np.ascontiguousarray(F, np.int32)
     S = np.ascontiguousarray(sites, np.float32)
     out = np.zeros_like(S)
     counts = np.zeros((max(iters, 1), 4), np.int32)
-    p = params(k=k, mode=mode, profile=profile, ex_quirk=ex_quirk, cell_factor=cell_factor)
+    p = prm if prm is not None else params(k=k, mode=mode, profile=profile, ex_quirk=ex_quirk, cell_factor=cell_factor)
     call("cvt_remesh", _ptr(V), V.shape[0], _ptr(F), F.shape[0], _ptr(S), S.shape[0], C.byref(p), int(iters),
          _ptr(out), _ptr(counts))
     return (out, counts[:iters]) if with_counts else out

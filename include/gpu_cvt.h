@@ -231,9 +231,20 @@ typedef struct {
   int ex_quirk;       /* mode 0: centroid->vertex KNN skips vertex index == site index */
   float cell_factor;  /* site-grid cell edge / expected (K+1)-th neighbour radius */
   int use_graph;      /* capture iterations in a CUDA graph */
+  /* launch shapes (threads per block); results do not depend on them:
+   * knn_block 64|128|256 (one warp per site), clip_block 64|128 (FP64
+   * profile: 32|64), proj_block 64|128|256; 0 = default. */
+  int knn_block, clip_block, proj_block;
 } cvt_params_t;
 
 void cvt_params_default(cvt_params_t* p);
+/* Launch-shape autotuner: times every candidate block size of the site KNN,
+ * clip and projection kernels over `iters` Lloyd iterations (iters >= 2) of
+ * the given sites on the mesh, in a scratch engine, and writes the fastest
+ * into p->knn_block / clip_block / proj_block (the other fields are used as
+ * given); a shape replaces the default only when it is > 3 % faster.  ms (may be NULL) receives the per-iteration ms of the chosen
+ * shapes {knn, clip, proj}.  Synchronous; allocates a scratch engine. */
+cvt_status_t cvt_autotune(cvt_mesh_t mesh, const float* sites, int n_sites, int iters, cvt_params_t* p, float* ms);
 
 typedef struct cvt_engine* cvt_engine_t;
 

@@ -106,6 +106,31 @@ def test_far_centroids_bitexact(eng, oracle, mode, profile):
     assert np.array_equal(counts, r["counts"])
 
 
+@pytest.mark.parametrize("profile", ["ref", "mixed", "fp64"])
+def test_launch_shapes_same_results_and_autotune(eng, small_torus, profile):
+    """Every launch shape of the KNN, clip and projection kernels gives the
+    same run bit for bit; the autotuner picks supported shapes."""
+    m, S0 = small_torus
+    M = eng.Mesh(m.V, m.F)
+    clip = (32, 64) if profile == "fp64" else (64, 128)
+    outs = []
+    for kb, cb, pb in ((64, clip[0], 64), (128, clip[1], 128), (256, clip[1], 256)):
+        e = eng.Engine(eng.params(k=24, mode=1, profile=profile, knn_block=kb, clip_block=cb, proj_block=pb), 1,
+                       len(S0), eng.grid_cells(M, len(S0), 24))
+        g = e.add(M, S0)
+        e.run(12)
+        outs.append(e.sites_f64(g) if profile == "fp64" else e.sites(g))
+        e.close()
+    assert all(np.array_equal(outs[0], o) for o in outs[1:])
+    q, ms = eng.autotune(M, S0, eng.params(k=24, mode=1, profile=profile), iters=3)
+    assert q.knn_block in (64, 128, 256) and q.proj_block in (64, 128, 256) and q.clip_block in clip
+    assert all(v > 0 for v in ms.values())
+    from gpu_cvt_b200._lib import CvtError
+    with pytest.raises(CvtError):
+        eng.Engine(eng.params(k=24, knn_block=96), 1, 10, 100)
+    M.close()
+
+
 def test_fp64_profile_matches_fp64_oracle(eng, oracle, c1):
     m, S0 = c1
     S, st, counts = run_engine(eng, m, S0, 20, 0, 10, profile="fp64")
