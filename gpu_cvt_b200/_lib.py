@@ -67,6 +67,7 @@ _SIGS = {
     "cvt_mesh_get_bvh": [vp, vp, i32, vp, i32, vp],
     "cvt_release_cached_memory": [],
     "cvt_autotune": [vp, vp, i32, i32, vp, vp],
+    "cvt_segment_cells": [vp, i32, vp, vp],
     "cvt_mesh_create": [vp, i32, vp, i32, vp],
     "cvt_set_vertex_cell_factor": [f32],
     "cvt_mesh_info": [vp, vp],

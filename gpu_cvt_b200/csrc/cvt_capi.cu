@@ -1473,10 +1473,16 @@ static void engine_caps(const cvt_mesh* m, int n, const cvt_params_t* p, int* ce
   *cells = g.ncell + 1;
 }
 
+extern "C" cvt_status_t cvt_segment_cells(cvt_mesh_t mesh, int n_sites, const cvt_params_t* p, int* cells) {
+  if (!mesh || n_sites < 0 || !p || !cells) return fail(CVT_ERR_INVALID, "cvt_segment_cells: bad arguments");
+  engine_caps(mesh, n_sites, p, cells);
+  return CVT_OK;
+}
+
 // Three timed passes over the same fresh copy of the sites: pass r runs
-// knn/proj candidate r and clip candidate min(r, 1) (candidate 0 = default).  The kernels are timed
-// separately by cvt_engine_profile, so one pass measures one candidate of
-// each; results do not depend on the shapes.
+// knn/proj candidate r and clip candidate min(r, 1) (candidate 0 = default).
+// The kernels are timed separately by cvt_engine_profile, so one pass
+// measures one candidate of each; results do not depend on the shapes.
 extern "C" cvt_status_t cvt_autotune(cvt_mesh_t mesh, const float* sites, int n_sites, int iters, cvt_params_t* p,
                                      float* ms_out) {
   if (!mesh || !sites || n_sites < 1 || iters < 2 || !p) return fail(CVT_ERR_INVALID, "cvt_autotune: bad arguments");

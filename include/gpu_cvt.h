@@ -256,6 +256,9 @@ typedef struct {
   int iter;
 } cvt_iter_stats_t;
 
+/* Grid cells a segment of n_sites sites on `mesh` reserves with params p
+ * (its cell_factor and k); sum them over the segments for max_cells. */
+cvt_status_t cvt_segment_cells(cvt_mesh_t mesh, int n_sites, const cvt_params_t* p, int* cells);
 /* Capacity-based engine: up to max_segments segments holding up to
  * max_sites sites and max_cells grid cells in total. */
 cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segments, int max_sites, int max_cells,

@@ -296,3 +296,17 @@ def test_cli_driver_contract(tmp_path):
     assert runs[0] == cli.RUNS_HEADER and runs[1].startswith("ball,freeze,")
     dH = float(rows[2].split(",")[9])
     assert 0 < dH < 0.05
+
+
+def test_c_driver_runs(tmp_path):
+    """The plain C driver: engine run + evaluation, then cvt_remesh on the same
+    input gives the same sites byte for byte."""
+    import subprocess
+    from test_host import build_c_driver
+    exe = build_c_driver(tmp_path / "remesh_driver")
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    f = r.stdout.split()
+    vals = dict(zip(f[0::2], f[1::2]))
+    assert int(vals["same"]) == 1 and int(vals["faces"]) > 8000
+    assert 0 < float(vals["dH"]) < 0.01 and float(vals["Qavg"]) > 0.8

@@ -99,3 +99,29 @@ def test_invalid_arguments_rejected_without_gpu():
     h = ctypes.c_void_p()
     st = _lib.load().cvt_engine_create(ctypes.byref(p), 1, 10, 10, ctypes.byref(h))
     assert st == 4 and "k must be one of" in _lib.last_error()
+
+
+def build_c_driver(out_path):
+    """Compile tests/c_driver/remesh_driver.c, a plain C caller of the ABI,
+    against include/gpu_cvt.h and link it to libgpucvt.so."""
+    import shutil
+    import subprocess
+    from gpu_cvt_b200 import _lib
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    _lib.load()
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    cmd = [cc, "-std=c99", "-O2", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(root, "include"),
+           os.path.join(root, "tests", "c_driver", "remesh_driver.c"), "-L", libdir, "-lgpucvt",
+           "-Wl,-rpath," + libdir, "-lm", "-o", str(out_path)]
+    subprocess.run(cmd, check=True, capture_output=True, text=True)
+    return str(out_path)
+
+
+def test_c_driver_compiles_and_links(tmp_path):
+    """The C ABI is usable from C as it stands: the driver builds with
+    -Wall -Wextra -Werror and links against the library."""
+    exe = build_c_driver(tmp_path / "remesh_driver")
+    assert os.path.getsize(exe) > 0
