@@ -1247,12 +1247,12 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   L++;
   if (ev) CK(cudaEventRecord(ev[1], st));
   switch (e->K) {
-    case 8: launch_site_knn<T, 9>(a, ns, e->p.knn_block, st); break;
-    case 12: launch_site_knn<T, 13>(a, ns, e->p.knn_block, st); break;
-    case 16: launch_site_knn<T, 17>(a, ns, e->p.knn_block, st); break;
-    case 20: launch_site_knn<T, 21>(a, ns, e->p.knn_block, st); break;
-    case 24: launch_site_knn<T, 25>(a, ns, e->p.knn_block, st); break;
-    default: launch_site_knn<T, 33>(a, ns, e->p.knn_block, st); break;
+    case 8: launch_site_knn<T, 8>(a, ns, e->p.knn_block, st); break;
+    case 12: launch_site_knn<T, 12>(a, ns, e->p.knn_block, st); break;
+    case 16: launch_site_knn<T, 16>(a, ns, e->p.knn_block, st); break;
+    case 20: launch_site_knn<T, 20>(a, ns, e->p.knn_block, st); break;
+    case 24: launch_site_knn<T, 24>(a, ns, e->p.knn_block, st); break;
+    default: launch_site_knn<T, 32>(a, ns, e->p.knn_block, st); break;
   }
   L++;
   if (ev) CK(cudaEventRecord(ev[2], st));

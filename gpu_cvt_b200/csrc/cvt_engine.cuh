@@ -60,7 +60,7 @@ struct SegDev {
   int mode;       // 0 / 1 / 2
   int ex_quirk;
   int iter;       // iterations completed (device-side count)
-  float kth_est;  // first-iteration estimate of the (K+1)-th squared distance
+  float kth_est;  // first-iteration estimate of the K-th neighbour's squared distance
   float stop_motion2;  // stop once an iteration's max squared motion <= this (< 0: never)
   int stop_iters;      // stop after this many iterations (0: never)
   float thr2_tier[6];
@@ -81,7 +81,7 @@ template <class T> struct EngineArgs {
   T* S[2];
   uint32_t* knn;      // K neighbours per site (local indices), the current list
   uint8_t* same;      // list unchanged vs the previous iteration (site KNN kernel)
-  float* kth;         // last (K+1)-th squared distance per site, < 0 unknown
+  float* kth;         // last K-th neighbour's squared distance per site, < 0 unknown
   int* act;           // sorted positions of the sites whose list is recomputed
   int* act_count;
   int* knnv;
@@ -341,13 +341,15 @@ __global__ void k_active_list(EngineArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// k_site_knn: one warp per active site.  Exact (K+1)-NN within its segment,
-// self dropped (site_knn.cuh:79-103); lane j holds the j-th neighbour, so the
-// list row is read (for the freeze test's equality) and written coalesced.
+// k_site_knn: one warp per active site.  Exact K nearest other sites within
+// its segment (the reference's K+1 nearest with self dropped,
+// site_knn.cuh:79-103); lane j holds the j-th neighbour, so the list row is
+// read (for the freeze test's equality) and written coalesced.
 // Sets same[g] (new list == stored list), kth[g] and the frame vertex nnv[g].
 // ---------------------------------------------------------------------------
 template <class T, int KK, int BS>
 __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
+  static_assert(KK <= 32, "one list entry per lane");
   using O = KeyOps<T>;
   const int lane = threadIdx.x & 31;
   const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
@@ -357,42 +359,28 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
   const int s = __ldg(a.site_seg + g);
   const SegDev& sd = a.segs[s];
   const MeshDev& md = a.meshes[sd.mesh];
-  constexpr int K = KK - 1;
+  // The K nearest other sites: the reference's K+1 nearest with self dropped
+  // (site_knn.cuh:79-103) are exactly these, also when duplicates of the site
+  // with smaller indices push self out of the K+1 (then the first K are kept,
+  // the same K points), and the K-th distance equals the (K+1)-th with self.
+  constexpr int K = KK;
   const V3<T> q{me.x, me.y, me.z};
   const GridGeom G = a.geom[s];
   const float kp = a.kth[g];
-  // candidates beyond 1.1x the last (K+1)-th squared distance are skipped;
-  // sites move little between iterations, and a bound that proves too tight
+  // candidates beyond 1.1x the last K-th squared distance are skipped; sites
+  // move little between iterations, and a bound that proves too tight
   // restarts the search without it (swept 1.02-1.5: 1.05-1.1 fastest)
   const T thr0 = kp >= 0.f ? (T)kp * (T)1.1 : (T)sd.kth_est;
   constexpr int R = (KK + 31) / 32;
   typename O::Key key[R];
-  warp_knn<T, T, KK>(G, a.cell_start, a.sorted, q, thr0, lane, [](uint32_t) { return true; }, key);
+  const uint32_t self = (uint32_t)g;
+  warp_knn<T, T, KK>(G, a.cell_start, a.sorted, q, thr0, lane, [self](uint32_t id) { return id != self; }, key);
   const auto kth = shfl_key(key[(KK - 1) / 32], (KK - 1) % 32);
   const bool full = !O::is_empty(kth);
   if (lane == 0) a.kth[g] = full ? (float)O::dist(kth) : -1.f;
-  // drop self: the entries after self move down one place
   const uint32_t base = (uint32_t)sd.site_base;
-  const uint32_t i = (uint32_t)g - base;
-  uint32_t loc[R];
-  unsigned selfmask[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    const uint32_t gid = O::idx(key[r]);
-    loc[r] = gid == 0xffffffffu ? 0xffffffffu : gid - base;
-    selfmask[r] = __ballot_sync(0xffffffffu, 32 * r + lane < KK && loc[r] == i);
-  }
-  int p = K;
-#pragma unroll
-  for (int r = R - 1; r >= 0; --r)
-    if (selfmask[r]) p = 32 * r + __ffs(selfmask[r]) - 1;
-  // entry j of the output (j < K <= 32) is loc[j] before self, loc[j+1] after
-  uint32_t next = __shfl_down_sync(0xffffffffu, loc[0], 1);
-  if (R > 1) {
-    const uint32_t first1 = __shfl_sync(0xffffffffu, loc[R - 1], 0);
-    if (lane == 31) next = first1;
-  }
-  const uint32_t out = lane < p ? loc[0] : next;
+  const uint32_t gid = O::idx(key[0]);
+  const uint32_t out = gid == 0xffffffffu ? 0xffffffffu : gid - base;
   uint32_t* row = a.knn + (size_t)g * K;
   bool diff = false;
   if (lane < K) {
