@@ -1281,32 +1281,16 @@ static cvt_status_t enqueue_iteration(cvt_engine* e, int parity, cudaStream_t st
   }
 }
 
-static cvt_status_t set_smem_attrs(cvt_engine* e) {
-  static bool done[3] = {false, false, false};
-  int pr = e->p.profile;
-  if (done[pr]) return CVT_OK;
-  const auto attr = cudaFuncAttributeMaxDynamicSharedMemorySize;
-  const int f128 = 2 * kCellCap * 128 * (int)sizeof(V2<float>), f64 = f128 / 2;
-  const int d64 = 2 * kCellCap * 64 * (int)sizeof(V2<double>), d32 = d64 / 2;
-  if (pr == CVT_PROFILE_REF) {
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_REF, 128, kCellCap>, attr, f128));
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_REF, 64, kCellCap>, attr, f64));
-  } else if (pr == CVT_PROFILE_MIXED) {
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_MIXED, 128, kCellCap>, attr, f128));
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_MIXED, 64, kCellCap>, attr, f64));
-  } else {
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_FP64, 64, kCellCap>, attr, d64));
-    CK(cudaFuncSetAttribute(k_site_clip<PROF_FP64, 32, kCellCap>, attr, d32));
-  }
-  done[pr] = true;
-  return CVT_OK;
-}
+// k_site_clip's dynamic shared memory (two 16-vertex polygon buffers per
+// thread) is at most 32 KB per block for every launch shape, within the
+// default 48 KB limit, so no function attribute is needed.
+static_assert(2 * kCellCap * 128 * sizeof(V2<float>) <= 48 * 1024 && 2 * kCellCap * 64 * sizeof(V2<double>) <= 48 * 1024,
+              "clip buffers exceed the default dynamic shared memory limit");
 
 extern "C" cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream) {
   if (!e || iters < 0) return fail(CVT_ERR_INVALID, "cvt_engine_run: bad arguments");
   cudaStream_t st = S_(stream);
-  cvt_status_t s = set_smem_attrs(e);
-  if (s != CVT_OK) return s;
+  cvt_status_t s = CVT_OK;
   long long launches = 0;
   for (int it = 0; it < iters; ++it) {
     int par = e->parity;
@@ -1346,8 +1330,7 @@ extern "C" cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream) 
 extern "C" cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms, void* stream) {
   if (!e || !ms || iters < 1) return fail(CVT_ERR_INVALID, "cvt_engine_profile: bad arguments");
   cudaStream_t st = S_(stream);
-  cvt_status_t s = set_smem_attrs(e);
-  if (s != CVT_OK) return s;
+  cvt_status_t s = CVT_OK;
   cudaEvent_t ev[6];
   for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
   double acc[5] = {0, 0, 0, 0, 0};

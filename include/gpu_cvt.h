@@ -7,8 +7,9 @@
  * float3 AoS), faces int[3], neighbour indices uint32 (the reference's idx_t)
  * unless stated, masks uint8.  `stream` is a cudaStream_t (NULL = legacy
  * default stream).  Stage functions are asynchronous on `stream`; they take
- * caller-owned DEVICE pointers and allocate their temporaries stream-ordered
- * (cudaMallocAsync), freeing them before return in stream order.
+ * caller-owned DEVICE pointers and take their temporaries stream-ordered
+ * from the library's memory pool (see cvt_release_cached_memory), freeing
+ * them in stream order before return.
  *
  * Every function returns cvt_status_t; CVT_OK is 0.  cvt_last_error() gives
  * the message of the last failure on the calling thread.  (The reference
