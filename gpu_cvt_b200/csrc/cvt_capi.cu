@@ -126,6 +126,15 @@ extern "C" cvt_status_t cvt_release_cached_memory(void) {
   return CVT_OK;
 }
 
+// streaming multiprocessors of the current device (grid size of the
+// grid-stride fallback kernels: one block per SM)
+static int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 148;
+  return n > 0 ? n : 148;
+}
+
 // stream-ordered scratch
 struct Scratch {
   cudaStream_t st;
@@ -319,7 +328,7 @@ static cvt_status_t clip_dispatch(const float* S, const float* U, const float* V
   }
   k_stage_clip<PROF, kClipBlock, kClipCap><<<cdiv(n, kClipBlock), kClipBlock, smem, st>>>(S, U, V, knn, n, K, R, cent, nverts, ovf);
   CKLAUNCH();
-  k_stage_clip_fallback<PROF><<<148, 64, 0, st>>>(S, U, V, knn, n, K, R, cent, nverts, ovf);
+  k_stage_clip_fallback<PROF><<<sm_count(), 64, 0, st>>>(S, U, V, knn, n, K, R, cent, nverts, ovf);
   CKLAUNCH();
   return CVT_OK;
 }
@@ -980,6 +989,7 @@ struct cvt_engine {
   int* d_stats = nullptr;
   int* d_ovf = nullptr;
   int* d_far = nullptr;
+  int num_sms = 148;
   void* d_cent = nullptr;
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -1011,6 +1021,7 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
                                      "64 or 128 (FP64 profile: 32 or 64)");
   cvt_engine* e = new cvt_engine();
   e->p = q;
+  e->num_sms = sm_count();
   e->K = p->k;
   e->f64 = p->profile == CVT_PROFILE_FP64;
   e->max_seg = max_segments;
@@ -1257,11 +1268,11 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   L++;
   if (ev) CK(cudaEventRecord(ev[2], st));
   launch_site_clip<PROF>(a, parity, ns, e->p.clip_block, st);
-  k_clip_overflow<PROF><<<148, 64, 0, st>>>(a, parity);
+  k_clip_overflow<PROF><<<e->num_sms, 64, 0, st>>>(a, parity);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[3], st));
   launch_site_proj<PROF>(a, parity, ns, e->p.proj_block, st);
-  k_site_far<PROF><<<148, 128, 0, st>>>(a, parity);
+  k_site_far<PROF><<<e->num_sms, 128, 0, st>>>(a, parity);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[4], st));
   k_seg_advance<<<1, 256, 0, st>>>(e->d_segs, e->d_active, e->max_seg, e->d_stats, e->d_ovf, e->d_far);
