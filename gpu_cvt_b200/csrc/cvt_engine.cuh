@@ -31,7 +31,6 @@ constexpr int kStatsRing = 256;   // iterations of per-segment statistics kept
 constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter, -, -
 constexpr int kKProj = 5;         // KPROJ (main.cu:394)
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
-constexpr int kKnnBuf = 64;       // parked candidates per thread (shared memory)
 // threads per SM that k_site_clip's launch bounds ask to keep resident: it
 // caps registers near 80 (6 blocks of 128 with 32 KB of polygon buffers each
 // for FP32 polygons, 6 of 64 for FP64 ones) whatever the block size

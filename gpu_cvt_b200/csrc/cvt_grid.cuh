@@ -149,100 +149,6 @@ __device__ __forceinline__ bool grid_knn(const GridGeom& g, const int* __restric
   return true;
 }
 
-// Same search with buffered insertion.  Candidates with d <= thr are parked
-// in a per-thread shared-memory column (their sorted positions) and inserted
-// at the end of each ring, when every lane of the warp flushes at once, so the
-// lanes run the insertion network together instead of once per candidate that
-// any one lane accepts.  thr starts at a caller estimate (last iteration's
-// K-th distance) and tightens to the current K-th distance at every flush.
-// The result is exact whatever the estimate: a skipped candidate lies above a
-// threshold that is >= the final K-th distance; an estimate that proves too
-// tight (the list is not full although every point within it was visited)
-// restarts the search with thr = +inf; a buffer overflow restarts it in
-// direct-insertion mode (the plain search above).  CAPB >= KK.
-template <class T, class PT, int KK, int CAPB, class Accept>
-__device__ __forceinline__ void grid_knn_buffered(const GridGeom& g, const int* __restrict__ cell_start,
-                                                  const Pt4<PT>* __restrict__ pts, V3<T> q, TopK<T, KK>& top,
-                                                  T thr0, uint32_t* buf, int stride, Accept accept) {
-  static_assert(CAPB >= KK, "the buffer must hold a full list");
-  if (!finite3(q)) return;
-  const int cx = grid_coord(g, q.x, 0), cy = grid_coord(g, q.y, 1), cz = grid_coord(g, q.z, 2);
-  const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
-  const float slack = 1e-3f * g.h;
-  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
-  const int c[3] = {cx, cy, cz};
-  const T INF = (T)INFINITY;
-  T thr = thr0 > (T)0 ? thr0 : INF;
-  bool direct = false, dropped = false;
-  int cnt = 0;
-  auto scan_range = [&](int b, int e) {
-    for (int k = b; k < e; ++k) {
-      const Pt4<PT> p = pts[k];
-      if (!accept(p.id)) continue;
-      const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
-      if (direct) {
-        if (d <= top.worst_d()) top.insert(KeyOps<T>::make(d, p.id));
-      } else if (d <= thr) {
-        if (cnt < CAPB) buf[(cnt++) * stride] = (uint32_t)k;
-        else dropped = true;
-      }
-    }
-  };
-  for (int r = 1; r <= rmax; ++r) {
-    const int z0 = max(cz - r, 0), z1 = min(cz + r, g.dim[2] - 1);
-    const int y0 = max(cy - r, 0), y1 = min(cy + r, g.dim[1] - 1);
-    const int x0 = max(cx - r, 0), x1 = min(cx + r, g.dim[0] - 1);
-    for (int z = z0; z <= z1; ++z) {
-      for (int y = y0; y <= y1; ++y) {
-        const int row = g.cell_base + (z * g.dim[1] + y) * g.dim[0];
-        const bool full_row = (r == 1) || abs(z - cz) == r || abs(y - cy) == r;
-        if (full_row) {
-          scan_range(__ldg(cell_start + row + x0), __ldg(cell_start + row + x1 + 1));
-        } else {
-          if (cx - r >= 0) scan_range(__ldg(cell_start + row + cx - r), __ldg(cell_start + row + cx - r + 1));
-          if (cx + r < g.dim[0]) scan_range(__ldg(cell_start + row + cx + r), __ldg(cell_start + row + cx + r + 1));
-        }
-      }
-    }
-    if (!direct) {
-      for (int k = 0; k < cnt; ++k) {
-        const Pt4<PT> p = pts[buf[k * stride]];
-        const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
-        top.insert(KeyOps<T>::make(d, p.id));
-      }
-      cnt = 0;
-      if (dropped) {  // candidates within thr were not parked: start over, direct
-        top = TopK<T, KK>();
-        direct = true;
-        dropped = false;
-        r = 0;
-        continue;
-      }
-      if (top.full()) thr = fmin(thr, top.worst_d());
-    }
-    float m = __int_as_float(0x7f800000);
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      if (c[a] - r > 0) m = fminf(m, qf[a] - (g.lo[a] + (float)(c[a] - r) * g.h));
-      if (c[a] + r < g.dim[a] - 1) m = fminf(m, (g.lo[a] + (float)(c[a] + r + 1) * g.h) - qf[a]);
-    }
-    const bool all_seen = isinf(m);
-    m -= slack;
-    if (top.full()) {
-      if (all_seen || (m > 0.f && (double)top.worst_d() < (double)m * (double)m)) break;
-    } else if (!direct && thr < INF && (all_seen || (m > 0.f && (double)thr < (double)m * (double)m))) {
-      // every point within the estimate was visited and the list is not full:
-      // the estimate was too tight -- search again, inserting directly
-      thr = INF;
-      direct = true;
-      top = TopK<T, KK>();
-      r = 0;
-    } else if (all_seen) {
-      break;
-    }
-  }
-}
-
 // ---------------------------------------------------------------------------
 // warp-cooperative search: one warp per query point
 // ---------------------------------------------------------------------------
@@ -329,9 +235,13 @@ __device__ __forceinline__ float ring_margin(const GridGeom& g, const float qf[3
 
 // Exact KK nearest points of q (uniform across the warp), KK <= 64.  The
 // sorted list spans R = ceil(KK/32) registers per lane: list[r] at lane j is
-// entry 32*r + j.  Candidates beyond the estimate thr0 are skipped; an
-// estimate that proves too tight restarts the search without it (see
-// grid_knn_buffered for why the result is exact).
+// entry 32*r + j.  Candidates beyond the estimate thr0 (the caller's guess of
+// the KK-th squared distance) are skipped, and thr tightens to the current
+// KK-th distance once the list is full.  The result is exact whatever the
+// estimate: a skipped candidate lies above a threshold that is >= the final
+// KK-th distance, and an estimate that proves too tight (the list is not full
+// although every point within it was visited) restarts the search with
+// thr = +inf.
 template <class T, class PT, int KK, class Accept>
 __device__ __forceinline__ void warp_knn(const GridGeom& g, const int* __restrict__ cell_start,
                                          const Pt4<PT>* __restrict__ pts, V3<T> q, T thr0, int lane, Accept accept,
