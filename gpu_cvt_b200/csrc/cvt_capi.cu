@@ -989,6 +989,7 @@ struct cvt_engine {
   int* d_stats = nullptr;
   int* d_ovf = nullptr;
   int* d_far = nullptr;
+  unsigned* d_tickets = nullptr;  // [0] grid scan, [1] far sites + bookkeeping (zero between launches)
   int num_sms = 148;
   void* d_cent = nullptr;
   // graphs
@@ -1074,6 +1075,7 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   ar.add(&e->d_stats, (size_t)max_segments * kStatsRing * kStatsWords);
   ar.add(&e->d_ovf, ns + 1);
   ar.add(&e->d_far, ns + 1);
+  ar.add(&e->d_tickets, 2);
   ar.add(reinterpret_cast<char**>(&e->d_cent), tsz * 3 * ns);
   ECK(ar.commit(&e->arena));
   e->bytes = ar.size;
@@ -1246,14 +1248,13 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   k_grid_count<T><<<cdiv(ns, 256), 256, 0, st>>>(ns, (const T*)e->d_S[parity], SegGrid{e->d_geom, e->d_site_seg, e->d_active},
                                                  e->d_cell_count, e->d_cellrank);
   L++;
-  launch_exclusive_scan(e->max_cells, e->d_cell_count, e->d_part, e->d_cell_start, st, true);
-  L += 3;
+  L += launch_exclusive_scan(e->max_cells, e->d_cell_count, e->d_part, e->d_cell_start, st, true, e->d_tickets);
   k_grid_scatter<T><<<cdiv(ns, 256), 256, 0, st>>>(ns, (const T*)e->d_S[parity], e->d_cellrank, e->d_cell_start,
                                                    (Pt4<T>*)e->d_sorted);
   L++;
   // cell_start[max_cells] is the number of gridded sites (read on the device)
   a.total_cells = e->max_cells;
-  CK(cudaMemsetAsync(e->d_act_count, 0, sizeof(int), st));
+  // d_act_count is zero here: set at creation, reset by the bookkeeping
   k_active_list<T><<<cdiv(ns, 256), 256, 0, st>>>(a);
   L++;
   if (ev) CK(cudaEventRecord(ev[1], st));
@@ -1272,11 +1273,9 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   L += 2;
   if (ev) CK(cudaEventRecord(ev[3], st));
   launch_site_proj<PROF>(a, parity, ns, e->p.proj_block, st);
-  k_site_far<PROF><<<e->num_sms, 128, 0, st>>>(a, parity);
+  k_site_far<PROF><<<e->num_sms, 128, 0, st>>>(a, parity, e->d_segs, e->d_active, e->max_seg, e->d_tickets + 1);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[4], st));
-  k_seg_advance<<<1, 256, 0, st>>>(e->d_segs, e->d_active, e->max_seg, e->d_stats, e->d_ovf, e->d_far);
-  L++;
   if (ev) CK(cudaEventRecord(ev[5], st));
   CK(cudaGetLastError());
   *nlaunch = L;

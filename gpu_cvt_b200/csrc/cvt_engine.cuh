@@ -19,7 +19,8 @@
 //   k_site_far   the sites whose centroid lies so far off the surface that
 //                the vertex grid search gave up: exact brute-force 5-NN by
 //                a block, then the rest of the step
-//   k_seg_advance  per-segment iteration counters / statistics slots
+//   (bookkeeping) per-segment iteration counters / statistics slots, run by
+//                the last block of k_site_far
 // All sizes come from device memory, so the whole iteration is captured once
 // in a CUDA graph and relaunched while segments come and go.
 #pragma once
@@ -606,15 +607,42 @@ __global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::
   stats_flush(a.stats, a.segs, o);
 }
 
+// Iteration bookkeeping, run by one block: advance active segments, clear
+// their next stats slot, apply each segment's stop rule (a stopped segment is
+// no longer gridded or iterated: active = 2), reset the overflow, deferred
+// and active-site counts for the next iteration.
+__device__ __forceinline__ void seg_advance(SegDev* segs, int* active, int nseg, int* stats, int* ovf, int* far,
+                                            int* act_count) {
+  for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
+    if (active[s] != 1) continue;
+    int it = segs[s].iter;
+    int* cur = stats + ((size_t)s * kStatsRing + (it % kStatsRing)) * kStatsWords;
+    cur[5] = it;
+    const float d2 = __uint_as_float((unsigned)cur[4]);
+    int nx = it + 1;
+    int* sl = stats + ((size_t)s * kStatsRing + (nx % kStatsRing)) * kStatsWords;
+    for (int w = 0; w < kStatsWords; ++w) sl[w] = 0;
+    segs[s].iter = nx;
+    const float lim = segs[s].stop_motion2;
+    const int cap = segs[s].stop_iters;
+    if ((lim >= 0.f && d2 <= lim) || (cap > 0 && nx >= cap)) active[s] = 2;
+  }
+  if (threadIdx.x == 0) { ovf[0] = 0; far[0] = 0; *act_count = 0; }
+}
+
 // Deferred sites (a.far): one block per site finds the 5 nearest mesh
 // vertices of the centroid by scanning all of them (each thread every 128th
 // vertex, then a merge of the 128 lists by thread 0; exact, the keys are
 // unique), then thread 0 finishes the site.
+// The last block to finish then runs the iteration's bookkeeping
+// (seg_advance), counted by `ticket`, which it leaves at zero.
 template <int PROF>
-__global__ void __launch_bounds__(128) k_site_far(EngineArgs<typename PT<PROF>::T> a, int parity) {
+__global__ void __launch_bounds__(128) k_site_far(EngineArgs<typename PT<PROF>::T> a, int parity, SegDev* segs,
+                                                   int* active, int nseg, unsigned* ticket) {
   using T = typename PT<PROF>::T;
   using Key = typename KeyOps<T>::Key;
   __shared__ Key keys[128 * kKProj];
+  __shared__ bool last;
   const int n = *(volatile int*)a.far;
   for (int k = blockIdx.x; k < n; k += gridDim.x) {
     const int g = a.far[1 + k];
@@ -646,27 +674,15 @@ __global__ void __launch_bounds__(128) k_site_far(EngineArgs<typename PT<PROF>::
     }
     __syncthreads();
   }
-}
-
-// iteration bookkeeping: advance active segments, clear their next stats
-// slot, apply each segment's stop rule (a stopped segment is no longer
-// gridded or iterated: active = 2), reset the overflow list
-__global__ void k_seg_advance(SegDev* segs, int* active, int nseg, int* stats, int* ovf, int* far) {
-  for (int s = threadIdx.x; s < nseg; s += blockDim.x) {
-    if (active[s] != 1) continue;
-    int it = segs[s].iter;
-    int* cur = stats + ((size_t)s * kStatsRing + (it % kStatsRing)) * kStatsWords;
-    cur[5] = it;
-    const float d2 = __uint_as_float((unsigned)cur[4]);
-    int nx = it + 1;
-    int* sl = stats + ((size_t)s * kStatsRing + (nx % kStatsRing)) * kStatsWords;
-    for (int w = 0; w < kStatsWords; ++w) sl[w] = 0;
-    segs[s].iter = nx;
-    const float lim = segs[s].stop_motion2;
-    const int cap = segs[s].stop_iters;
-    if ((lim >= 0.f && d2 <= lim) || (cap > 0 && nx >= cap)) active[s] = 2;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
   }
-  if (threadIdx.x == 0) { ovf[0] = 0; far[0] = 0; }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  seg_advance(segs, active, nseg, a.stats, a.ovf, a.far, a.act_count);
+  if (threadIdx.x == 0) *ticket = 0u;
 }
 
 }  // namespace cvt

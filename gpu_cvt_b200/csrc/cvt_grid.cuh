@@ -412,20 +412,8 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* smem_warp, int& 
   return r;
 }
 
-__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(int n, const int* __restrict__ in, int* __restrict__ part) {
-  __shared__ int sw[33];
-  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
-  int s = 0;
-#pragma unroll
-  for (int k = 0; k < kScanItems; ++k) s += (base + k < n) ? in[base + k] : 0;
-  int total;
-  block_exclusive_scan(s, sw, total);
-  if (threadIdx.x == 0) part[blockIdx.x] = total;
-}
-
 // one block scans the block sums tile by tile, carrying the running total
-__global__ void __launch_bounds__(kScanThreads) k_scan_partials(int nb, int* __restrict__ part) {
-  __shared__ int sw[33];
+__device__ __forceinline__ void scan_partials_block(int nb, int* __restrict__ part, int* sw) {
   int carry = 0;
   for (int tile = 0; tile < nb; tile += kScanTile) {
     int base = tile + threadIdx.x * kScanItems;
@@ -443,6 +431,37 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_partials(int nb, int* __r
     carry += total;
   }
   if (threadIdx.x == 0) part[nb] = carry;
+}
+
+// Block sums of the input.  With a ticket (a zeroed counter), the last block
+// to finish also scans the block sums (the partials step), so the scan takes
+// two launches; it leaves the ticket at zero again.
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(int n, const int* __restrict__ in, int* __restrict__ part,
+                                                              unsigned* ticket) {
+  __shared__ int sw[33];
+  __shared__ bool last;
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) s += (base + k < n) ? in[base + k] : 0;
+  int total;
+  block_exclusive_scan(s, sw, total);
+  if (threadIdx.x == 0) part[blockIdx.x] = total;
+  if (ticket == nullptr) return;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  scan_partials_block(gridDim.x, part, sw);
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_partials(int nb, int* __restrict__ part) {
+  __shared__ int sw[33];
+  scan_partials_block(nb, part, sw);
 }
 
 // clear_in: the input is zeroed once read (the engine's cell counts are then
@@ -473,12 +492,17 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(int n, int* __restr
 inline int scan_blocks(int n) { return (n + kScanTile - 1) / kScanTile; }
 
 // part must hold scan_blocks(n) + 1 ints
-inline void launch_exclusive_scan(int n, int* in, int* part, int* out, cudaStream_t st, bool clear_in = false) {
+// Exclusive scan of n ints, out[n] = total.  With a ticket (a zeroed
+// counter owned by the caller) two launches, else three; returns the number
+// of launches.
+inline int launch_exclusive_scan(int n, int* in, int* part, int* out, cudaStream_t st, bool clear_in = false,
+                                 unsigned* ticket = nullptr) {
   int nb = scan_blocks(n);
   if (nb < 1) nb = 1;
-  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(n, in, part);
-  k_scan_partials<<<1, kScanThreads, 0, st>>>(nb, part);
+  k_scan_reduce<<<nb, kScanThreads, 0, st>>>(n, in, part, ticket);
+  if (ticket == nullptr) k_scan_partials<<<1, kScanThreads, 0, st>>>(nb, part);
   k_scan_apply<<<nb, kScanThreads, 0, st>>>(n, in, part, out, clear_in ? 1 : 0);
+  return ticket == nullptr ? 3 : 2;
 }
 
 }  // namespace cvt
