@@ -22,7 +22,8 @@ Per-stage times come from CUDA events between the fused kernel groups:
 knn_sites_ms = grid build + site KNN (the site->vertex search is fused into
 it, so knn_site_to_mesh_ms is 0), centroids_ms = the per-site kernel (frame,
 clip, centroid, centroid->vertex KNN, projection, freeze test; uv, centroid
-KNN and projection columns are 0), freeze_ms = the bookkeeping kernels.
+KNN and projection columns are 0); freeze_ms is 0 as well, the freeze test
+and the bookkeeping being part of the projection kernels counted there.
 """
 from __future__ import annotations
 

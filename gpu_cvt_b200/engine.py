@@ -190,8 +190,8 @@ class Engine:
         return v.value
 
     def profile(self, iters: int, stream=None):
-        """Per-kernel-group ms per iteration: grid, knn, clip, proj, tail, and
-        cell = clip + proj."""
+        """Per-kernel-group ms per iteration: grid, knn, clip, proj (with the
+        deferred sites and the bookkeeping), tail (0), and cell = clip + proj."""
         ms = (C.c_float * 5)()
         call("cvt_engine_profile", self.handle, int(iters), ms, stream)
         d = dict(zip(("grid", "knn", "clip", "proj", "tail"), [float(x) for x in ms]))

@@ -290,7 +290,8 @@ cvt_status_t cvt_engine_segment_iters(cvt_engine_t e, int seg_id, int* iters);
 /* Run `iters` iterations without a graph, timing each kernel group with CUDA
  * events on `stream`; ms[5] = average ms per iteration of {grid build, site
  * KNN kernel, clip kernel (+ overflow fallback), projection kernel (+ far
- * fallback), bookkeeping}.  Synchronous. */
+ * fallback and the iteration's bookkeeping, which runs in its last block),
+ * 0 (kept for layout)}.  Synchronous. */
 cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms, void* stream);
 /* The evaluation of main.cu:883-1040 for one segment: frames of the current
  * sites, dual triangles with the last iteration's neighbour lists, quality,
