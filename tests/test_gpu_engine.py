@@ -84,6 +84,19 @@ def test_mixed_profile_bitexact(eng, oracle, small_torus):
     assert np.array_equal(S, r["S"]) and np.array_equal(counts, r["counts"])
 
 
+@pytest.mark.parametrize("k", [8, 32])
+def test_list_sizes_bitexact(eng, oracle, small_torus, k):
+    """The smallest and the largest supported K (K=32 is the 1M-site
+    workload's): lists, masks and positions equal the oracle's run."""
+    m, S0 = small_torus
+    S, st, counts = run_engine(eng, m, S0, k, 1, 15, profile="mixed")
+    r = oracle.lloyd_run(m.V, m.F, S0, k, 1, 15, profile=oracle.P_MIXED)
+    assert np.array_equal(st["knn"], r["knn"])
+    assert np.array_equal(counts, r["counts"])
+    assert np.array_equal(st["frozen"], r["frozen"])
+    assert np.array_equal(S, r["S"])
+
+
 @pytest.mark.parametrize("mode,profile", [(0, "ref"), (1, "mixed")])
 def test_far_centroids_bitexact(eng, oracle, mode, profile):
     """Sites cut off from the rest (a cap of 300 plus three lone sites) get
