@@ -323,14 +323,26 @@ __device__ inline int tier_of(int mode, int i, int n, int K, const uint32_t* row
 // recomputed this iteration (frozen sites keep theirs, main.cu:678); the
 // warp-aggregated append keeps runs of 32 spatially adjacent sites together
 // ---------------------------------------------------------------------------
+// It also finds each listed site's nearest mesh vertex (the frame vertex,
+// main.cu:685-700), one thread per site: the same exact grid search and key
+// order as any other, so the same vertex.
 template <class T>
 __global__ void k_active_list(EngineArgs<T> a) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   bool act = false;
   if (t < n_grid) {
-    const int g = (int)a.sorted[t].id;
-    act = !(a.segs[__ldg(a.site_seg + g)].mode != 0 && a.frozen[g]);
+    const Pt4<T> me = a.sorted[t];
+    const int g = (int)me.id;
+    const SegDev& sd = a.segs[__ldg(a.site_seg + g)];
+    act = !(sd.mode != 0 && a.frozen[g]);
+    if (act) {
+      const MeshDev& md = a.meshes[sd.mesh];
+      TopK<T, 1> nv;
+      grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, V3<T>{me.x, me.y, me.z}, nv,
+                            [](uint32_t) { return true; });
+      a.nnv[g] = (int)KeyOps<T>::idx(nv.k[0]);
+    }
   }
   const unsigned m = __ballot_sync(0xffffffffu, act);
   const int lane = threadIdx.x & 31;
@@ -345,7 +357,7 @@ __global__ void k_active_list(EngineArgs<T> a) {
 // its segment (the reference's K+1 nearest with self dropped,
 // site_knn.cuh:79-103); lane j holds the j-th neighbour, so the list row is
 // read (for the freeze test's equality) and written coalesced.
-// Sets same[g] (new list == stored list), kth[g] and the frame vertex nnv[g].
+// Sets same[g] (new list == stored list) and kth[g].
 // ---------------------------------------------------------------------------
 template <class T, int KK, int BS>
 __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
@@ -358,7 +370,6 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
   const int g = (int)me.id;
   const int s = __ldg(a.site_seg + g);
   const SegDev& sd = a.segs[s];
-  const MeshDev& md = a.meshes[sd.mesh];
   // The K nearest other sites: the reference's K+1 nearest with self dropped
   // (site_knn.cuh:79-103) are exactly these, also when duplicates of the site
   // with smaller indices push self out of the K+1 (then the first K are kept,
@@ -389,9 +400,6 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
   }
   const unsigned changed = __ballot_sync(0xffffffffu, diff);
   if (lane == 0) a.same[g] = changed ? 0 : 1;
-  // nearest mesh vertex of the site (frame vertex)
-  const auto nv = warp_nearest<T, float>(md.vg, md.vcell_start, md.vsorted, q, lane);
-  if (lane == 0) a.nnv[g] = (int)O::idx(nv);
 }
 
 // ---------------------------------------------------------------------------

@@ -314,35 +314,6 @@ __device__ __forceinline__ void warp_knn(const GridGeom& g, const int* __restric
   }
 }
 
-// Nearest point of q (uniform across the warp); every lane returns its key.
-template <class T, class PT>
-__device__ __forceinline__ typename KeyOps<T>::Key warp_nearest(const GridGeom& g, const int* __restrict__ cell_start,
-                                                                const Pt4<PT>* __restrict__ pts, V3<T> q, int lane) {
-  using O = KeyOps<T>;
-  using Key = typename O::Key;
-  Key best = O::empty();
-  if (!finite3(q)) return best;
-  const int c[3] = {grid_coord(g, q.x, 0), grid_coord(g, q.y, 1), grid_coord(g, q.z, 2)};
-  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
-  const int rmax = max(g.dim[0], max(g.dim[1], g.dim[2]));
-  const float slack = 1e-3f * g.h;
-  for (int r = 1; r <= rmax; ++r) {
-    warp_ring(g, cell_start, c[0], c[1], c[2], r, lane, [&](int pos) {
-      if (pos >= 0) {
-        const Pt4<PT> p = pts[pos];
-        best = O::kmin(best, O::make(dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q), p.id));
-      }
-    });
-#pragma unroll
-    for (int o = 16; o; o >>= 1) best = O::kmin(best, shfl_key(best, lane ^ o));
-    float m = ring_margin(g, qf, c, r);
-    if (isinf(m)) break;
-    m -= slack;
-    if (!O::is_empty(best) && m > 0.f && (double)O::dist(best) < (double)m * (double)m) break;
-  }
-  return best;
-}
-
 // ---------------------------------------------------------------------------
 // grid build: count -> exclusive scan -> scatter
 // ---------------------------------------------------------------------------
