@@ -406,7 +406,7 @@ struct cvt_mesh {
   GridGeom vg{};
   int* dvcell_start = nullptr;
   Pt4<float>* dvsorted = nullptr;
-  float4* dring = nullptr;    // one-ring records (3 per CSR entry)
+  float4* dring = nullptr;    // one-ring records (kRingWords per CSR entry)
   float* dunref = nullptr;    // input vertices no face uses (Hausdorff probes only)
   int n_unref = 0;
   BVHNode* dnodes = nullptr;  // built on first use (Hausdorff)
@@ -689,7 +689,7 @@ extern "C" cvt_status_t cvt_mesh_create(const float* V, int nV, const int* F, in
   ar.add(&m->doff, (size_t)nn + 1);
   ar.add(&m->dfcs, (size_t)n3);
   ar.add(&m->dN, 3 * (size_t)nn);
-  ar.add(&m->dring, 9 * (size_t)nF);
+  ar.add(&m->dring, (size_t)kRingWords * 3 * nF);
   ar.add(&m->dunref, 3 * (size_t)m->n_unref);
   // the vertex grid's cell array is sized after the area is known
   MCK(ar.commit(&m->arena));

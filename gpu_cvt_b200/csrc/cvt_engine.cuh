@@ -46,7 +46,7 @@ struct MeshDev {
   const float* N;
   const int* vcell_start;
   const Pt4<float>* vsorted;
-  const float4* ring;  // one-ring records, 3 per CSR entry (k_build_ring_records)
+  const float4* ring;  // one-ring records, kRingWords per CSR entry (k_build_ring_records)
   GridGeom vg;
   int nV, nF;
   float R;     // clip square half-size: longest input bbox edge (main.cu:421)

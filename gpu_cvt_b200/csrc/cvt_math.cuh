@@ -196,10 +196,20 @@ __device__ __forceinline__ V3<T> project_onering(V3<T> c, const float* __restric
 }
 
 // One-ring records: for every vertex->face CSR entry (same order as the CSR),
-// the face's three corner positions and vertex ids in three 16-byte words,
-//   r0 = {A.x, A.y, A.z, B.x}, r1 = {B.y, B.z, C.x, C.y}, r2 = {C.z, ia, ib, ic}
+// the face's three corner positions and vertex ids and a bounding sphere in
+// four 16-byte words,
+//   r0 = {A.x, A.y, A.z, B.x}, r1 = {B.y, B.z, C.x, C.y}, r2 = {C.z, ia, ib, ic},
+//   r3 = {centre.x, centre.y, centre.z, radius}
 // (ids as int bits), so a projection reads one offset and then independent
-// 16-byte loads instead of the chain CSR entry -> face -> corners.
+// 16-byte loads instead of the chain CSR entry -> face -> corners.  The
+// sphere is centred on the float-rounded centroid; its radius is the largest
+// corner distance, computed in double and rounded up, so it holds the whole
+// triangle.  radius < 0 marks a face the projection never skips: an invalid
+// entry, or a triangle with a corner angle below ~5.7 degrees
+// (sin^2 < kPruneSin2), whose face-region formula is ill-conditioned.
+constexpr int kRingWords = 4;
+constexpr double kPruneSin2 = 0.01;
+
 __global__ void k_build_ring_records(const float* __restrict__ V, const int* __restrict__ F, int nF,
                                      const int* __restrict__ fcs, long n_entries, float4* __restrict__ rec) {
   const long ii = (long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -207,28 +217,68 @@ __global__ void k_build_ring_records(const float* __restrict__ V, const int* __r
   const int fi = fcs[ii];
   int ia = -1, ib = -1, ic = -1;
   float a[3] = {0.f, 0.f, 0.f}, b[3] = {0.f, 0.f, 0.f}, c[3] = {0.f, 0.f, 0.f};
+  float4 sph = make_float4(0.f, 0.f, 0.f, -1.f);
   if ((unsigned)fi < (unsigned)nF) {
     ia = F[3 * fi]; ib = F[3 * fi + 1]; ic = F[3 * fi + 2];
     for (int k = 0; k < 3; ++k) { a[k] = V[3 * ia + k]; b[k] = V[3 * ib + k]; c[k] = V[3 * ic + k]; }
+    float m[3];
+    double r2 = 0.0;
+    for (int k = 0; k < 3; ++k) m[k] = (float)(((double)a[k] + (double)b[k] + (double)c[k]) / 3.0);
+    const float* P[3] = {a, b, c};
+    bool ok = true;
+    for (int j = 0; j < 3; ++j) {
+      double d2 = 0.0, u[3], v[3];
+      for (int k = 0; k < 3; ++k) {
+        const double d = (double)P[j][k] - (double)m[k];
+        d2 += d * d;
+        u[k] = (double)P[(j + 1) % 3][k] - (double)P[j][k];
+        v[k] = (double)P[(j + 2) % 3][k] - (double)P[j][k];
+      }
+      r2 = fmax(r2, d2);
+      const double cx = u[1] * v[2] - u[2] * v[1], cy = u[2] * v[0] - u[0] * v[2], cz = u[0] * v[1] - u[1] * v[0];
+      const double uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2], vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+      ok = ok && (cx * cx + cy * cy + cz * cz) >= kPruneSin2 * (uu * vv);  // false for NaN / zero-length edges
+    }
+    const float rad = __double2float_ru(sqrt(r2) * (1.0 + 1e-9));
+    if (ok && isfinite(rad)) sph = make_float4(m[0], m[1], m[2], rad);
   }
-  rec[3 * ii] = make_float4(a[0], a[1], a[2], b[0]);
-  rec[3 * ii + 1] = make_float4(b[1], b[2], c[0], c[1]);
-  rec[3 * ii + 2] = make_float4(c[2], __int_as_float(ia), __int_as_float(ib), __int_as_float(ic));
+  rec[kRingWords * ii] = make_float4(a[0], a[1], a[2], b[0]);
+  rec[kRingWords * ii + 1] = make_float4(b[1], b[2], c[0], c[1]);
+  rec[kRingWords * ii + 2] = make_float4(c[2], __int_as_float(ia), __int_as_float(ib), __int_as_float(ic));
+  rec[kRingWords * ii + 3] = sph;
 }
 
 // project_onering over the one-ring records: the same faces in the same
 // order, the same arithmetic, so the same result bit for bit.
+//
+// A face whose bounding sphere lies so far from c that its computed d2 must
+// be >= the best so far cannot pass the strict '<' and is skipped, which
+// leaves the result unchanged.  The lower bound on the distance from c to
+// any point the closest-point code can return for the face,
+//   lb = |c - centre| - radius - 0.05 (|c - centre| + radius)
+//        - 1e-4 max|coordinate| - 1e-4 |c - centre|^2 / radius,
+// subtracts margins far above the rounding involved: the vertex and edge
+// results lie on the triangle up to the rounding of one fma per coordinate
+// (edge parameters are in [0, 1] under correct rounding); the face-region
+// result errs by about kappa u |AP|^2 / |edge| for kappa = 1/sin^2 <= 100
+// (the corner-angle flag), unit roundoff u <= 2^-24 and |AP| <= |c - centre|
+// + radius; |c - centre| is computed in FP32 from coordinates of magnitude
+// <= max|coordinate|; and the computed d2 is >= (1 - 5u) |p - c|^2.  A face is
+// skipped when lb > 0 and lb^2 > 1.001 best.
 template <class T, class Q>
 __device__ __forceinline__ V3<T> project_onering_rec(V3<T> c, const float4* __restrict__ rec, int nV,
                                                      const int* __restrict__ off, const int* knnv, int kproj) {
   V3<Q> cq = cvt3<Q>(c), bp = cq;
   Q best = (Q)1e30;
+  const float qx = (float)c.x, qy = (float)c.y, qz = (float)c.z;
+  const float qm = fmaxf(fabsf(qx), fmaxf(fabsf(qy), fabsf(qz)));
   for (int t = 0; t < kproj; ++t) {
     int v = knnv[t];
     if ((unsigned)v >= (unsigned)nV) continue;
     int beg = __ldg(off + v), end = __ldg(off + v + 1);
     for (int ii = beg; ii < end; ++ii) {
-      const float4 r0 = __ldg(rec + 3 * ii), r1 = __ldg(rec + 3 * ii + 1), r2 = __ldg(rec + 3 * ii + 2);
+      const float4* r = rec + kRingWords * (long)ii;
+      const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
       const int ia = __float_as_int(r2.y), ib = __float_as_int(r2.z), ic = __float_as_int(r2.w);
       if (ia < 0) continue;
       bool seen = false;
@@ -237,6 +287,13 @@ __device__ __forceinline__ V3<T> project_onering_rec(V3<T> c, const float4* __re
         seen = seen || w == ia || w == ib || w == ic;
       }
       if (seen) continue;
+      if (r3.w >= 0.f) {
+        const float dx = qx - r3.x, dy = qy - r3.y, dz = qz - r3.z;
+        const float dc = __fsqrt_rn(fmaT(dz, dz, fmaT(dy, dy, dx * dx)));
+        const float mc = fmaxf(qm, fmaxf(fabsf(r3.x), fmaxf(fabsf(r3.y), fabsf(r3.z))));
+        const float lb = dc - r3.w - 0.05f * (dc + r3.w) - 1e-4f * mc - 1e-4f * divT(dc * dc, r3.w);
+        if (lb > 0.f && (double)lb * (double)lb > 1.001 * (double)best) continue;
+      }
       V3<Q> A = {(Q)r0.x, (Q)r0.y, (Q)r0.z};
       V3<Q> B = {(Q)r0.w, (Q)r1.x, (Q)r1.y};
       V3<Q> C = {(Q)r1.z, (Q)r1.w, (Q)r2.x};

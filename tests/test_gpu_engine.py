@@ -119,6 +119,42 @@ def test_far_centroids_bitexact(eng, oracle, mode, profile):
     assert np.array_equal(counts, r["counts"])
 
 
+def _unflagged_fraction(m):
+    """Share of faces with a corner angle below ~5.7 degrees (sin^2 < 0.01),
+    which the projection never skips."""
+    V = m.V.astype(np.float64)
+    P = [V[m.F[:, j]] for j in range(3)]
+    ok = np.ones(len(m.F), bool)
+    for j in range(3):
+        u, v = P[(j + 1) % 3] - P[j], P[(j + 2) % 3] - P[j]
+        cr = np.cross(u, v)
+        ok &= (cr * cr).sum(1) >= 0.01 * (u * u).sum(1) * (v * v).sum(1)
+    return 1.0 - ok.mean()
+
+
+@pytest.mark.parametrize("case", ["thin_faces", "far_from_origin"])
+@pytest.mark.parametrize("profile", ["ref", "mixed", "fp64"])
+def test_face_skip_guards_bitexact(eng, oracle, case, profile):
+    """The projection skips a face when its bounding sphere is provably
+    farther than the best face so far.  Meshes that stress the rule's
+    guards: long thin triangles, 40 % of them below the corner-angle limit
+    under which a face is never skipped, and a torus centred ~370 units from
+    the origin, where the FP32 distance to a sphere centre keeps few digits.
+    Positions, vertex lists and counts equal the oracle's run."""
+    if case == "thin_faces":
+        m = mg.torus(1.0, 0.3, 400, 12, noise_sigma=0.002, seed=4)
+        assert 0.3 < _unflagged_fraction(m) < 0.6
+    else:
+        m = mg.torus(1.0, 0.3, 80, 40, noise_sigma=0.002, seed=5, center=(300.0, -200.0, 100.0))
+        assert np.abs(m.V).max() > 250
+    S0 = mg.sample_sites(m.V, m.F, 3000, seed=6)
+    S, st, counts = run_engine(eng, m, S0, 24, 1, 12, profile=profile)
+    r = oracle.lloyd_run(m.V, m.F, S0, 24, 1, 12, profile=oracle.PROFILES[profile])
+    assert np.array_equal(S, r["S"])
+    assert np.array_equal(st["knnv"], r["knnv"])
+    assert np.array_equal(counts, r["counts"])
+
+
 @pytest.mark.parametrize("profile", ["ref", "mixed", "fp64"])
 def test_launch_shapes_same_results_and_autotune(eng, small_torus, profile):
     """Every launch shape of the KNN, clip and projection kernels gives the

@@ -150,3 +150,71 @@ def test_extract_faces_dual_mesh(oracle):
     assert F.shape[0] > len(S)                    # roughly 2 triangles per site
     assert (F[:, 0] < F[:, 1]).all() and (F[:, 1] < F[:, 2]).all()
     assert len(np.unique(F, axis=0)) == len(F)
+
+
+def _ru32(x):
+    """float64 -> float32 rounded toward +inf."""
+    r = np.float32(x)
+    return np.where(r.astype(np.float64) < x, np.nextafter(r, np.float32(np.inf)), r).astype(np.float32)
+
+
+def test_face_skip_bound_is_sound(oracle):
+    """The projection kernel skips a face when lb > 0 and lb^2 > 1.001 best,
+    lb being its lower bound on the distance from the query to whatever the
+    closest-point code returns for the face (bounding sphere about the FP32
+    centroid, radius rounded up; margins 0.05 (dc + radius) + 1e-4
+    max|coordinate| + 1e-4 dc^2 / radius; faces with a corner angle under
+    ~5.7 degrees are never skipped).  The same bound, restated here, stays
+    below the distance of the oracle's FP32 closest point (the arithmetic of
+    the FP32 profile, the one with the largest rounding) on thin triangles,
+    small and large scales, coordinates up to 1e4 and queries on, near and
+    far from the face."""
+    rng = np.random.default_rng(11)
+    n = 6000
+    scale = 10.0 ** rng.uniform(-3, 0, n)
+    base = rng.normal(size=(n, 3)) * (10.0 ** rng.uniform(-1, 4, n))[:, None]
+    # corners: half random shapes, half thin ones near the angle limit
+    a = np.zeros((n, 3))
+    b = np.stack([np.ones(n), np.zeros(n), np.zeros(n)], 1)
+    ang = np.where(rng.random(n) < 0.5, rng.uniform(0.3, 2.5, n), rng.uniform(0.101, 0.2, n))
+    ln = rng.uniform(0.3, 1.0, n)
+    c = np.stack([ln * np.cos(ang), ln * np.sin(ang), np.zeros(n)], 1)
+    q, _ = np.linalg.qr(rng.normal(size=(n, 3, 3)))
+    rot = lambda x: np.einsum("nij,nj->ni", q, x) * scale[:, None] + base
+    A, B, C = (rot(x).astype(np.float32) for x in (a, b, c))
+    A64, B64, C64 = (x.astype(np.float64) for x in (A, B, C))
+    m = ((A64 + B64 + C64) / 3.0).astype(np.float32)
+    r2 = np.max([((X - m.astype(np.float64)) ** 2).sum(1) for X in (A64, B64, C64)], axis=0)
+    rad = _ru32(np.sqrt(r2) * (1.0 + 1e-9))
+    P = [A64, B64, C64]
+    flag = np.ones(n, bool)
+    for j in range(3):
+        u, v = P[(j + 1) % 3] - P[j], P[(j + 2) % 3] - P[j]
+        cr = np.cross(u, v)
+        flag &= (cr * cr).sum(1) >= 0.01 * (u * u).sum(1) * (v * v).sum(1)
+    # triangles that FP32 collapses (tiny faces at coordinates of ~1e4) have
+    # no normal; the angle flag already excludes them
+    nrm = np.cross(B64 - A64, C64 - A64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+    checked = 0
+    worst = np.inf
+    for trial in range(3):
+        w = rng.uniform(-0.5, 1.5, (n, 3))
+        w /= w.sum(1, keepdims=True)
+        on = w[:, :1] * A64 + w[:, 1:2] * B64 + w[:, 2:] * C64
+        h = scale * 10.0 ** rng.uniform(-5, 2, n) * rng.choice([-1.0, 1.0], n)
+        Q = (on + h[:, None] * nrm).astype(np.float32)
+        d = Q - m
+        dc = np.sqrt((d * d).sum(1, dtype=np.float32)).astype(np.float32)
+        mc = np.maximum(np.abs(Q).max(1), np.abs(m).max(1))
+        lb = (dc - rad - np.float32(0.05) * (dc + rad) - np.float32(1e-4) * mc
+              - np.float32(1e-4) * (dc * dc / rad)).astype(np.float32)
+        for i in np.nonzero(flag & (lb > 0))[0]:
+            p = oracle.closest_point_tri(Q[i], A[i], B[i], C[i]).astype(np.float64)
+            d2 = float(((p - Q[i].astype(np.float64)) ** 2).sum())
+            ratio = d2 / (float(lb[i]) ** 2)
+            worst = min(worst, ratio)
+            checked += 1
+    assert checked > 5000
+    assert worst >= 1.0, f"bound above the computed distance: d2 / lb^2 = {worst}"
