@@ -135,6 +135,37 @@ static int sm_count() {
   return n > 0 ? n : 148;
 }
 
+// Streams a host thread runs engine iterations on besides the caller's: the
+// second branch of an eagerly launched iteration, and the origin and second
+// branch of a graph capture.  One set per thread and device, because a
+// capture in cudaStreamCaptureModeThreadLocal must not share a stream with
+// another thread's work; created on first use, destroyed at thread exit.
+// (Creating and destroying streams per engine cost ~0.3 ms per one-call
+// remesh.)
+struct ThreadStreams {
+  cudaStream_t side = nullptr, cap = nullptr, cap_side = nullptr;
+};
+struct ThreadStreamSet {
+  std::vector<ThreadStreams> dev;
+  ~ThreadStreamSet() {
+    for (ThreadStreams& t : dev)
+      for (cudaStream_t s : {t.side, t.cap, t.cap_side})
+        if (s) cudaStreamDestroy(s);
+  }
+};
+static cudaError_t thread_streams(ThreadStreams** out) {
+  static thread_local ThreadStreamSet set;
+  int d = 0;
+  cudaError_t e = cudaGetDevice(&d);
+  if (e != cudaSuccess) return e;
+  if ((int)set.dev.size() <= d) set.dev.resize(d + 1);
+  ThreadStreams& t = set.dev[d];
+  for (cudaStream_t* s : {&t.side, &t.cap, &t.cap_side})
+    if (!*s && (e = cudaStreamCreateWithFlags(s, cudaStreamNonBlocking)) != cudaSuccess) return e;
+  *out = &t;
+  return cudaSuccess;
+}
+
 // stream-ordered scratch
 struct Scratch {
   cudaStream_t st;
@@ -994,6 +1025,9 @@ struct cvt_engine {
   void* d_cent = nullptr;
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  // fork / join of the frame-vertex search, which runs on a second stream
+  // while the site KNN runs: for eager iterations and for graph captures
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_cfork = nullptr, ev_cjoin = nullptr;
   int graph_nodes = 0;
   long long last_launches = 0;
 };
@@ -1002,6 +1036,8 @@ static void engine_free(cvt_engine* e) {
   if (!e) return;
   for (int k = 0; k < 2; ++k)
     if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
+  for (cudaEvent_t ev : {e->ev_fork, e->ev_join, e->ev_cfork, e->ev_cjoin})
+    if (ev) cudaEventDestroy(ev);
   dev_free_sync(e->arena);
   delete e;
 }
@@ -1083,6 +1119,8 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   k_fill_int<<<cdiv((long)ns, 256), 256>>>(e->d_site_seg, (int)ns, -1);
   LAUNCHED(1);
   ECK(cudaGetLastError());
+  for (cudaEvent_t* ev : {&e->ev_fork, &e->ev_join, &e->ev_cfork, &e->ev_cjoin})
+    ECK(cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
   ECK(cudaDeviceSynchronize());
 #undef ECK
   *out = e;
@@ -1233,11 +1271,18 @@ static void launch_site_proj(const EngineArgs<typename PT<PROF>::T>& a, int pari
 }
 
 
+// the second branch of an iteration: its stream and the fork / join events
+struct Branch {
+  cudaStream_t side;
+  cudaEvent_t fork, join;
+};
+
 // ev (optional, 6 events): recorded before the grid build, after it, after
 // the KNN kernel, after the clip kernels, after the projection kernels and
 // after the bookkeeping kernel
 template <int PROF>
-static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t st, int* nlaunch, cudaEvent_t* ev) {
+static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t st, const Branch& br, int* nlaunch,
+                                        cudaEvent_t* ev) {
   using T = typename PT<PROF>::T;
   using PP = typename PT<PROF>::PP;
   EngineArgs<T> a = engine_args<T>(e);
@@ -1257,6 +1302,13 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   // d_act_count is zero here: set at creation, reset by the bookkeeping
   k_active_list<T><<<cdiv(ns, 256), 256, 0, st>>>(a);
   L++;
+  // the frame vertices are first read by the clip: search them on the side
+  // stream while the site KNN runs
+  CK(cudaEventRecord(br.fork, st));
+  CK(cudaStreamWaitEvent(br.side, br.fork, 0));
+  k_frame_vertex<T><<<cdiv(ns, 128), 128, 0, br.side>>>(a);
+  CK(cudaEventRecord(br.join, br.side));
+  L++;
   if (ev) CK(cudaEventRecord(ev[1], st));
   switch (e->K) {
     case 8: launch_site_knn<T, 8>(a, ns, e->p.knn_block, st); break;
@@ -1268,6 +1320,7 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   }
   L++;
   if (ev) CK(cudaEventRecord(ev[2], st));
+  CK(cudaStreamWaitEvent(st, br.join, 0));
   launch_site_clip<PROF>(a, parity, ns, e->p.clip_block, st);
   k_clip_overflow<PROF><<<e->num_sms, 64, 0, st>>>(a, parity);
   L += 2;
@@ -1282,12 +1335,12 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   return CVT_OK;
 }
 
-static cvt_status_t enqueue_iteration(cvt_engine* e, int parity, cudaStream_t st, int* nlaunch,
+static cvt_status_t enqueue_iteration(cvt_engine* e, int parity, cudaStream_t st, const Branch& br, int* nlaunch,
                                       cudaEvent_t* ev = nullptr) {
   switch (e->p.profile) {
-    case CVT_PROFILE_REF: return enqueue_iteration_t<PROF_REF>(e, parity, st, nlaunch, ev);
-    case CVT_PROFILE_MIXED: return enqueue_iteration_t<PROF_MIXED>(e, parity, st, nlaunch, ev);
-    default: return enqueue_iteration_t<PROF_FP64>(e, parity, st, nlaunch, ev);
+    case CVT_PROFILE_REF: return enqueue_iteration_t<PROF_REF>(e, parity, st, br, nlaunch, ev);
+    case CVT_PROFILE_MIXED: return enqueue_iteration_t<PROF_MIXED>(e, parity, st, br, nlaunch, ev);
+    default: return enqueue_iteration_t<PROF_FP64>(e, parity, st, br, nlaunch, ev);
   }
 }
 
@@ -1302,32 +1355,35 @@ extern "C" cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream) 
   cudaStream_t st = S_(stream);
   cvt_status_t s = CVT_OK;
   long long launches = 0;
+  ThreadStreams* ts = nullptr;
+  if (iters > 0) CK(thread_streams(&ts));
+  const Branch eager{ts ? ts->side : nullptr, e->ev_fork, e->ev_join};
   for (int it = 0; it < iters; ++it) {
     int par = e->parity;
     int nl = 0;
-    if (e->p.use_graph) {
-      if (!e->gexec[par]) {
-        cudaStream_t cs;
-        CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-        CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-        cvt_status_t q = enqueue_iteration(e, par, cs, &nl);
+    if (e->p.use_graph && e->gexec[par]) {
+      CK(cudaGraphLaunch(e->gexec[par], st));
+      nl = e->graph_nodes;
+      LAUNCHED(nl);
+    } else {
+      // an iteration without a graph yet runs eagerly; its graph is then
+      // captured and instantiated while the GPU runs it
+      s = enqueue_iteration(e, par, st, eager, &nl);
+      if (s != CVT_OK) return s;
+      LAUNCHED(nl);
+      if (e->p.use_graph) {
+        int ng = 0;
+        CK(cudaStreamBeginCapture(ts->cap, cudaStreamCaptureModeThreadLocal));
+        cvt_status_t q = enqueue_iteration(e, par, ts->cap, Branch{ts->cap_side, e->ev_cfork, e->ev_cjoin}, &ng);
         cudaGraph_t gr = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(cs, &gr);
-        cudaStreamDestroy(cs);
+        cudaError_t ce = cudaStreamEndCapture(ts->cap, &gr);
         if (q != CVT_OK) { if (gr) cudaGraphDestroy(gr); return q; }
         if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
         ce = cudaGraphInstantiate(&e->gexec[par], gr, 0);
         cudaGraphDestroy(gr);
         if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-        e->graph_nodes = nl;
+        e->graph_nodes = ng;
       }
-      CK(cudaGraphLaunch(e->gexec[par], st));
-      nl = e->graph_nodes;
-      LAUNCHED(nl);
-    } else {
-      s = enqueue_iteration(e, par, st, &nl);
-      if (s != CVT_OK) return s;
-      LAUNCHED(nl);
     }
     launches += nl;
     e->parity ^= 1;
@@ -1341,12 +1397,14 @@ extern "C" cvt_status_t cvt_engine_profile(cvt_engine_t e, int iters, float* ms,
   if (!e || !ms || iters < 1) return fail(CVT_ERR_INVALID, "cvt_engine_profile: bad arguments");
   cudaStream_t st = S_(stream);
   cvt_status_t s = CVT_OK;
+  ThreadStreams* ts = nullptr;
+  CK(thread_streams(&ts));
   cudaEvent_t ev[6];
   for (int k = 0; k < 6; ++k) CK(cudaEventCreate(&ev[k]));
   double acc[5] = {0, 0, 0, 0, 0};
   for (int it = 0; it < iters; ++it) {
     int nl = 0;
-    s = enqueue_iteration(e, e->parity, st, &nl, ev);
+    s = enqueue_iteration(e, e->parity, st, Branch{ts->side, e->ev_fork, e->ev_join}, &nl, ev);
     if (s != CVT_OK) break;
     LAUNCHED(nl);
     e->parity ^= 1;

@@ -1,11 +1,14 @@
 // Fused Lloyd-iteration kernels over many (mesh, site set) segments.
 //
 // One iteration (main.cu:669-881 per segment) is:
-//   grid build over all active sites   (count -> scan -> scatter)
-//   k_site_knn   per site: exact (K+1)-NN in its segment, drop self
-//                (site_knn.cuh:79), restore the previous list for frozen
-//                sites (main.cu:678), nearest mesh vertex for the frame
-//                (main.cu:685-700)
+//   grid build over the sites of active segments (count -> scan -> scatter)
+//   k_active_list  the non-frozen sites
+//   k_frame_vertex the mesh vertex nearest to each of them (its normal
+//                gives the frame, main.cu:685-700), on a second stream
+//                while k_site_knn runs
+//   k_site_knn   per active site (one warp): exact (K+1)-NN in its segment,
+//                drop self (site_knn.cuh:79); frozen sites keep the
+//                previous list (main.cu:678)
 //   k_site_clip  per site (one thread): frame (site_normals.cuh:69),
 //                tangent-plane clip and centroid (2dClip.cuh:82)
 //   k_clip_overflow  the same for the rare cells whose polygon outgrows
@@ -323,26 +326,15 @@ __device__ inline int tier_of(int mode, int i, int n, int K, const uint32_t* row
 // recomputed this iteration (frozen sites keep theirs, main.cu:678); the
 // warp-aggregated append keeps runs of 32 spatially adjacent sites together
 // ---------------------------------------------------------------------------
-// It also finds each listed site's nearest mesh vertex (the frame vertex,
-// main.cu:685-700), one thread per site: the same exact grid search and key
-// order as any other, so the same vertex.
 template <class T>
 __global__ void k_active_list(EngineArgs<T> a) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   bool act = false;
   if (t < n_grid) {
-    const Pt4<T> me = a.sorted[t];
-    const int g = (int)me.id;
+    const int g = (int)a.sorted[t].id;
     const SegDev& sd = a.segs[__ldg(a.site_seg + g)];
     act = !(sd.mode != 0 && a.frozen[g]);
-    if (act) {
-      const MeshDev& md = a.meshes[sd.mesh];
-      TopK<T, 1> nv;
-      grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, V3<T>{me.x, me.y, me.z}, nv,
-                            [](uint32_t) { return true; });
-      a.nnv[g] = (int)KeyOps<T>::idx(nv.k[0]);
-    }
   }
   const unsigned m = __ballot_sync(0xffffffffu, act);
   const int lane = threadIdx.x & 31;
@@ -350,6 +342,25 @@ __global__ void k_active_list(EngineArgs<T> a) {
   if (lane == 0 && m) base = atomicAdd(a.act_count, __popc(m));
   base = __shfl_sync(0xffffffffu, base, 0);
   if (act) a.act[base + __popc(m & ((1u << lane) - 1u))] = t;
+}
+
+// ---------------------------------------------------------------------------
+// k_frame_vertex: each listed site's nearest mesh vertex (the frame vertex,
+// main.cu:685-700), one thread per site: the same exact grid search and key
+// order as any other, so the same vertex.  Runs on a second stream while
+// k_site_knn runs; k_site_clip is the first kernel to read a.nnv.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_frame_vertex(EngineArgs<T> a) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= __ldg(a.act_count)) return;
+  const Pt4<T> me = a.sorted[a.act[w]];
+  const int g = (int)me.id;
+  const MeshDev& md = a.meshes[a.segs[__ldg(a.site_seg + g)].mesh];
+  TopK<T, 1> nv;
+  grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, V3<T>{me.x, me.y, me.z}, nv,
+                        [](uint32_t) { return true; });
+  a.nnv[g] = (int)KeyOps<T>::idx(nv.k[0]);
 }
 
 // ---------------------------------------------------------------------------

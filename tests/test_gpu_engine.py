@@ -188,6 +188,50 @@ def test_fp64_profile_matches_fp64_oracle(eng, oracle, c1):
     assert np.array_equal(counts, r["counts"])
 
 
+def test_graph_eager_and_threads_same_results(eng, c1, small_torus):
+    """The same run launched three ways gives the same sites bit for bit:
+    eagerly (use_graph off), through the per-parity graphs (the first
+    iteration of each parity runs eagerly while its graph is captured), and
+    from two host threads at once, each with its own engine (the second
+    stream of an iteration and the capture streams belong to the thread)."""
+    import threading
+
+    def run(mesh_np, S0, graph, iters=12):
+        m = eng.Mesh(mesh_np.V, mesh_np.F)
+        e = eng.Engine(eng.params(k=20, mode=1, profile="mixed", use_graph=graph), 1, len(S0),
+                       eng.grid_cells(m, len(S0), 20))
+        seg = e.add(m, S0)
+        e.run(5)
+        e.run(iters - 5)
+        out = e.sites(seg)
+        e.close()
+        m.close()
+        return out
+
+    cases = [c1, small_torus]
+    ref = [run(m, S0, False) for m, S0 in cases]
+    for (m, S0), r in zip(cases, ref):
+        assert np.array_equal(run(m, S0, True), r)
+    got = [None, None]
+    errs = []
+
+    def worker(i):
+        try:
+            with torch.cuda.device(0):
+                got[i] = run(*cases[i], True)
+        except Exception as ex:  # reported below
+            errs.append(ex)
+
+    th = [threading.Thread(target=worker, args=(i,)) for i in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=120)
+    assert not errs, errs
+    for g, r in zip(got, ref):
+        assert g is not None and np.array_equal(g, r)
+
+
 def test_batched_segments_equal_alone(eng, c1, small_torus):
     """Three meshes in one engine give, per mesh, the same bits as alone."""
     (m1, S1), (m2, S2) = c1, small_torus
