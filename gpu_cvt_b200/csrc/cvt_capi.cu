@@ -116,7 +116,10 @@ static void dev_free_sync(void* p) {
   if (p) { cudaFreeAsync(p, 0); cudaStreamSynchronize(0); }
 }
 
+static void graph_cache_clear();
+
 extern "C" cvt_status_t cvt_release_cached_memory(void) {
+  graph_cache_clear();
   std::lock_guard<std::mutex> lk(g_pool_mu);
   for (cudaMemPool_t pool : g_pools)
     if (pool) {
@@ -1032,10 +1035,72 @@ struct cvt_engine {
   long long last_launches = 0;
 };
 
+// Instantiated iteration graphs of destroyed engines, kept for reuse: an
+// engine whose iteration has the same shape (device, precision profile, K,
+// launch shapes: the same kernels in the same order) loads its own kernel
+// parameters into a kept graph with cudaGraphExecUpdate instead of
+// instantiating a new one, and a destroyed engine hands its graphs back
+// instead of destroying them (destroying two cost ~0.3 ms per one-call
+// remesh).  At most kGraphCacheMax are kept; cvt_release_cached_memory
+// destroys them.
+struct GraphKey {
+  int dev, profile, k, knn_block, clip_block, proj_block;
+  bool operator==(const GraphKey& o) const {
+    return dev == o.dev && profile == o.profile && k == o.k && knn_block == o.knn_block &&
+           clip_block == o.clip_block && proj_block == o.proj_block;
+  }
+};
+constexpr size_t kGraphCacheMax = 16;
+static std::mutex g_graph_mu;
+static std::vector<std::pair<GraphKey, cudaGraphExec_t>> g_graph_cache;
+
+static GraphKey graph_key(const cvt_engine* e) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return {dev, e->p.profile, e->K, e->p.knn_block, e->p.clip_block, e->p.proj_block};
+}
+
+static cudaGraphExec_t graph_cache_take(const GraphKey& k) {
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  for (size_t i = 0; i < g_graph_cache.size(); ++i)
+    if (g_graph_cache[i].first == k) {
+      cudaGraphExec_t x = g_graph_cache[i].second;
+      g_graph_cache.erase(g_graph_cache.begin() + i);
+      return x;
+    }
+  return nullptr;
+}
+
+static void graph_cache_put(const GraphKey& k, cudaGraphExec_t x) {
+  {
+    std::lock_guard<std::mutex> lk(g_graph_mu);
+    if (g_graph_cache.size() < kGraphCacheMax) { g_graph_cache.emplace_back(k, x); return; }
+  }
+  cudaGraphExecDestroy(x);
+}
+
+static void graph_cache_clear() {
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  for (auto& kv : g_graph_cache) cudaGraphExecDestroy(kv.second);
+  g_graph_cache.clear();
+}
+
+// the graph of this iteration: a kept graph of the same shape updated with
+// gr's parameters, else a new instantiation
+static cudaError_t graph_exec_for(const GraphKey& k, cudaGraph_t gr, cudaGraphExec_t* out) {
+  if (cudaGraphExec_t x = graph_cache_take(k)) {
+    cudaGraphExecUpdateResultInfo info{};
+    if (cudaGraphExecUpdate(x, gr, &info) == cudaSuccess) { *out = x; return cudaSuccess; }
+    cudaGetLastError();  // a rejected update leaves no sticky error
+    cudaGraphExecDestroy(x);
+  }
+  return cudaGraphInstantiate(out, gr, 0);
+}
+
 static void engine_free(cvt_engine* e) {
   if (!e) return;
   for (int k = 0; k < 2; ++k)
-    if (e->gexec[k]) cudaGraphExecDestroy(e->gexec[k]);
+    if (e->gexec[k]) graph_cache_put(graph_key(e), e->gexec[k]);
   for (cudaEvent_t ev : {e->ev_fork, e->ev_join, e->ev_cfork, e->ev_cjoin})
     if (ev) cudaEventDestroy(ev);
   dev_free_sync(e->arena);
@@ -1379,7 +1444,7 @@ extern "C" cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream) 
         cudaError_t ce = cudaStreamEndCapture(ts->cap, &gr);
         if (q != CVT_OK) { if (gr) cudaGraphDestroy(gr); return q; }
         if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&e->gexec[par], gr, 0);
+        ce = graph_exec_for(graph_key(e), gr, &e->gexec[par]);
         cudaGraphDestroy(gr);
         if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
         e->graph_nodes = ng;

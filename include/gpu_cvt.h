@@ -169,8 +169,10 @@ cvt_status_t cvt_quality(const float* V, const int* F, int nF, float* out, void*
 
 /* Device memory of meshes, engines and call temporaries comes from one
  * stream-ordered pool per device that keeps freed memory for reuse, so calls
- * after the first allocate nothing from the driver.  This hands the cached,
- * unused part back (e.g. before another library needs the HBM). */
+ * after the first allocate nothing from the driver; destroyed engines also
+ * leave their instantiated iteration graphs (at most 16) for the next engine
+ * of the same shape.  This hands the cached, unused memory back and destroys
+ * the kept graphs (e.g. before another library needs the HBM). */
 cvt_status_t cvt_release_cached_memory(void);
 
 /* ======================================================================

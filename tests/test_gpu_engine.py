@@ -232,6 +232,33 @@ def test_graph_eager_and_threads_same_results(eng, c1, small_torus):
         assert g is not None and np.array_equal(g, r)
 
 
+def test_kept_graphs_reused_across_engines(eng, c1, small_torus):
+    """A destroyed engine leaves its instantiated iteration graphs for the
+    next engine of the same shape, which loads its own pointers and grid
+    sizes into them.  Runs on other meshes and site counts through kept
+    graphs equal runs through freshly instantiated ones."""
+    from gpu_cvt_b200 import _lib
+
+    def run(mesh_np, S0):
+        m = eng.Mesh(mesh_np.V, mesh_np.F)
+        e = eng.Engine(eng.params(k=24, mode=1, profile="mixed"), 1, len(S0), eng.grid_cells(m, len(S0), 24))
+        seg = e.add(m, S0)
+        e.run(8)
+        out = e.sites(seg)
+        e.close()
+        m.close()
+        return out
+
+    cases = [small_torus, c1, (small_torus[0], small_torus[1][:1500])]
+    fresh = []
+    for m, S0 in cases:
+        _lib.call("cvt_release_cached_memory")
+        fresh.append(run(m, S0))
+    for _ in range(2):
+        for (m, S0), f in zip(cases, fresh):
+            assert np.array_equal(run(m, S0), f)
+
+
 def test_batched_segments_equal_alone(eng, c1, small_torus):
     """Three meshes in one engine give, per mesh, the same bits as alone."""
     (m1, S1), (m2, S2) = c1, small_torus
