@@ -985,6 +985,7 @@ __global__ void k_f64_to_f32(const double* a, float* b, long n) {
 struct cvt_engine {
   cvt_params_t p{};
   int K = 24, max_seg = 0, max_sites = 0, max_cells = 0;
+  int dev = 0;  // device the engine lives on
   bool f64 = false;
   // host mirrors
   std::vector<SegDev> segs;
@@ -1055,9 +1056,7 @@ static std::mutex g_graph_mu;
 static std::vector<std::pair<GraphKey, cudaGraphExec_t>> g_graph_cache;
 
 static GraphKey graph_key(const cvt_engine* e) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  return {dev, e->p.profile, e->K, e->p.knn_block, e->p.clip_block, e->p.proj_block};
+  return {e->dev, e->p.profile, e->K, e->p.knn_block, e->p.clip_block, e->p.proj_block};
 }
 
 static cudaGraphExec_t graph_cache_take(const GraphKey& k) {
@@ -1124,6 +1123,7 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   cvt_engine* e = new cvt_engine();
   e->p = q;
   e->num_sms = sm_count();
+  cudaGetDevice(&e->dev);
   e->K = p->k;
   e->f64 = p->profile == CVT_PROFILE_FP64;
   e->max_seg = max_segments;
