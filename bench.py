@@ -149,6 +149,31 @@ def traffic_from_profiles(kernel_key):
     return d.get(kernel_key)
 
 
+def issue_roofline(prof, iters, sm_mhz):
+    """Warp-instruction issue rate of the site kernels against the B200's
+    issue peak (SMs x 4 schedulers x SM clock), the bound these kernels meet
+    long before HBM.  Warp instructions per remesh of this workload come from
+    profiles/instructions.json (ncu smsp__inst_executed.sum over the launches
+    of one remesh), the kernel times from this run's CUDA events (the
+    projection group includes the deferred-site kernel and the bookkeeping)."""
+    path = os.path.join(ROOT, "profiles", "instructions.json")
+    if not os.path.exists(path) or not sm_mhz:
+        return None
+    with open(path) as fh:
+        counts = json.load(fh)["warp_instructions_per_remesh"]
+    import torch
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    peak = sms * 4 * sm_mhz * 1e6
+    out = {"bound": "issue", "unit": "warp instructions/s", "peak": peak,
+           "peak_from": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz (median SM clock of the timed region)",
+           "counts": "profiles/instructions.json", "kernels": {}}
+    for kernel, group in (("k_site_knn", "knn"), ("k_site_clip", "clip"), ("k_site_proj", "proj")):
+        if kernel in counts and prof.get(group, 0) > 0:
+            achieved = counts[kernel] / (prof[group] * 1e-3 * iters)
+            out["kernels"][kernel] = {"achieved": achieved, "frac": achieved / peak}
+    return out
+
+
 # ---------------------------------------------------------------------------
 def cpu_baseline(m, S, p, budget_s=15.0):
     """The oracle port of the reference's algorithm on the host cores."""
@@ -348,7 +373,9 @@ def run_ours(args):
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "api": "cvt_remesh (host buffers)",
                         "same_sites_as_engine": same_as_engine},
                 "gpu_launches": int(sum(launches)),
-                "roofline": roofline, "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
+                "roofline": roofline,
+                "issue_roofline": issue_roofline(prof, iters, clk.get("sm_mhz") or clk.get("sm_max_mhz")),
+                "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
                 "libgpucvt_launches_total": _lib.launch_count()}
         print(json.dumps(line), flush=True)
     if ws > 1:
