@@ -1423,38 +1423,40 @@ extern "C" cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream) 
   ThreadStreams* ts = nullptr;
   if (iters > 0) CK(thread_streams(&ts));
   const Branch eager{ts ? ts->side : nullptr, e->ev_fork, e->ev_join};
+  e->last_launches = 0;
   for (int it = 0; it < iters; ++it) {
-    int par = e->parity;
+    const int par = e->parity;
+    const bool capture = e->p.use_graph && !e->gexec[par];
     int nl = 0;
-    if (e->p.use_graph && e->gexec[par]) {
+    if (e->p.use_graph && !capture) {
       CK(cudaGraphLaunch(e->gexec[par], st));
       nl = e->graph_nodes;
-      LAUNCHED(nl);
     } else {
       // an iteration without a graph yet runs eagerly; its graph is then
       // captured and instantiated while the GPU runs it
       s = enqueue_iteration(e, par, st, eager, &nl);
       if (s != CVT_OK) return s;
-      LAUNCHED(nl);
-      if (e->p.use_graph) {
-        int ng = 0;
-        CK(cudaStreamBeginCapture(ts->cap, cudaStreamCaptureModeThreadLocal));
-        cvt_status_t q = enqueue_iteration(e, par, ts->cap, Branch{ts->cap_side, e->ev_cfork, e->ev_cjoin}, &ng);
-        cudaGraph_t gr = nullptr;
-        cudaError_t ce = cudaStreamEndCapture(ts->cap, &gr);
-        if (q != CVT_OK) { if (gr) cudaGraphDestroy(gr); return q; }
-        if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
-        ce = graph_exec_for(graph_key(e), gr, &e->gexec[par]);
-        cudaGraphDestroy(gr);
-        if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
-        e->graph_nodes = ng;
-      }
     }
+    LAUNCHED(nl);
+    // the iteration is enqueued: account for it before anything can fail
     launches += nl;
+    e->last_launches = launches;
     e->parity ^= 1;
     for (int k = 0; k < e->max_seg; ++k) if (e->active[k] == 1) e->host_iters[k]++;
+    if (capture) {
+      int ng = 0;
+      CK(cudaStreamBeginCapture(ts->cap, cudaStreamCaptureModeThreadLocal));
+      cvt_status_t q = enqueue_iteration(e, par, ts->cap, Branch{ts->cap_side, e->ev_cfork, e->ev_cjoin}, &ng);
+      cudaGraph_t gr = nullptr;
+      cudaError_t ce = cudaStreamEndCapture(ts->cap, &gr);
+      if (q != CVT_OK) { if (gr) cudaGraphDestroy(gr); return q; }
+      if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+      ce = graph_exec_for(graph_key(e), gr, &e->gexec[par]);
+      cudaGraphDestroy(gr);
+      if (ce != cudaSuccess) return fail(CVT_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ce));
+      e->graph_nodes = ng;
+    }
   }
-  e->last_launches = launches;
   return CVT_OK;
 }
 

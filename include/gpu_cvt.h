@@ -273,7 +273,12 @@ cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, const float
                                     int sites_on_device, int* seg_id, void* stream);
 /* Free a segment's slot (its sites stop being iterated at once). */
 cvt_status_t cvt_engine_remove_segment(cvt_engine_t e, int seg_id);
-/* Run `iters` Lloyd iterations of every active segment (asynchronous). */
+/* Run `iters` Lloyd iterations of every active segment (asynchronous).  With
+ * use_graph, each iteration replays one of two CUDA graphs (one per buffer
+ * parity); an iteration whose graph does not exist yet is launched directly,
+ * and its graph is captured while the GPU runs it.  Each iteration forks a
+ * second stream owned by the calling host thread.  One engine must not run
+ * from two threads at once. */
 cvt_status_t cvt_engine_run(cvt_engine_t e, int iters, void* stream);
 /* Copy a segment's current sites out (n*3 floats; FP64 engines convert).
  * Synchronous (it reads the segment's iteration count from the device). */
