@@ -397,7 +397,7 @@ def run_batched(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"batched_{args.meshes}_meshes", "seed": 3, "k": 24, "iters": 100, "mode": 0,
                        "profile": "ref", "sites_total": r["sites_total"],
-                       "tris_per_mesh": [r["tris_min"], r["tris_max"]]},
+                       "tris_per_mesh": [r["tris_min"], r["tris_max"]], "tiles": r["tiles"]},
             "plain_loop": {"value": r["plain_sites_iters_per_s"], "ms": r["plain_loop_s"] * 1e3},
             "batched_over_plain": r["speedup"], "identical_results": r["identical_results"],
             "mesh_generation_s": r["mesh_generation_s"]}
@@ -418,23 +418,29 @@ def run_serve(args):
     meshes, reqs = server.request_stream(n_requests=args.requests, rate=200.0, site_lo=2_000, site_hi=2_000_000,
                                          n_meshes=8, seed=4)
     gen_s = time.perf_counter() - t0
+    # launch shapes tuned on the largest request (untimed), used by both loops
+    from gpu_cvt_b200 import engine as E, meshgen as mg, workloads
+    big = max(reqs, key=lambda r: r.n)
+    Vb, Fb = meshes[big.mesh]
+    prm, tune_ms = workloads.tune_for(Vb, Fb, mg.sample_sites(Vb, Fb, big.n, seed=big.seed % (2**31)), k=24, mode=1,
+                                      profile="mixed")
     # warm-up: graph capture and first-touch costs on a tiny stream
     wm, wr = server.request_stream(n_requests=4, rate=1000.0, site_lo=1000, site_hi=5000, n_meshes=1, seed=5)
-    srv = server.RemeshServer(meshes, hbm_budget=args.hbm_gb << 30, max_segments=64)
-    srv_w = server.RemeshServer(wm, hbm_budget=64 << 20, max_segments=4)
+    srv = server.RemeshServer(meshes, hbm_budget=args.hbm_gb << 30, max_segments=64, prm=prm)
+    srv_w = server.RemeshServer(wm, hbm_budget=64 << 20, max_segments=4, prm=prm)
     srv_w.run(wr)
     srv_w.close()
     plain_reqs = [copy.copy(r) for r in reqs]
     served = srv.run(reqs)
     srv.close()
-    plain = server.serve_plain(srv.M, plain_reqs)
+    plain = server.serve_plain(srv.M, plain_reqs, prm=prm)
     line = {"metric": METRIC, "value": served["sites_iters_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1,
             "warmup": 1, "ms_per_step": served["makespan_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "serve_poisson", "requests": args.requests, "rate_per_s": 200.0, "seed": 4,
                        "sites_per_request": [2000, 2000000], "stop": "max motion < 1e-4 bbox diag, cap 150",
                        "k": 24, "mode": 1, "profile": "mixed", "hbm_budget_gb": args.hbm_gb,
-                       "sites_total": int(sum(r.n for r in reqs))},
+                       "sites_total": int(sum(r.n for r in reqs)), "tiles": E.tiles(prm)},
             "latency_s": {"p50": served["latency_p50_s"], "p99": served["latency_p99_s"],
                           "mean": served["latency_mean_s"]},
             "served": served, "plain_fifo": plain,

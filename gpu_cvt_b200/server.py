@@ -70,7 +70,7 @@ def _percentile(x, q):
 
 class RemeshServer:
     def __init__(self, meshes, k=24, mode=1, profile="mixed", hbm_budget=4 << 30, max_segments=64, tol=1e-4,
-                 max_iters=150, chunk=5, keep_results=False):
+                 max_iters=150, chunk=5, keep_results=False, prm=None):
         import torch
         self.torch = torch
         self.M = [m if isinstance(m, E.Mesh) else E.Mesh(*m) for m in meshes]
@@ -80,8 +80,8 @@ class RemeshServer:
         self.max_sites = int(hbm_budget // (per_site + 4 * BYTES_PER_CELL))
         self.max_cells = int(4 * self.max_sites + 65 * max_segments)
         self.max_segments = max_segments
-        self.engine = E.Engine(E.params(k=k, mode=mode, profile=profile), max_segments, self.max_sites,
-                               self.max_cells)
+        self.engine = E.Engine(prm if prm is not None else E.params(k=k, mode=mode, profile=profile), max_segments,
+                               self.max_sites, self.max_cells)
         self.keep_results = keep_results
         self.stream = torch.cuda.current_stream()
         self.sp = C.c_void_p(self.stream.cuda_stream)
@@ -151,13 +151,13 @@ class RemeshServer:
 
 
 def serve_plain(meshes, requests, k=24, mode=1, profile="mixed", tol=1e-4, max_iters=150, chunk=5,
-                keep_results=False):
+                keep_results=False, prm=None):
     """The baseline: one request at a time, first come first served."""
     import torch
     M = [m if isinstance(m, E.Mesh) else E.Mesh(*m) for m in meshes]
     nmax = max(r.n for r in requests)
     cells = max(E.grid_cells(M[r.mesh], r.n, k) for r in requests)
-    eng = E.Engine(E.params(k=k, mode=mode, profile=profile), 1, nmax, cells)
+    eng = E.Engine(prm if prm is not None else E.params(k=k, mode=mode, profile=profile), 1, nmax, cells)
     sp = C.c_void_p(torch.cuda.current_stream().cuda_stream)
     launches = 0
     t0 = time.perf_counter()

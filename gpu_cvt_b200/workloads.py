@@ -37,14 +37,15 @@ def _sync():
     torch.cuda.synchronize()
 
 
-def run_batched(meshes, k=24, mode=0, profile="ref", iters=100, stream=None):
+def run_batched(meshes, k=24, mode=0, profile="ref", iters=100, stream=None, prm=None):
     """All meshes as segments of one engine; returns (seconds, engine, segs).
-    Mesh upload/preprocessing is outside the timed region."""
+    Mesh upload/preprocessing is outside the timed region.  prm (e.g. from
+    tune_for) replaces the default parameters."""
     import torch
     M = [E.Mesh(V, F) for _, V, F, _ in meshes]
     n_tot = sum(S.shape[0] for *_, S in meshes)
     cells = sum(E.grid_cells(m, S.shape[0], k) for m, (*_, S) in zip(M, meshes))
-    eng = E.Engine(E.params(k=k, mode=mode, profile=profile), len(meshes), n_tot, cells)
+    eng = E.Engine(prm if prm is not None else E.params(k=k, mode=mode, profile=profile), len(meshes), n_tot, cells)
     segs = [eng.add(m, S) for m, (*_, S) in zip(M, meshes)]
     eng.run(1, stream)          # graph capture + first iteration (untimed warm-up)
     _sync()
@@ -60,14 +61,14 @@ def run_batched(meshes, k=24, mode=0, profile="ref", iters=100, stream=None):
     return e0.elapsed_time(e1) / 1e3, eng, segs, M
 
 
-def run_plain_loop(meshes, k=24, mode=0, profile="ref", iters=100):
+def run_plain_loop(meshes, k=24, mode=0, profile="ref", iters=100, prm=None):
     """One mesh at a time through one engine sized for the largest; every
     mesh's 100 iterations replayed from the same CUDA graphs."""
     import torch
     M = [E.Mesh(V, F) for _, V, F, _ in meshes]
     nmax = max(S.shape[0] for *_, S in meshes)
     cells = max(E.grid_cells(m, S.shape[0], k) for m, (*_, S) in zip(M, meshes))
-    eng = E.Engine(E.params(k=k, mode=mode, profile=profile), 1, nmax, cells)
+    eng = E.Engine(prm if prm is not None else E.params(k=k, mode=mode, profile=profile), 1, nmax, cells)
     st = torch.cuda.current_stream()
     g = eng.add(M[0], meshes[0][3])
     eng.run(2, C_stream(st))    # graph capture (untimed)
@@ -96,24 +97,40 @@ def C_stream(st):
     return ctypes.c_void_p(st.cuda_stream)
 
 
+def tune_for(V, F, sites, k=24, mode=0, profile="ref", iters=4):
+    """Launch shapes from the autotuner (cvt_autotune) on one mesh and site
+    set: (tuned params, their per-iteration ms).  Results do not depend on
+    the shapes, only the time does."""
+    m = E.Mesh(V, F)
+    try:
+        return E.autotune(m, sites, E.params(k=k, mode=mode, profile=profile), iters=iters)
+    finally:
+        m.close()
+
+
 def batched_vs_plain(n_meshes=256, iters=100, k=24, mode=0, profile="ref", seed=3, check=True):
     t0 = time.perf_counter()
     meshes = batched_set(seed=seed, n_meshes=n_meshes)
     gen_s = time.perf_counter() - t0
     n_tot = sum(S.shape[0] for *_, S in meshes)
-    tb, eng, segs, M = run_batched(meshes, k=k, mode=mode, profile=profile, iters=iters)
+    # launch shapes tuned on the mesh with the most sites (untimed), used by
+    # both the batched engine and the plain loop
+    _, Vb, Fb, Sb = max(meshes, key=lambda x: x[3].shape[0])
+    prm, tune_ms = tune_for(Vb, Fb, Sb, k=k, mode=mode, profile=profile)
+    tb, eng, segs, M = run_batched(meshes, k=k, mode=mode, profile=profile, iters=iters, prm=prm)
     batched_sites = [eng.sites(s) for s in segs]
     eng.close()
     for m in M:
         m.close()
-    tp, finals = run_plain_loop(meshes, k=k, mode=mode, profile=profile, iters=iters)
+    tp, finals = run_plain_loop(meshes, k=k, mode=mode, profile=profile, iters=iters, prm=prm)
     same = all(np.array_equal(a, b) for a, b in zip(batched_sites, finals)) if check else None
     tris = [F.shape[0] for _, _, F, _ in meshes]
     return {"meshes": n_meshes, "sites_total": int(n_tot), "tris_min": int(min(tris)), "tris_max": int(max(tris)),
             "k": k, "mode": mode, "profile": profile, "iters": iters,
             "batched_s": tb, "plain_loop_s": tp,
             "batched_sites_iters_per_s": n_tot * iters / tb, "plain_sites_iters_per_s": n_tot * iters / tp,
-            "speedup": tp / tb, "identical_results": same, "mesh_generation_s": gen_s}
+            "speedup": tp / tb, "identical_results": same, "mesh_generation_s": gen_s,
+            "tiles": E.tiles(prm), "tune_ms_per_iter": tune_ms}
 
 
 def precision_study(iters=200, k=32, mode=1, n_sites=1_000_000, tris=2_000_000, seed=2):
