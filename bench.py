@@ -149,7 +149,7 @@ def traffic_from_profiles(kernel_key):
     return d.get(kernel_key)
 
 
-def issue_roofline(prof, iters, sm_mhz):
+def issue_roofline(prof, iters, sm_mhz, sms=None):
     """Warp-instruction issue rate of the site kernels against the B200's
     issue peak (SMs x 4 schedulers x SM clock), the bound these kernels meet
     long before HBM.  Warp instructions per remesh of this workload come from
@@ -161,8 +161,9 @@ def issue_roofline(prof, iters, sm_mhz):
         return None
     with open(path) as fh:
         counts = json.load(fh)["warp_instructions_per_remesh"]
-    import torch
-    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    if sms is None:
+        import torch
+        sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     peak = sms * 4 * sm_mhz * 1e6
     out = {"bound": "issue", "unit": "warp instructions/s", "peak": peak,
            "peak_from": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz (median SM clock of the timed region)",
@@ -204,7 +205,7 @@ def run_reference(args):
     t0 = time.perf_counter()
     O.lloyd_run(m.V, m.F, S, p["k"], p["mode"], 1, profile=O.P_MIXED)
     t1 = time.perf_counter() - t0
-    per_step_budget = 120.0 / max(args.steps + args.warmup, 1)
+    per_step_budget = args.ref_seconds / max(args.steps + args.warmup, 1)
     it = int(max(1, min(p["iters"], per_step_budget / max(t1, 1e-6))))
     for _ in range(args.warmup):
         O.lloyd_run(m.V, m.F, S, p["k"], p["mode"], 1, profile=O.P_MIXED)
@@ -474,6 +475,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-seconds", type=float, default=120.0,
+                    help="reference arm: seconds of CPU work to size the steps for")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--workload", choices=["torus_100k", "batched", "serve", "superellipsoid_1m"],

@@ -1,0 +1,43 @@
+"""bench.py's JSON contract where it runs without a GPU: the reference arm
+(the oracle port of the reference's CPU path, timed on the host cores) on a
+bounded sample, and the issue-roofline arithmetic."""
+import json
+import os
+import subprocess
+import sys
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def test_reference_arm_prints_contract_line():
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
+                        "--warmup", "0", "--ref-seconds", "1"],
+                       capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference"
+    assert line["metric"].startswith("sites")
+    assert line["unit"] == "sites*iters/s" and line["higher_is_better"] is True
+    assert line["value"] > 0 and line["steps"] == 1 and line["n_gpus"] == 1
+    assert line["config"]["workload"] == "torus_100k" and line["config"]["sites"] == 100_000
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    e2e = line["e2e"]
+    assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+
+
+def test_issue_roofline_arithmetic():
+    sys.path.insert(0, ROOT)
+    import bench
+    with open(os.path.join(ROOT, "profiles", "instructions.json")) as fh:
+        counts = json.load(fh)["warp_instructions_per_remesh"]
+    prof = {"grid": 0.03, "knn": 0.08, "clip": 0.06, "proj": 0.1}
+    out = bench.issue_roofline(prof, 100, 1965.0, sms=148)
+    assert out["bound"] == "issue" and out["peak"] == 148 * 4 * 1965e6
+    for kernel, group in (("k_site_knn", "knn"), ("k_site_clip", "clip"), ("k_site_proj", "proj")):
+        k = out["kernels"][kernel]
+        assert abs(k["achieved"] - counts[kernel] / (prof[group] * 1e-3 * 100)) < 1e-6 * k["achieved"]
+        assert abs(k["frac"] - k["achieved"] / out["peak"]) < 1e-12
+        assert 0.0 < k["frac"] < 1.0
+    assert bench.issue_roofline(prof, 100, None, sms=148) is None
