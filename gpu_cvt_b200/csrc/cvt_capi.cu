@@ -1365,7 +1365,7 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   // cell_start[max_cells] is the number of gridded sites (read on the device)
   a.total_cells = e->max_cells;
   // d_act_count is zero here: set at creation, reset by the bookkeeping
-  k_active_list<T><<<cdiv(ns, 256), 256, 0, st>>>(a);
+  k_active_list<T><<<cdiv(ns, kActiveListThreads), kActiveListThreads, 0, st>>>(a);
   L++;
   // the frame vertices are first read by the clip: search them on the side
   // stream while the site KNN runs

@@ -323,11 +323,17 @@ __device__ inline int tier_of(int mode, int i, int n, int K, const uint32_t* row
 
 // ---------------------------------------------------------------------------
 // k_active_list: sorted positions of the sites whose neighbour list is
-// recomputed this iteration (frozen sites keep theirs, main.cu:678); the
-// warp-aggregated append keeps runs of 32 spatially adjacent sites together
+// recomputed this iteration (frozen sites keep theirs, main.cu:678).  The
+// append is aggregated per block (one atomic per block, not per warp: the
+// per-warp atomics on one counter serialised the kernel), which keeps each
+// block's active sites together and in sorted order.
 // ---------------------------------------------------------------------------
+constexpr int kActiveListThreads = 256;
+
 template <class T>
-__global__ void k_active_list(EngineArgs<T> a) {
+__global__ void __launch_bounds__(kActiveListThreads) k_active_list(EngineArgs<T> a) {
+  __shared__ int warp_base[kActiveListThreads / 32];
+  __shared__ int block_base;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   bool act = false;
@@ -337,11 +343,20 @@ __global__ void k_active_list(EngineArgs<T> a) {
     act = !(sd.mode != 0 && a.frozen[g]);
   }
   const unsigned m = __ballot_sync(0xffffffffu, act);
-  const int lane = threadIdx.x & 31;
-  int base = 0;
-  if (lane == 0 && m) base = atomicAdd(a.act_count, __popc(m));
-  base = __shfl_sync(0xffffffffu, base, 0);
-  if (act) a.act[base + __popc(m & ((1u << lane) - 1u))] = t;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) warp_base[wid] = __popc(m);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int sum = 0;
+    for (int w = 0; w < kActiveListThreads / 32; ++w) {
+      const int c = warp_base[w];
+      warp_base[w] = sum;
+      sum += c;
+    }
+    block_base = sum ? atomicAdd(a.act_count, sum) : 0;
+  }
+  __syncthreads();
+  if (act) a.act[block_base + warp_base[wid] + __popc(m & ((1u << lane) - 1u))] = t;
 }
 
 // ---------------------------------------------------------------------------
@@ -595,7 +610,22 @@ __device__ __forceinline__ void stats_atomic(int* stats, const SegDev* segs, con
   atomicMax(reinterpret_cast<unsigned*>(sl + 4), __float_as_uint(o.disp2));
 }
 
-__device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, const SiteOut& o) {
+// Per-block staging of the per-segment counters: the first segment a warp
+// of the block reports claims the slot; counts of other segments go to
+// global memory directly.  (One set of global atomics per block instead of
+// per warp: thousands of warps adding to the same few words serialised in
+// L2.)  Sums and a max of float bits, so the totals do not depend on order.
+struct StatsStage {
+  int seg;
+  unsigned v[5];  // same, low, both, newly, max squared displacement (float bits)
+};
+
+__device__ __forceinline__ void stats_stage_init(StatsStage& s) {
+  if (threadIdx.x < 5) s.v[threadIdx.x] = 0u;
+  if (threadIdx.x == 0) s.seg = -1;
+}
+
+__device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, const SiteOut& o, StatsStage& stage) {
   // warp-aggregated per-segment counters; every lane of the warp takes part
   const unsigned full = 0xffffffffu;
   const int key = o.seg;
@@ -608,22 +638,45 @@ __device__ __forceinline__ void stats_flush(int* stats, const SegDev* segs, cons
   const int newly = __popc(__ballot_sync(full, o.newly) & peers);
   const unsigned dbits = __reduce_max_sync(peers, __float_as_uint(o.seg >= 0 ? o.disp2 : 0.f));
   if (lane == leader && key >= 0) {
-    int* sl = stats + ((size_t)key * kStatsRing + (segs[key].iter % kStatsRing)) * kStatsWords;
-    if (same) atomicAdd(sl + 0, same);
-    if (low) atomicAdd(sl + 1, low);
-    if (both) atomicAdd(sl + 2, both);
-    if (newly) atomicAdd(sl + 3, newly);
-    atomicMax(reinterpret_cast<unsigned*>(sl + 4), dbits);
+    const int owner = atomicCAS(&stage.seg, -1, key);
+    if (owner == -1 || owner == key) {
+      if (same) atomicAdd(&stage.v[0], (unsigned)same);
+      if (low) atomicAdd(&stage.v[1], (unsigned)low);
+      if (both) atomicAdd(&stage.v[2], (unsigned)both);
+      if (newly) atomicAdd(&stage.v[3], (unsigned)newly);
+      atomicMax(&stage.v[4], dbits);
+    } else {
+      int* sl = stats + ((size_t)key * kStatsRing + (segs[key].iter % kStatsRing)) * kStatsWords;
+      if (same) atomicAdd(sl + 0, same);
+      if (low) atomicAdd(sl + 1, low);
+      if (both) atomicAdd(sl + 2, both);
+      if (newly) atomicAdd(sl + 3, newly);
+      atomicMax(reinterpret_cast<unsigned*>(sl + 4), dbits);
+    }
   }
+}
+
+// after a __syncthreads that follows every warp's stats_flush
+__device__ __forceinline__ void stats_stage_flush(int* stats, const SegDev* segs, const StatsStage& stage) {
+  if (threadIdx.x != 0 || stage.seg < 0) return;
+  int* sl = stats + ((size_t)stage.seg * kStatsRing + (segs[stage.seg].iter % kStatsRing)) * kStatsWords;
+  for (int w = 0; w < 4; ++w)
+    if (stage.v[w]) atomicAdd(sl + w, (int)stage.v[w]);
+  atomicMax(reinterpret_cast<unsigned*>(sl + 4), stage.v[4]);
 }
 
 template <int PROF, int BS>
 __global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  __shared__ StatsStage stage;
+  stats_stage_init(stage);
+  __syncthreads();
   const int t = blockIdx.x * BS + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   SiteOut o{-1, 0, 0, 0, 0, 0.f};
   if (t < n_grid) site_proj<PROF>(a, parity, (int)a.sorted[t].id, o);
-  stats_flush(a.stats, a.segs, o);
+  stats_flush(a.stats, a.segs, o, stage);
+  __syncthreads();
+  stats_stage_flush(a.stats, a.segs, stage);
 }
 
 // Iteration bookkeeping, run by one block: advance active segments, clear
