@@ -124,8 +124,9 @@ def measured_peaks():
 # mesh arrays are gathered from L2 and not counted, like the neighbours'
 # positions, which are the sites' own positions read again)
 def knn_bytes_per_site(K):
-    # own position 12 + neighbour ids written 4K + frame vertex id 4
-    return 12 + 4 * K + 4
+    # own position 12 + neighbour ids written 4K (the frame vertex is
+    # written by the separate frame-vertex kernel)
+    return 12 + 4 * K
 
 
 def clip_bytes_per_site(K):
