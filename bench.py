@@ -1,20 +1,31 @@
 #!/usr/bin/env python
 """Benchmark: restricted-Voronoi CVT remeshing throughput on B200.
 
-One *step* = one complete remesh of the workload: 100 Lloyd iterations of
-100,000 area-uniform sites on the noisy (R=1, r=0.3, 200x100) torus, K=24,
-freezing on (mode 1), mixed FP32/FP64 profile.  ``value`` is sites x
-Lloyd-iterations per second over the whole job with the mesh and initial
-sites resident in HBM; ``e2e`` is the same metric through the one-call C ABI
-(``cvt_remesh``: host arrays in, upload + iterate + download).
+Default workload (``--workload batched``): 256 seeded procedural meshes
+(spheres, tori, superquadrics; 5k-200k triangles each) with log-uniform site
+counts in [1k, 50k] (about 3.1M sites in total), K=24, 100 Lloyd iterations,
+freezing off (every site is recomputed in every iteration), mixed FP32/FP64
+profile.  One *step* = one complete remesh of all 256 meshes as segments of
+one engine.  ``value`` is sites x Lloyd-iterations per second over the timed
+steps with the meshes and initial sites resident in HBM; beside it the line
+carries the plain per-mesh loop (the same meshes one after another, as the
+reference's driver runs them) with the batched/plain ratio, p50/p99 per-mesh
+latency of both, per-mesh Hausdorff / bbox diagonal, the 1M-site rounded-box
+figures (KNN + clip time per iteration and HBM fraction), and ``e2e``: the
+same remesh through the one-call C ABI ``cvt_remesh_batch`` with pinned host
+buffers (upload + iterate + download inside the timed region).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload batched|torus_100k|superellipsoid_1m|serve]
 
-N > 1 (launched by torch.distributed.run) runs independent replicas, one per
-GPU (the path shards at mesh granularity; there is no exchange step), and
-reports the aggregate over ranks with the max-over-ranks device time.
-``--impl reference`` times the CPU implementation of the same path (the
-oracle port of the reference's algorithm) on the host cores.
+N > 1 (launched by torch.distributed.run): the meshes are partitioned over
+the ranks by site count (the path shards at mesh granularity, with no
+exchange step); value = all ranks' sites x iterations / the max-over-ranks
+device time.  ``--impl reference`` times the CPU implementation of the same
+path (the oracle port of the reference's algorithm, all host threads) on the
+same configuration: every step runs whole remeshes (all 100 iterations) of
+meshes drawn from a seeded permutation of the 256, and the rate of that
+sample stands for the whole job.
 """
 from __future__ import annotations
 
@@ -35,16 +46,7 @@ sys.path.insert(0, ROOT)
 METRIC = "sites·Lloyd-iters/s and p50/p99 remesh latency, batched/served vs plain, equal Hausdorff"
 UNIT = "sites*iters/s"
 PROFILE = "mixed"
-
-
-def workload():
-    from gpu_cvt_b200 import meshgen as mg
-    m, S, p = mg.workload_mesh("torus_100k")
-    cfg = {"workload": "torus_100k",
-           "mesh": "torus R=1 r=0.3, 200x100 grid (20,000 V / 40,000 F), N(0,0.002) normal noise, seed 1",
-           "sites": int(S.shape[0]), "site_seed": 1, "k": p["k"], "iters": p["iters"], "mode": p["mode"],
-           "profile": PROFILE, "kproj": 5, "l2": "flushed (256 MiB write) before every timed step"}
-    return m, S, p, cfg
+L2_NOTE = "flushed (256 MiB write) before every timed step"
 
 
 # ---------------------------------------------------------------------------
@@ -55,8 +57,38 @@ def dist_setup():
     return ws, rank, local
 
 
+def _smi_once(gpu: int):
+    """One read-only nvidia-smi query: (sm MHz, max sm MHz) or None."""
+    try:
+        out = subprocess.run(["nvidia-smi", "--query-gpu=clocks.sm,clocks.max.sm", "--format=csv,noheader,nounits",
+                              "-i", str(gpu)], capture_output=True, text=True, timeout=20).stdout
+        a, b = [float(x) for x in out.strip().splitlines()[0].split(",")[:2]]
+        return a, b
+    except Exception:
+        return None
+
+
+def _nvml_max_clock(gpu: int):
+    """The device's maximum SM clock from NVML (read-only), or None."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByIndex(gpu)
+            return float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        finally:
+            pynvml.nvmlShutdown()
+    except Exception:
+        return None
+
+
 class Clocks:
-    """nvidia-smi clock / throttle sampling during the timed region."""
+    """nvidia-smi clock / throttle sampling during the timed region.
+
+    A timed region shorter than the 200 ms sampling period can end before
+    the first sample; the clock then comes from one-shot queries taken just
+    before and just after the region, or, failing those, from the device's
+    maximum SM clock (NVML).  ``source`` says which."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -67,8 +99,10 @@ class Clocks:
         self.proc = None
         self.lines = []
         self.thread = None
+        self.before = None
 
     def start(self):
+        self.before = _smi_once(self.gpu)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-lms", "200", "-i", str(self.gpu)], stdout=subprocess.PIPE,
@@ -84,15 +118,14 @@ class Clocks:
             self.lines.append(line.strip())
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        if self.thread:
-            self.thread.join(timeout=2)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in self.lines:
@@ -107,8 +140,18 @@ class Clocks:
             for nm, v in zip(names, f[5:9]):
                 if v.lower() == "active":
                     reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        if sm:
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "samples": len(sm),
+                    "reasons": sorted(reasons), "source": "nvidia-smi -lms 200 during the timed region"}
+        once = [x for x in (self.before, _smi_once(self.gpu)) if x]
+        if once:
+            return {"sm_mhz": statistics.median([a for a, _ in once]), "sm_max_mhz": max(b for _, b in once),
+                    "samples": 0, "reasons": [],
+                    "source": "no sample inside the timed region (shorter than the sampling period): "
+                              "one-shot nvidia-smi queries just before and after it"}
+        mx = _nvml_max_clock(self.gpu)
+        return {"sm_mhz": None, "sm_max_mhz": mx, "samples": 0, "reasons": [],
+                "source": "nvidia-smi unavailable; sm_max_mhz from NVML" if mx else "no clock source available"}
 
 
 def measured_peaks():
@@ -116,8 +159,8 @@ def measured_peaks():
     if os.path.exists(p):
         with open(p) as fh:
             d = json.load(fh)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s, earlier measurement on this pool)"
 
 
 # algorithmic bytes per site and launch (fp32 positions, uint32 ids; the
@@ -141,87 +184,143 @@ def proj_bytes_per_site(K):
     return 12 + 12 + 20 + 12 + 4 + 2
 
 
-def traffic_from_profiles(kernel_key):
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+def _recorded(name):
+    p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     with open(p) as fh:
-        d = json.load(fh)
-    return d.get(kernel_key)
+        return json.load(fh)
 
 
-def issue_roofline(prof, iters, sm_mhz, sms=None):
+def traffic_recorded(workload, kernel_key, sites_in_launch):
+    """DRAM read + write bytes per launch of a kernel from a recorded ncu
+    capture (profiles/traffic.json), scaled from the captured launch's sites
+    to this launch's sites when the capture was a smaller case."""
+    d = _recorded("traffic.json")
+    w = (d or {}).get("workloads", {}).get(workload)
+    if not w or kernel_key not in w.get("bytes_per_launch", {}):
+        return None, None
+    b = float(w["bytes_per_launch"][kernel_key])
+    sites = float(w.get("sites_per_launch", {}).get(kernel_key, sites_in_launch) or sites_in_launch)
+    return b * sites_in_launch / sites, f"recorded ncu capture: {w['command']} (scaled by sites per launch)"
+
+
+def issue_roofline(workload, prof, iters, sm_mhz, sms=None, sites_scale=1.0):
     """Warp-instruction issue rate of the site kernels against the B200's
     issue peak (SMs x 4 schedulers x SM clock), the bound these kernels meet
-    long before HBM.  Warp instructions per remesh of this workload come from
-    profiles/instructions.json (ncu smsp__inst_executed.sum over the launches
-    of one remesh), the kernel times from this run's CUDA events (the
-    projection group includes the deferred-site kernel and the bookkeeping)."""
-    path = os.path.join(ROOT, "profiles", "instructions.json")
-    if not os.path.exists(path) or not sm_mhz:
+    long before HBM.  Warp instructions per remesh come from a recorded ncu
+    capture (profiles/instructions.json: smsp__inst_executed.sum summed over
+    the launches of one remesh of the named workload, scaled by sites when
+    the capture was a smaller case); the kernel times come from this run's
+    CUDA events.  None when no count is recorded for the workload or no
+    clock is known."""
+    d = _recorded("instructions.json")
+    w = (d or {}).get("workloads", {}).get(workload)
+    if not w or not sm_mhz:
         return None
-    with open(path) as fh:
-        counts = json.load(fh)["warp_instructions_per_remesh"]
+    counts = w["warp_instructions_per_remesh"]
     if sms is None:
         import torch
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     peak = sms * 4 * sm_mhz * 1e6
     out = {"bound": "issue", "unit": "warp instructions/s", "peak": peak,
-           "peak_from": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz (median SM clock of the timed region)",
-           "counts": "profiles/instructions.json", "kernels": {}}
+           "peak_from": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz",
+           "counts": f"recorded ncu capture: {w['command']}, not this run", "kernels": {}}
     for kernel, group in (("k_site_knn", "knn"), ("k_site_clip", "clip"), ("k_site_proj", "proj")):
         if kernel in counts and prof.get(group, 0) > 0:
-            achieved = counts[kernel] / (prof[group] * 1e-3 * iters)
+            achieved = counts[kernel] * sites_scale / (prof[group] * 1e-3 * iters)
             out["kernels"][kernel] = {"achieved": achieved, "frac": achieved / peak}
     return out
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(m, S, p, budget_s=15.0):
-    """The oracle port of the reference's algorithm on the host cores."""
+# workloads and their configuration (identical in both arms)
+# ---------------------------------------------------------------------------
+def parallelism(ws):
+    return "single GPU" if ws == 1 else f"{ws} GPUs, meshes partitioned over ranks by site count (no exchange)"
+
+
+def batched_workload(n_meshes, ws):
+    from gpu_cvt_b200 import workloads
+    t0 = time.perf_counter()
+    meshes = workloads.batched_set(seed=3, n_meshes=n_meshes)
+    gen_s = time.perf_counter() - t0
+    sizes = [int(S.shape[0]) for *_, S in meshes]
+    tris = [int(F.shape[0]) for _, _, F, _ in meshes]
+    cfg = {"workload": f"batched_{n_meshes}_meshes",
+           "meshes": n_meshes, "seed": 3, "families": "spheres, tori, superquadrics (random parameters)",
+           "tris_per_mesh": [min(tris), max(tris)], "sites_per_mesh": "log-uniform in [1000, 50000]",
+           "sites_total": int(sum(sizes)), "k": 24, "iters": 100, "mode": 0, "freezing": "off",
+           "profile": PROFILE, "kproj": 5, "l2": L2_NOTE, "parallelism": parallelism(ws)}
+    return meshes, cfg, gen_s
+
+
+def torus_workload(ws):
+    from gpu_cvt_b200 import meshgen as mg
+    m, S, p = mg.workload_mesh("torus_100k")
+    cfg = {"workload": "torus_100k",
+           "mesh": "torus R=1 r=0.3, 200x100 grid (20,000 V / 40,000 F), N(0,0.002) normal noise, seed 1",
+           "sites": int(S.shape[0]), "site_seed": 1, "k": p["k"], "iters": p["iters"], "mode": p["mode"],
+           "freezing": "on", "profile": PROFILE, "kproj": 5, "l2": L2_NOTE, "parallelism": parallelism(ws)}
+    return m, S, p, cfg
+
+
+def cpu_sample(meshes, k, mode, iters, budget_s, seed=11, start=0, min_meshes=1):
+    """The oracle port (all host threads) on whole remeshes of meshes drawn
+    in a seeded order, until budget_s of CPU time is spent.  Returns
+    (site-iterations, seconds, meshes used, next start)."""
     from oracle import oracle as O
-    threads = O.max_threads()
-    n = S.shape[0]
-    t0 = time.perf_counter()
-    O.lloyd_run(m.V, m.F, S, p["k"], p["mode"], 2, profile=O.P_MIXED)
-    t2 = time.perf_counter() - t0
-    it = int(max(2, min(p["iters"], budget_s / max(t2 / 2, 1e-6))))
-    t0 = time.perf_counter()
-    O.lloyd_run(m.V, m.F, S, p["k"], p["mode"], it, profile=O.P_MIXED)
-    dt = time.perf_counter() - t0
-    return {"value": n * it / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{n} sites x the first {it} of {p['iters']} Lloyd iterations (mode {p['mode']}, "
-                      f"mixed profile), {dt:.1f} s"}
+    order = np.random.default_rng(seed).permutation(len(meshes))
+    done, secs, used, i = 0, 0.0, 0, start
+    while (secs < budget_s or used < min_meshes) and used < len(meshes):
+        _, V, F, S = meshes[int(order[i % len(meshes)])]
+        t0 = time.perf_counter()
+        O.lloyd_run(V, F, S, k, mode, iters, profile=O.P_MIXED)
+        secs += time.perf_counter() - t0
+        done += int(S.shape[0]) * iters
+        used += 1
+        i += 1
+    return done, secs, used, i
 
 
+# ---------------------------------------------------------------------------
 def run_reference(args):
     ws, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    m, S, p, cfg = workload()
     from oracle import oracle as O
     threads = O.max_threads()
-    n = S.shape[0]
-    # size each step so that warmup + steps end within a few minutes
-    t0 = time.perf_counter()
-    O.lloyd_run(m.V, m.F, S, p["k"], p["mode"], 1, profile=O.P_MIXED)
-    t1 = time.perf_counter() - t0
-    per_step_budget = args.ref_seconds / max(args.steps + args.warmup, 1)
-    it = int(max(1, min(p["iters"], per_step_budget / max(t1, 1e-6))))
+    if args.workload == "batched":
+        meshes, cfg, _ = batched_workload(args.meshes, ws)
+        k, mode, iters = cfg["k"], cfg["mode"], cfg["iters"]
+    elif args.workload == "torus_100k":
+        m, S, p, cfg = torus_workload(ws)
+        meshes = [("torus", m.V, m.F, S)]
+        k, mode, iters = p["k"], p["mode"], p["iters"]
+    else:
+        print(json.dumps({"impl": "reference", "unavailable": f"no CPU arm for --workload {args.workload}"}))
+        return 0
+    per_step = args.ref_seconds / max(args.steps + args.warmup, 1)
+    # warm-up steps: the smallest mesh, two iterations each (page-in, thread start-up)
+    small = min(meshes, key=lambda x: x[3].shape[0])
     for _ in range(args.warmup):
-        O.lloyd_run(m.V, m.F, S, p["k"], p["mode"], 1, profile=O.P_MIXED)
+        O.lloyd_run(small[1], small[2], small[3], k, mode, 2, profile=O.P_MIXED)
+    tot_si, tot_s, used, nxt = 0, 0.0, 0, 0
     times = []
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        O.lloyd_run(m.V, m.F, S, p["k"], p["mode"], it, profile=O.P_MIXED)
-        times.append(time.perf_counter() - t0)
-    tot = sum(times)
-    value = n * it * args.steps / tot
-    sample = f"{n} sites x the first {it} of {p['iters']} Lloyd iterations per step, mixed profile"
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": cfg,
+        si, secs, u, nxt = cpu_sample(meshes, k, mode, iters, per_step, start=nxt)
+        tot_si += si
+        tot_s += secs
+        used += u
+        times.append(secs)
+    value = tot_si / tot_s
+    sample = (f"{used} whole remeshes ({iters} iterations each, {tot_si / iters:.0f} sites) of meshes drawn in a "
+              f"seeded order from the {len(meshes)} of the workload, {tot_s:.1f} s; the sample's rate stands for "
+              f"the whole job (extrapolated)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot_s / args.steps,
+            "higher_is_better": True, "scaling": "strong" if args.workload == "batched" else "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -229,31 +328,290 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
-def run_ours(args):
+def _init_dist(ws, local):
     import torch
     import torch.distributed as dist
-    from gpu_cvt_b200 import engine as E
-    from gpu_cvt_b200 import _lib
-
-    ws, rank, local = dist_setup()
     torch.cuda.set_device(local)
     if ws > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    m, S, p, cfg = workload()
+
+
+def _max_over_ranks(x, ws):
+    if ws == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(ws):
+    import torch
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_ours_batched(args):
+    import torch
+    from gpu_cvt_b200 import _lib, replicas, workloads
+    from gpu_cvt_b200 import engine as E
+
+    ws, rank, local = dist_setup()
+    _init_dist(ws, local)
+    meshes_all, cfg, gen_s = batched_workload(args.meshes, ws)
+    sizes = [int(S.shape[0]) for *_, S in meshes_all]
+    mine = replicas.partition(sizes, ws, rank) if ws > 1 else list(range(len(meshes_all)))
+    meshes = [meshes_all[i] for i in mine]
+    K, mode, iters = cfg["k"], cfg["mode"], cfg["iters"]
+    n_mine = sum(int(S.shape[0]) for *_, S in meshes)
+    n_all = int(sum(sizes))
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    # launch shapes from the autotuner on this rank's largest mesh (untimed;
+    # results never depend on them)
+    _, Vb, Fb, Sb = max(meshes, key=lambda x: x[3].shape[0])
+    prm, tune_ms = workloads.tune_for(Vb, Fb, Sb, k=K, mode=mode, profile=PROFILE)
+    M = [E.Mesh(V, F) for _, V, F, _ in meshes]
+    cells = sum(E.grid_cells(m, S.shape[0], K) for m, (*_, S) in zip(M, meshes))
+    eng = E.Engine(prm, len(M), n_mine, cells)
+    S_dev = [torch.from_numpy(S).cuda() for *_, S in meshes]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    segs = []
+
+    def reset():
+        for g in segs:
+            eng.remove(g)
+        segs.clear()
+        segs.extend(eng.add(m, s, sp) for m, s in zip(M, S_dev))
+
+    def step(timed_list, launches):
+        reset()
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        eng.run(iters, sp)
+        e1.record(stream)
+        e1.synchronize()
+        timed_list.append(e0.elapsed_time(e1))
+        launches.append(eng.last_launches())
+
+    warm, wl = [], []
+    for _ in range(max(args.warmup, 3)):
+        step(warm, wl)
+    _barrier(ws)
+    clocks = Clocks(local)
+    clocks.start()
+    times, launches = [], []
+    for _ in range(args.steps):
+        step(times, launches)
+    _barrier(ws)
+    clk = clocks.stop()
+    tot = _max_over_ranks(float(sum(times)), ws)
+    value = n_all * iters * args.steps / (tot / 1e3)
+    finals = [eng.sites(g) for g in segs]
+    evals = [eng.evaluate(g) for g in segs]
+    dH_rel = np.array([ev["dH_rel"] for ev in evals], np.float64)
+
+    # ---- the plain per-mesh loop: same meshes, same kernels, one at a time --
+    plain = None
+    if not args.no_plain:
+        tp, pfinals, each = workloads.run_plain_loop(meshes, k=K, mode=mode, profile=PROFILE, iters=iters,
+                                                     prm=prm, per_mesh=True)
+        tp = _max_over_ranks(tp, ws)
+        each_ms = np.array(each) * 1e3
+        done_ms = np.cumsum(each_ms)
+        plain = {"value": n_all * iters / tp, "unit": UNIT, "ms": tp * 1e3,
+                 "latency_ms": {"p50": float(np.percentile(each_ms, 50)), "p99": float(np.percentile(each_ms, 99)),
+                                "what": "device time of one mesh's remesh, meshes run one after another"},
+                 "completion_ms": {"p50": float(np.percentile(done_ms, 50)),
+                                   "p99": float(np.percentile(done_ms, 99)),
+                                   "what": "time from the job's start until the mesh's result is ready"},
+                 "identical_results": bool(all(np.array_equal(a, b) for a, b in zip(finals, pfinals)))}
+
+    # ---- e2e through the one-call batched C ABI with pinned host buffers ----
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    Vh = [pin(V) for _, V, _, _ in meshes]
+    Fh = [pin(F) for _, _, F, _ in meshes]
+    Sh = [pin(S) for *_, S in meshes]
+    Oh = [torch.empty((int(S.shape[0]), 3), dtype=torch.float32).pin_memory() for *_, S in meshes]
+    e2e_t, e2e_wall = [], []
+    for r in range(3):
+        ds = torch.cuda.default_stream()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        w0 = time.perf_counter()
+        e0.record(ds)
+        E.remesh_batch(Vh, Fh, Sh, prm, iters, outs=Oh)
+        e1.record(ds)
+        e1.synchronize()
+        if r > 0:   # the first call is the warm-up
+            e2e_t.append(e0.elapsed_time(e1))
+            e2e_wall.append((time.perf_counter() - w0) * 1e3)
+    e2e_ms = _max_over_ranks(float(np.mean(e2e_t)), ws)
+    same_as_engine = bool(all(np.array_equal(o.numpy(), f) for o, f in zip(Oh, finals)))
+    h2d = int(sum(v.numel() * 4 + f.numel() * 4 + s.numel() * 4 for v, f, s in zip(Vh, Fh, Sh)))
+    d2h = int(sum(o.numel() * 4 for o in Oh))
+
+    # ---- per-kernel timing over one whole batched remesh ----------------
+    reset()
+    prof = eng.profile(iters, sp)
+    groups = {"k_site_knn": (prof["knn"], n_mine * knn_bytes_per_site(K)),
+              "k_site_clip": (prof["clip"], n_mine * clip_bytes_per_site(K)),
+              "k_site_proj": (prof["proj"], n_mine * proj_bytes_per_site(K))}
+    dom = max(groups, key=lambda g: groups[g][0])
+    ms, alg_bytes = groups[dom]
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms * 1e-3) / 1e9
+    tr, tr_src = traffic_recorded(cfg["workload"], dom, n_mine)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": tr, "traffic_source": tr_src, "kernel": dom,
+                "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": ms, "peak_source": peak_kind,
+                "stage_ms_per_iter": {k: round(v, 5) for k, v in prof.items()},
+                "knn_clip": {"ms_per_iter": prof["knn"] + prof["clip"],
+                             "achieved_gbs": n_mine * (knn_bytes_per_site(K) + clip_bytes_per_site(K))
+                             / ((prof["knn"] + prof["clip"]) * 1e-3) / 1e9}}
+    roofline["knn_clip"]["frac"] = roofline["knn_clip"]["achieved_gbs"] / peak
+    sm_clock = clk.get("sm_mhz") or clk.get("sm_max_mhz")
+    ir = issue_roofline(cfg["workload"], prof, iters, sm_clock)
+
+    # ---- accuracy: the same remesh with FP64 state and arithmetic ---------
+    acc = None
+    if not args.no_accuracy:
+        e64 = E.Engine(E.params(k=K, mode=mode, profile="fp64"), len(M), n_mine, cells)
+        g64 = [e64.add(m, s, sp) for m, s in zip(M, S_dev)]
+        e64.run(iters, sp)
+        drift = []
+        ddH = []
+        for j, g in enumerate(g64):
+            S64 = e64.sites_f64(g)
+            drift.append(np.linalg.norm(finals[j].astype(np.float64) - S64, axis=1) / M[j].diag)
+            ddH.append(abs(evals[j]["dH"] - e64.evaluate(g)["dH"]) / M[j].diag)
+        e64.close()
+        d = np.concatenate(drift)
+        acc = {"site_drift_vs_fp64": {"max": float(d.max()), "p99": float(np.percentile(d, 99)),
+                                      "mean": float(d.mean())},
+               "hausdorff_minus_fp64_max": float(max(ddH)),
+               "unit": "fraction of each mesh's bbox diagonal",
+               "fp64": "same engine, FP64 state and arithmetic (bit-identical to the FP64 oracle)"}
+
+    # ---- 1M sites on the jittered rounded box (rank 0) ---------------------
+    c3 = None
+    if rank == 0 and not args.no_c3:
+        c3 = c3_figures(peak, peak_kind)
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        si, secs, used, _ = cpu_sample(meshes_all, K, mode, iters, args.cpu_seconds)
+        from oracle import oracle as O
+        cpu = {"value": si / secs, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+               "sample": f"{used} whole remeshes ({iters} iterations each, {si / iters:.0f} sites) of meshes drawn "
+                         f"in a seeded order, mixed profile, {secs:.1f} s"}
+
+    eng.close()
+    for m in M:
+        m.close()
+    if rank == 0:
+        batched_lat = float(np.percentile(times, 50)), float(np.percentile(times, 99))
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+                "warmup": max(args.warmup, 3), "ms_per_step": tot / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+                "latency_ms": {"p50": batched_lat[0], "p99": batched_lat[1],
+                               "what": "batched: every mesh's result is ready when the step ends, so a mesh's "
+                                       "latency is the step's device time (p50/p99 over the timed steps)"},
+                "plain_loop": plain,
+                "batched_over_plain": (value / plain["value"]) if plain else None,
+                "hausdorff_rel": {"p50": float(np.median(dH_rel)), "max": float(dH_rel.max()),
+                                  "what": "per mesh, one-sided (dual mesh -> input), / bbox diagonal"},
+                "e2e": {"value": n_all * iters / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                        "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "wall_ms_per_step": float(np.mean(e2e_wall)),
+                        "api": "cvt_remesh_batch (pinned host buffers; mesh ingest, upload, iterations, download)",
+                        "same_sites_as_engine": same_as_engine},
+                "gpu_launches": int(sum(launches)),
+                "roofline": roofline, "issue_roofline": ir, "superellipsoid_1m": c3,
+                "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
+                "tiles": E.tiles(prm), "tune_ms_per_iter": tune_ms, "mesh_generation_s": gen_s,
+                "libgpucvt_launches_total": _lib.launch_count()}
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def c3_figures(peak, peak_kind, iters=200, k=32):
+    """1M area-uniform sites on the rounded box |x|^8+|y|^8+|z|^8=1 (~2M
+    triangles, 1% jittered by 1e-3), K=32, 200 iterations, freezing on,
+    mixed profile: remesh time, KNN + clip time per iteration and its HBM
+    fraction (while every site is active, and averaged over the run)."""
+    import torch
+    from gpu_cvt_b200 import engine as E, meshgen as mg
+    m = mg.superellipsoid(8.0, 2_000_000, 0.01, 1e-3, seed=2)
+    S0 = mg.sample_sites(m.V, m.F, 1_000_000, seed=2)
+    n = S0.shape[0]
+    M = E.Mesh(m.V, m.F)
+    cells = E.grid_cells(M, n, k)
+    eng = E.Engine(E.params(k=k, mode=1, profile=PROFILE), 1, n, cells)
+    st = torch.cuda.current_stream()
+    sp = st.cuda_stream
+    g = eng.add(M, S0, sp)
+    eng.run(2, sp)                     # graph capture (untimed)
+    torch.cuda.synchronize()
+    eng.remove(g)
+    g = eng.add(M, S0, sp)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    eng.run(iters, sp)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ev = eng.evaluate(g)
+    eng.remove(g)
+    g = eng.add(M, S0, sp)
+    first = eng.profile(3, sp)          # iterations 0-2: every site active
+    eng.remove(g)
+    g = eng.add(M, S0, sp)
+    whole = eng.profile(iters, sp)
+    eng.close()
+    M.close()
+    b = n * (knn_bytes_per_site(k) + clip_bytes_per_site(k))
+    kc_first = first["knn"] + first["clip"]
+    kc_avg = whole["knn"] + whole["clip"]
+    return {"mesh": f"superellipsoid p=8, {m.nF} triangles, 1% jittered by 1e-3 (seed 2)", "sites": n, "k": k,
+            "iters": iters, "mode": 1, "profile": PROFILE, "ms_per_remesh": ms,
+            "sites_iters_per_s": n * iters / (ms / 1e3), "dH_rel": ev["dH_rel"],
+            "knn_clip_ms_per_iter": {"all_sites_active": kc_first, "run_average": kc_avg},
+            "knn_clip_hbm_frac_all_active": b / (kc_first * 1e-3) / 1e9 / peak,
+            "knn_clip_bytes_per_site": knn_bytes_per_site(k) + clip_bytes_per_site(k),
+            "peak_gbs": peak, "peak_source": peak_kind,
+            "stage_ms_per_iter_all_active": {k_: round(v, 5) for k_, v in first.items()}}
+
+
+def run_ours_torus(args):
+    import torch
+    from gpu_cvt_b200 import engine as E
+    from gpu_cvt_b200 import _lib
+
+    ws, rank, local = dist_setup()
+    _init_dist(ws, local)
+    m, S, p, cfg = torus_workload(ws)
     n, iters = S.shape[0], p["iters"]
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
 
     mesh = E.Mesh(m.V, m.F)
     cells = E.grid_cells(mesh, n, p["k"])
-    # launch shapes from the autotuner (untimed; results do not depend on them)
     prm, tune_ms = E.autotune(mesh, S, E.params(k=p["k"], mode=p["mode"], profile=PROFILE), iters=4)
-    cfg = dict(cfg, tiles=E.tiles(prm))
     eng = E.Engine(prm, 1, n, cells)
     S_dev = torch.from_numpy(S).cuda()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
     state = {"seg": None}
 
     def reset():
@@ -273,40 +631,26 @@ def run_ours(args):
         timed_list.append(e0.elapsed_time(e1))
         launches.append(eng.last_launches())
 
-    def barrier():
-        torch.cuda.synchronize()
-        if ws > 1:
-            dist.barrier()
-
     warm, wl = [], []
     for _ in range(max(args.warmup, 3)):
         step(warm, wl)
-    barrier()
+    _barrier(ws)
     clocks = Clocks(local)
     clocks.start()
     times, launches = [], []
     for _ in range(args.steps):
         step(times, launches)
-    barrier()
+    _barrier(ws)
     clk = clocks.stop()
-    tot = float(sum(times))
-    if ws > 1:
-        t = torch.tensor([tot], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        tot = float(t.item())
+    tot = _max_over_ranks(float(sum(times)), ws)
     value = ws * n * iters * args.steps / (tot / 1e3)
-    lat = sorted(times)
-    p50 = float(np.percentile(lat, 50))
-    p99 = float(np.percentile(lat, 99))
     seg = state["seg"]
     final = eng.sites(seg)
     frozen = int(eng.state(seg)["frozen"].sum())
 
-    # ---- e2e through the one-call C ABI with host buffers ----------------
     V, F = m.V, m.F
     e2e_t = []
-    for k in range(3):
-        out = np.empty_like(S)
+    for r in range(3):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -314,24 +658,16 @@ def run_ours(args):
         out, _ = E.remesh(V, F, S, iters=iters, with_counts=True, prm=prm)
         e1.record(torch.cuda.default_stream())
         e1.synchronize()
-        if k > 0:
+        if r > 0:
             e2e_t.append(e0.elapsed_time(e1))
-    e2e_ms = float(np.mean(e2e_t))
-    if ws > 1:
-        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = _max_over_ranks(float(np.mean(e2e_t)), ws)
     same_as_engine = bool(np.array_equal(out, final))
     h2d = int(V.nbytes + F.nbytes + S.nbytes)
     d2h = int(S.nbytes + 16 * iters)
 
-    # ---- per-kernel timing (CUDA events on the launching stream) over one
-    # whole remesh: average per launch of each kernel group --------------
     reset()
     prof = eng.profile(iters, sp)
     K = p["k"]
-    # the KNN kernel runs for the sites not yet frozen at the start of each
-    # iteration (frozen counts from the engine's per-iteration statistics)
     newly = np.array([eng.stats(state["seg"], i)["newly_frozen"] for i in range(iters)], np.float64)
     active_mean = float(np.mean(n - np.concatenate([[0.0], np.cumsum(newly)[:-1]])))
     groups = {"k_site_knn": (prof["knn"], active_mean * knn_bytes_per_site(K)),
@@ -341,13 +677,12 @@ def run_ours(args):
     ms, alg_bytes = groups[dom]
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (ms * 1e-3) / 1e9
-    tr = traffic_from_profiles(dom)
+    tr, tr_src = traffic_recorded(cfg["workload"], dom, n)
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": tr, "kernel": dom, "algorithmic_bytes_per_launch": alg_bytes,
-                "ms_per_launch": ms, "peak_source": peak_kind,
+                "traffic": tr, "traffic_source": tr_src, "kernel": dom,
+                "algorithmic_bytes_per_launch": alg_bytes, "ms_per_launch": ms, "peak_source": peak_kind,
                 "stage_ms_per_iter": {k: round(v, 5) for k, v in prof.items()}}
 
-    # ---- accuracy: drift of the mixed profile vs FP64 state ----------------
     acc = None
     if not args.no_accuracy and rank == 0:
         e64 = E.Engine(E.params(k=K, mode=p["mode"], profile="fp64"), 1, n, cells)
@@ -361,49 +696,32 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
-        cpu = cpu_baseline(m, S, p, budget_s=args.cpu_seconds)
+        si, secs, used, _ = cpu_sample([("torus", m.V, m.F, S)], K, p["mode"], iters, args.cpu_seconds)
+        from oracle import oracle as O
+        cpu = {"value": si / secs, "unit": UNIT, "cores": O.max_threads(), "kind": "port",
+               "sample": f"{used} whole remesh(es) of {n} sites x {iters} iterations, mixed profile, {secs:.1f} s"}
 
     eng.close()
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
                 "warmup": max(args.warmup, 3), "ms_per_step": tot / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(cfg, parallelism=f"replicas x{ws}" if ws > 1 else "single GPU"),
-                "latency_ms": {"p50": p50, "p99": p99, "what": "one full remesh (100 iterations), device time"},
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": cfg,
+                "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99)),
+                               "what": "one full remesh (100 iterations), device time"},
                 "frozen_sites_at_end": frozen,
                 "e2e": {"value": ws * n * iters / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms, "api": "cvt_remesh (host buffers)",
                         "same_sites_as_engine": same_as_engine},
                 "gpu_launches": int(sum(launches)),
                 "roofline": roofline,
-                "issue_roofline": issue_roofline(prof, iters, clk.get("sm_mhz") or clk.get("sm_max_mhz")),
-                "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
+                "issue_roofline": issue_roofline(cfg["workload"], prof, iters, clk.get("sm_mhz") or clk.get("sm_max_mhz")),
+                "cpu_baseline": cpu, "accuracy": acc, "clocks": clk, "tiles": E.tiles(prm),
                 "libgpucvt_launches_total": _lib.launch_count()}
         print(json.dumps(line), flush=True)
     if ws > 1:
+        import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
-    return 0
-
-
-def run_batched(args):
-    """256 procedural meshes (spheres, tori, superquadrics; 4.8k-200k
-    triangles, ~3.1M sites in total, K=24, 100 iterations) as segments of one
-    engine vs the plain per-mesh loop (same kernels, one mesh at a time)."""
-    import torch
-    from gpu_cvt_b200 import workloads
-    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    r = workloads.batched_vs_plain(n_meshes=args.meshes, iters=100, k=24, mode=0, profile="ref", seed=3)
-    line = {"metric": METRIC, "value": r["batched_sites_iters_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1,
-            "warmup": 1, "ms_per_step": r["batched_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"batched_{args.meshes}_meshes", "seed": 3, "k": 24, "iters": 100, "mode": 0,
-                       "profile": "ref", "sites_total": r["sites_total"],
-                       "tris_per_mesh": [r["tris_min"], r["tris_max"]], "tiles": r["tiles"]},
-            "plain_loop": {"value": r["plain_sites_iters_per_s"], "ms": r["plain_loop_s"] * 1e3},
-            "batched_over_plain": r["speedup"], "identical_results": r["identical_results"],
-            "mesh_generation_s": r["mesh_generation_s"]}
-    print(json.dumps(line), flush=True)
     return 0
 
 
@@ -442,7 +760,8 @@ def run_serve(args):
             "config": {"workload": "serve_poisson", "requests": args.requests, "rate_per_s": 200.0, "seed": 4,
                        "sites_per_request": [2000, 2000000], "stop": "max motion < 1e-4 bbox diag, cap 150",
                        "k": 24, "mode": 1, "profile": "mixed", "hbm_budget_gb": args.hbm_gb,
-                       "sites_total": int(sum(r.n for r in reqs)), "tiles": E.tiles(prm)},
+                       "sites_total": int(sum(r.n for r in reqs))},
+            "tiles": E.tiles(prm),
             "latency_s": {"p50": served["latency_p50_s"], "p99": served["latency_p99_s"],
                           "mean": served["latency_mean_s"]},
             "served": served, "plain_fifo": plain,
@@ -472,29 +791,30 @@ def run_precision(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["batched", "torus_100k", "serve", "superellipsoid_1m"], default="batched")
+    ap.add_argument("--meshes", type=int, default=256, help="batched workload: number of meshes (256)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=120.0,
                     help="reference arm: seconds of CPU work to size the steps for")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
-    ap.add_argument("--workload", choices=["torus_100k", "batched", "serve", "superellipsoid_1m"],
-                    default="torus_100k")
-    ap.add_argument("--meshes", type=int, default=256)
+    ap.add_argument("--no-plain", action="store_true", help="batched: skip the plain per-mesh loop")
+    ap.add_argument("--no-c3", action="store_true", help="batched: skip the 1M-site rounded-box figures")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--hbm-gb", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "batched":
-        return run_batched(args)
+        return run_ours_batched(args)
     if args.workload == "serve":
         return run_serve(args)
     if args.workload == "superellipsoid_1m":
         return run_precision(args)
-    return run_ours(args)
+    return run_ours_torus(args)
 
 
 if __name__ == "__main__":

@@ -30,7 +30,7 @@ class MeshInfo(C.Structure):
 class Params(C.Structure):
     _fields_ = [("k", i32), ("mode", i32), ("profile", i32), ("kproj", i32), ("ex_quirk", i32),
                 ("cell_factor", f32), ("use_graph", i32), ("knn_block", i32), ("clip_block", i32),
-                ("proj_block", i32)]
+                ("proj_block", i32), ("proj_mode", i32), ("frame_mode", i32)]
 
 
 class EvalOut(C.Structure):
@@ -57,6 +57,8 @@ _SIGS = {
     "cvt_restore_frozen_rows": [vp, vp, vp, i32, i32, vp],
     "cvt_vertex_normals": [vp, i32, vp, i32, vp, vp, vp, vp],
     "cvt_frames": [vp, vp, i32, i32, vp, vp, vp],
+    "cvt_frames_pca": [vp, i32, vp, i32, vp, vp, i32, vp, vp, vp],
+    "cvt_project_bvh": [vp, vp, i32, i32, vp, vp, vp],
     "cvt_clip_centroids": [vp, vp, vp, vp, i32, i32, f32, i32, vp, vp, vp],
     "cvt_project": [vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, vp, vp, vp],
     "cvt_freeze": [vp, vp, vp, vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp],
@@ -94,6 +96,7 @@ _SIGS = {
     "cvt_extract_faces": [vp, vp, vp, vp, i32, i32, f32, vp, i32, vp, vp],
     "cvt_quality": [vp, vp, i32, vp, vp],
     "cvt_remesh": [vp, i32, vp, i32, vp, i32, vp, i32, vp, vp],
+    "cvt_remesh_batch": [i32, vp, vp, vp, vp, vp, vp, vp, i32, vp],
 }
 _RESTYPES = {"cvt_status_string": C.c_char_p, "cvt_last_error": C.c_char_p, "cvt_version": i32,
              "cvt_launch_count": u64, "cvt_set_vertex_cell_factor": None, "cvt_params_default": None}

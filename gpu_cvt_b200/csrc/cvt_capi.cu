@@ -2,6 +2,7 @@
 // Unity translation unit: the device code lives in the included headers.
 #include <algorithm>
 #include <atomic>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -344,6 +345,16 @@ extern "C" cvt_status_t cvt_frames(const float* N0, const int* knnV, int kproj, 
   return CVT_OK;
 }
 
+extern "C" cvt_status_t cvt_frames_pca(const float* S, int n, const uint32_t* knn, int K, const float* N0,
+                                       const int* knnV, int kproj, float* U, float* V, void* stream) {
+  if (n < 0 || K < 1 || kproj < 1 || (n > 0 && (!S || !knn || !N0 || !knnV || !U || !V)))
+    return fail(CVT_ERR_INVALID, "cvt_frames_pca: bad arguments");
+  if (n == 0) return CVT_OK;
+  k_stage_frames_pca<<<cdiv(n, 128), 128, 0, S_(stream)>>>(S, n, knn, K, N0, knnV, kproj, U, V);
+  CKLAUNCH();
+  return CVT_OK;
+}
+
 constexpr int kClipBlock = 128;
 constexpr int kClipCap = 32;
 
@@ -454,6 +465,7 @@ struct cvt_mesh {
     MeshDev m;
     m.V = dV; m.F = dF; m.vf_off = doff; m.vf_faces = dfcs; m.N = dN;
     m.vcell_start = dvcell_start; m.vsorted = dvsorted; m.ring = dring; m.vg = vg;
+    m.bvh = dnodes; m.bvh_tri = dtri;
     m.nV = nV; m.nF = nF; m.R = R;
     m.thr2 = ((0.01f * R) * 0.01f) * R;
     return m;
@@ -860,6 +872,32 @@ extern "C" cvt_status_t cvt_mesh_get_bvh(cvt_mesh_t m, void* nodes, int nodes_ca
   return CVT_OK;
 }
 
+extern "C" cvt_status_t cvt_project_bvh(cvt_mesh_t m, const float* cent, int n, int profile, const float* Sold,
+                                        float* Snew, void* stream) {
+  if (!m || n < 0 || (n > 0 && (!cent || !Snew))) return fail(CVT_ERR_INVALID, "cvt_project_bvh: bad arguments");
+  if (profile == CVT_PROFILE_MIXED && n > 0 && !Sold) return fail(CVT_ERR_INVALID, "cvt_project_bvh: MIXED needs Sold");
+  if (profile != CVT_PROFILE_REF && profile != CVT_PROFILE_MIXED)
+    return fail(CVT_ERR_UNSUPPORTED, "cvt_project_bvh: profile must be REF or MIXED (FP64 runs in the engine)");
+  if (n == 0) return CVT_OK;
+  cvt_status_t ls = mesh_ensure_bvh(m);
+  if (ls != CVT_OK) return ls;
+  cudaStream_t st = S_(stream);
+  Scratch sc(st);
+  int* ovf;
+  CK(sc.get(&ovf, 1));
+  CK(cudaMemsetAsync(ovf, 0, sizeof(int), st));
+  if (profile == CVT_PROFILE_REF)
+    k_stage_project_bvh<PROF_REF><<<cdiv(n, 128), 128, 0, st>>>(cent, n, m->dnodes, m->dtri, m->dV, m->dF, Sold, Snew, ovf);
+  else
+    k_stage_project_bvh<PROF_MIXED><<<cdiv(n, 128), 128, 0, st>>>(cent, n, m->dnodes, m->dtri, m->dV, m->dF, Sold, Snew, ovf);
+  CKLAUNCH();
+  int h_ovf = 0;
+  CK(cudaMemcpyAsync(&h_ovf, ovf, sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (h_ovf) return fail(CVT_ERR_CAPACITY, "cvt_project_bvh: BVH traversal stack overflow");
+  return CVT_OK;
+}
+
 extern "C" cvt_status_t cvt_hausdorff_meshes(cvt_mesh_t a, cvt_mesh_t b, float* out, float* a_to_b, float* b_to_a,
                                              void* stream) {
   if (!a || !b || !out) return fail(CVT_ERR_INVALID, "cvt_hausdorff_meshes: bad arguments");
@@ -917,6 +955,8 @@ extern "C" void cvt_params_default(cvt_params_t* p) {
   p->cell_factor = 1.1f;
   p->use_graph = 1;
   p->knn_block = p->clip_block = p->proj_block = 0;
+  p->proj_mode = CVT_PROJ_ONERING;
+  p->frame_mode = CVT_FRAME_VERTEX_NORMAL;
 }
 
 // launch shapes the tiles may take (cvt_params_t knn_block / clip_block /
@@ -1024,7 +1064,8 @@ struct cvt_engine {
   int* d_stats = nullptr;
   int* d_ovf = nullptr;
   int* d_far = nullptr;
-  unsigned* d_tickets = nullptr;  // [0] grid scan, [1] far sites + bookkeeping (zero between launches)
+  unsigned* d_tickets = nullptr;  // [0] grid scan, [1] far sites + bookkeeping (zero between launches),
+                                  // [2] BVH stack overflows of the projection (never expected)
   int num_sms = 148;
   void* d_cent = nullptr;
   // graphs
@@ -1045,10 +1086,11 @@ struct cvt_engine {
 // remesh).  At most kGraphCacheMax are kept; cvt_release_cached_memory
 // destroys them.
 struct GraphKey {
-  int dev, profile, k, knn_block, clip_block, proj_block;
+  int dev, profile, k, knn_block, clip_block, proj_block, proj_mode, frame_mode;
   bool operator==(const GraphKey& o) const {
     return dev == o.dev && profile == o.profile && k == o.k && knn_block == o.knn_block &&
-           clip_block == o.clip_block && proj_block == o.proj_block;
+           clip_block == o.clip_block && proj_block == o.proj_block && proj_mode == o.proj_mode &&
+           frame_mode == o.frame_mode;
   }
 };
 constexpr size_t kGraphCacheMax = 16;
@@ -1056,7 +1098,8 @@ static std::mutex g_graph_mu;
 static std::vector<std::pair<GraphKey, cudaGraphExec_t>> g_graph_cache;
 
 static GraphKey graph_key(const cvt_engine* e) {
-  return {e->dev, e->p.profile, e->K, e->p.knn_block, e->p.clip_block, e->p.proj_block};
+  return {e->dev, e->p.profile, e->K, e->p.knn_block, e->p.clip_block, e->p.proj_block, e->p.proj_mode,
+          e->p.frame_mode};
 }
 
 static cudaGraphExec_t graph_cache_take(const GraphKey& k) {
@@ -1116,6 +1159,8 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   if (p->kproj != kKProj) return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: kproj must be 5");
   if (p->mode < 0 || p->mode > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: mode must be 0, 1 or 2");
   if (p->profile < 0 || p->profile > 2) return fail(CVT_ERR_INVALID, "cvt_engine_create: profile");
+  if (p->proj_mode < 0 || p->proj_mode > 1) return fail(CVT_ERR_INVALID, "cvt_engine_create: proj_mode must be 0 or 1");
+  if (p->frame_mode < 0 || p->frame_mode > 1) return fail(CVT_ERR_INVALID, "cvt_engine_create: frame_mode must be 0 or 1");
   cvt_params_t q = *p;
   if (!resolve_tiles(&q))
     return fail(CVT_ERR_UNSUPPORTED, "cvt_engine_create: knn_block / proj_block must be 64, 128 or 256, clip_block "
@@ -1176,7 +1221,7 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   ar.add(&e->d_stats, (size_t)max_segments * kStatsRing * kStatsWords);
   ar.add(&e->d_ovf, ns + 1);
   ar.add(&e->d_far, ns + 1);
-  ar.add(&e->d_tickets, 2);
+  ar.add(&e->d_tickets, 3);  // scan ticket, bookkeeping ticket, BVH stack overflows
   ar.add(reinterpret_cast<char**>(&e->d_cent), tsz * 3 * ns);
   ECK(ar.commit(&e->arena));
   e->bytes = ar.size;
@@ -1206,6 +1251,10 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   int s = -1;
   for (int k = 0; k < e->max_seg; ++k) if (!e->active[k] && !e->seg_mesh[k]) { s = k; break; }
   if (s < 0) return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: no free segment slot");
+  if (e->p.proj_mode == CVT_PROJ_BVH) {
+    cvt_status_t bs = mesh_ensure_bvh(mesh);  // the projection walks it
+    if (bs != CVT_OK) return bs;
+  }
   GridGeom g = surface_grid(mesh->lo, mesh->hi, mesh->area, n, (double)(e->K + 1), e->p.cell_factor, 4L * n + 64);
   int cells = g.ncell + 1;
   int base = e->site_alloc.take(n);
@@ -1303,6 +1352,7 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   a.frozen = e->d_frozen; a.streak = e->d_streak; a.tier = e->d_tier;
   a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
   a.stats = e->d_stats; a.ovf = e->d_ovf; a.far = e->d_far; a.cent = (T*)e->d_cent; a.K = e->K;
+  a.proj_mode = e->p.proj_mode; a.bvh_ovf = reinterpret_cast<int*>(e->d_tickets + 2);
   return a;
 }
 
@@ -1315,24 +1365,41 @@ static void launch_site_knn(const EngineArgs<T>& a, int nsites, int bs, cudaStre
   else k_site_knn<T, KK, 128><<<nb, 128, 0, st>>>(a);
 }
 
-template <int PROF>
-static void launch_site_clip(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, cudaStream_t st) {
+template <int PROF, int FRAME>
+static void launch_site_clip_f(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, int nsm,
+                               cudaStream_t st) {
   using PP = typename PT<PROF>::PP;
   const size_t smem = 2 * kCellCap * (size_t)bs * sizeof(V2<PP>);
   if (sizeof(PP) == 8) {
-    if (bs == 32) k_site_clip<PROF, 32, kCellCap><<<cdiv(ns, 32), 32, smem, st>>>(a, parity);
-    else k_site_clip<PROF, 64, kCellCap><<<cdiv(ns, 64), 64, smem, st>>>(a, parity);
+    if (bs == 32) k_site_clip<PROF, 32, kCellCap, FRAME><<<cdiv(ns, 32), 32, smem, st>>>(a, parity);
+    else k_site_clip<PROF, 64, kCellCap, FRAME><<<cdiv(ns, 64), 64, smem, st>>>(a, parity);
   } else {
-    if (bs == 64) k_site_clip<PROF, 64, kCellCap><<<cdiv(ns, 64), 64, smem, st>>>(a, parity);
-    else k_site_clip<PROF, 128, kCellCap><<<cdiv(ns, 128), 128, smem, st>>>(a, parity);
+    if (bs == 64) k_site_clip<PROF, 64, kCellCap, FRAME><<<cdiv(ns, 64), 64, smem, st>>>(a, parity);
+    else k_site_clip<PROF, 128, kCellCap, FRAME><<<cdiv(ns, 128), 128, smem, st>>>(a, parity);
   }
+  k_clip_overflow<PROF, FRAME><<<nsm, 64, 0, st>>>(a, parity);
+}
+
+// the clip kernel and its overflow fallback (two launches)
+template <int PROF>
+static void launch_site_clip(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, int frame_mode,
+                             int nsm, cudaStream_t st) {
+  if (frame_mode == 1) launch_site_clip_f<PROF, 1>(a, parity, ns, bs, nsm, st);
+  else launch_site_clip_f<PROF, 0>(a, parity, ns, bs, nsm, st);
+}
+
+template <int PROF, int PROJ>
+static void launch_site_proj_p(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, cudaStream_t st) {
+  if (bs == 64) k_site_proj<PROF, 64, PROJ><<<cdiv(ns, 64), 64, 0, st>>>(a, parity);
+  else if (bs == 256) k_site_proj<PROF, 256, PROJ><<<cdiv(ns, 256), 256, 0, st>>>(a, parity);
+  else k_site_proj<PROF, 128, PROJ><<<cdiv(ns, 128), 128, 0, st>>>(a, parity);
 }
 
 template <int PROF>
-static void launch_site_proj(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, cudaStream_t st) {
-  if (bs == 64) k_site_proj<PROF, 64><<<cdiv(ns, 64), 64, 0, st>>>(a, parity);
-  else if (bs == 256) k_site_proj<PROF, 256><<<cdiv(ns, 256), 256, 0, st>>>(a, parity);
-  else k_site_proj<PROF, 128><<<cdiv(ns, 128), 128, 0, st>>>(a, parity);
+static void launch_site_proj(const EngineArgs<typename PT<PROF>::T>& a, int parity, int ns, int bs, int proj_mode,
+                             cudaStream_t st) {
+  if (proj_mode == 1) launch_site_proj_p<PROF, 1>(a, parity, ns, bs, st);
+  else launch_site_proj_p<PROF, 0>(a, parity, ns, bs, st);
 }
 
 
@@ -1386,11 +1453,10 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   L++;
   if (ev) CK(cudaEventRecord(ev[2], st));
   CK(cudaStreamWaitEvent(st, br.join, 0));
-  launch_site_clip<PROF>(a, parity, ns, e->p.clip_block, st);
-  k_clip_overflow<PROF><<<e->num_sms, 64, 0, st>>>(a, parity);
+  launch_site_clip<PROF>(a, parity, ns, e->p.clip_block, e->p.frame_mode, e->num_sms, st);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[3], st));
-  launch_site_proj<PROF>(a, parity, ns, e->p.proj_block, st);
+  launch_site_proj<PROF>(a, parity, ns, e->p.proj_block, e->p.proj_mode, st);
   k_site_far<PROF><<<e->num_sms, 128, 0, st>>>(a, parity, e->d_segs, e->d_active, e->max_seg, e->d_tickets + 1);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[4], st));
@@ -1671,6 +1737,42 @@ extern "C" cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF,
   }
   cvt_engine_destroy(e);
   cvt_mesh_destroy(m);
+  return s;
+}
+
+// Many meshes in one call: every mesh becomes a segment of one engine, so
+// each Lloyd iteration of all of them is one pass of the iteration's kernels.
+extern "C" cvt_status_t cvt_remesh_batch(int n_meshes, const float* const* V, const int* nV, const int* const* F,
+                                         const int* nF, const float* const* sites_in, const int* n_sites,
+                                         const cvt_params_t* p, int iters, float* const* sites_out) {
+  if (n_meshes < 1 || !V || !nV || !F || !nF || !sites_in || !n_sites || !p || !sites_out || iters < 0)
+    return fail(CVT_ERR_INVALID, "cvt_remesh_batch: bad arguments");
+  for (int i = 0; i < n_meshes; ++i)
+    if (!V[i] || !F[i] || !sites_in[i] || !sites_out[i] || n_sites[i] < 1)
+      return fail(CVT_ERR_INVALID, "cvt_remesh_batch: bad arguments for mesh " + std::to_string(i));
+  std::vector<cvt_mesh_t> meshes(n_meshes, nullptr);
+  cvt_status_t s = CVT_OK;
+  long total_sites = 0, total_cells = 0;
+  for (int i = 0; i < n_meshes && s == CVT_OK; ++i) {
+    s = cvt_mesh_create(V[i], nV[i], F[i], nF[i], &meshes[i]);
+    if (s != CVT_OK) break;
+    int cells = 0;
+    engine_caps(meshes[i], n_sites[i], p, &cells);
+    total_sites += n_sites[i];
+    total_cells += cells;
+  }
+  if (s == CVT_OK && (total_sites > INT_MAX || total_cells > INT_MAX))
+    s = fail(CVT_ERR_CAPACITY, "cvt_remesh_batch: more than 2^31 sites or grid cells in one call");
+  cvt_engine_t e = nullptr;
+  if (s == CVT_OK) s = cvt_engine_create(p, n_meshes, (int)total_sites, (int)total_cells, &e);
+  std::vector<int> seg(n_meshes, -1);
+  for (int i = 0; i < n_meshes && s == CVT_OK; ++i)
+    s = cvt_engine_add_segment(e, meshes[i], sites_in[i], n_sites[i], 0, &seg[i], nullptr);
+  if (s == CVT_OK) s = cvt_engine_run(e, iters, nullptr);
+  for (int i = 0; i < n_meshes && s == CVT_OK; ++i) s = cvt_engine_get_sites(e, seg[i], sites_out[i], 0, nullptr);
+  if (e) cvt_engine_destroy(e);
+  for (cvt_mesh_t m : meshes)
+    if (m) cvt_mesh_destroy(m);
   return s;
 }
 

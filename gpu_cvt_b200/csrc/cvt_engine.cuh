@@ -9,13 +9,15 @@
 //   k_site_knn   per active site (one warp): exact (K+1)-NN in its segment,
 //                drop self (site_knn.cuh:79); frozen sites keep the
 //                previous list (main.cu:678)
-//   k_site_clip  per site (one thread): frame (site_normals.cuh:69),
+//   k_site_clip  per site (one thread): frame (site_normals.cuh:69; or,
+//                as an option, from the PCA normal of the neighbours),
 //                tangent-plane clip and centroid (2dClip.cuh:82)
 //   k_clip_overflow  the same for the rare cells whose polygon outgrows
 //                the shared-memory buffer (exact 64-vertex cap)
 //   k_site_proj  per site (one thread): centroid -> 5 nearest
 //                vertices (main.cu:719-735, frozen sites keep theirs),
-//                one-ring projection (near_project.cuh:149), freeze test
+//                one-ring projection (near_project.cuh:149; or, as an
+//                option, the exact closest point through the BVH), freeze test
 //                and apply (freezetest.cuh:155-212, 270-327, 451-466),
 //                tier assignment on the segment's first iteration
 //                (main.cu:640-667)
@@ -50,6 +52,8 @@ struct MeshDev {
   const int* vcell_start;
   const Pt4<float>* vsorted;
   const float4* ring;  // one-ring records, kRingWords per CSR entry (k_build_ring_records)
+  const BVHNode* bvh;  // BVH over the faces (built before a segment that projects through it is placed)
+  const int* bvh_tri;
   GridGeom vg;
   int nV, nF;
   float R;     // clip square half-size: longest input bbox edge (main.cu:421)
@@ -100,6 +104,8 @@ template <class T> struct EngineArgs {
   int* far;  // [0] = count, [1 + k] = site whose vertex search was deferred
   T* cent;   // centroid per site (3 values), k_site_clip -> k_site_proj
   int K;
+  int proj_mode;  // 0: one-ring of the KPROJ nearest vertices; 1: closest point through the BVH
+  int* bvh_ovf;   // BVH traversal stack overflows (never expected: the tree depth is bounded)
 };
 
 // polygon storage: vertex k at p[k * stride] (shared memory: thread-
@@ -439,7 +445,7 @@ struct SiteOut {
 
 // Frame, clip and centroid of site g into a.cent; false when the polygon
 // outgrew the buffers (the site is then redone by k_clip_overflow).
-template <int PROF>
+template <int PROF, int FRAME>
 __device__ __forceinline__ bool site_clip(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g,
                                           PolyRef<typename PT<PROF>::PP> A, PolyRef<typename PT<PROF>::PP> B,
                                           int cap) {
@@ -451,11 +457,19 @@ __device__ __forceinline__ bool site_clip(const EngineArgs<typename PT<PROF>::T>
   const T* __restrict__ S = a.S[parity];
   const bool fz = sd.mode != 0 && a.frozen[g];
   const V3<T> si = ld3(S, g);
-  // frame from the nearest vertex normal (frozen sites: their kept vertex list)
-  const int nn = fz ? a.knnv[(size_t)g * kKProj] : a.nnv[g];
+  // frame from the nearest vertex normal (frozen sites: their kept vertex
+  // list; with the BVH projection, which keeps no vertex list, their kept
+  // frame vertex); FRAME 1: from the PCA normal of the neighbour list,
+  // started from that vertex normal
+  const int nn = (fz && a.proj_mode == 0) ? a.knnv[(size_t)g * kKProj] : a.nnv[g];
   Frame<T> fr;
-  if (nn < 0) fr = {{(T)1, (T)0, (T)0}, {(T)0, (T)1, (T)0}};
-  else fr = frame_from_normal(V3<T>{(T)__ldg(md.N + 3 * nn), (T)__ldg(md.N + 3 * nn + 1), (T)__ldg(md.N + 3 * nn + 2)});
+  if (nn < 0) {
+    fr = {{(T)1, (T)0, (T)0}, {(T)0, (T)1, (T)0}};
+  } else {
+    V3<T> n0{(T)__ldg(md.N + 3 * nn), (T)__ldg(md.N + 3 * nn + 1), (T)__ldg(md.N + 3 * nn + 2)};
+    if (FRAME == 1) n0 = pca_normal(S, sd.site_base, sd.n_sites, a.knn + (size_t)g * a.K, a.K, si, n0);
+    fr = frame_from_normal(n0);
+  }
   PolyRef<PP> cur = A, nxt = B;
   const int np = clip_cell<PROF>(S, sd.site_base, sd.n_sites, si, a.knn + (size_t)g * a.K, a.K, fr, md.R, cur, nxt,
                                  cap, !fz);
@@ -473,7 +487,7 @@ __device__ __forceinline__ bool site_clip(const EngineArgs<typename PT<PROF>::T>
   return true;
 }
 
-template <int PROF, int BLOCK, int CAP>
+template <int PROF, int BLOCK, int CAP, int FRAME>
 __global__ void __launch_bounds__(BLOCK, (sizeof(typename PT<PROF>::PP) == 8 ? kClipThreadsD : kClipThreadsF) / BLOCK)
     k_site_clip(EngineArgs<typename PT<PROF>::T> a, int parity) {
   using PP = typename PT<PROF>::PP;
@@ -484,25 +498,26 @@ __global__ void __launch_bounds__(BLOCK, (sizeof(typename PT<PROF>::PP) == 8 ? k
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   if (t < n_grid) {
     const int g = (int)a.sorted[t].id;
-    if (!site_clip<PROF>(a, parity, g, A, B, CAP)) {
+    if (!site_clip<PROF, FRAME>(a, parity, g, A, B, CAP)) {
       const int k = atomicAdd(a.ovf, 1);
       a.ovf[1 + k] = g;
     }
   }
 }
 
-template <int PROF>
+template <int PROF, int FRAME>
 __global__ void __launch_bounds__(64) k_clip_overflow(EngineArgs<typename PT<PROF>::T> a, int parity) {
   using PP = typename PT<PROF>::PP;
   V2<PP> buf[2][kFallbackCap];
   const int n = *(volatile int*)a.ovf;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x)
-    site_clip<PROF>(a, parity, a.ovf[1 + k], PolyRef<PP>{buf[0], 1}, PolyRef<PP>{buf[1], 1}, kFallbackCap);
+    site_clip<PROF, FRAME>(a, parity, a.ovf[1 + k], PolyRef<PP>{buf[0], 1}, PolyRef<PP>{buf[1], 1}, kFallbackCap);
 }
 
 // Projection, tiers and the freeze test of site g, given the centroid in
-// a.cent and its 5 nearest vertices knnv.
-template <int PROF>
+// a.cent and (PROJ 0) its 5 nearest vertices knnv; PROJ 1 projects through
+// the mesh's BVH and ignores knnv.
+template <int PROF, int PROJ>
 __device__ __forceinline__ void site_finish(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g,
                                             const int (&knnv)[kKProj], SiteOut& o) {
   using T = typename PT<PROF>::T;
@@ -520,6 +535,9 @@ __device__ __forceinline__ void site_finish(const EngineArgs<typename PT<PROF>::
   V3<T> sn;
   if (PROF == PROF_MIXED && !finite3(cent)) {
     sn = si;
+  } else if (PROJ == 1) {
+    using Q = typename PT<PROF>::Q;
+    sn = project_bvh<T, Q>(cent, md.bvh, md.bvh_tri, md.V, md.F, (Q)bvh_bound2(cent, si), a.bvh_ovf);
   } else if (PROF == PROF_REF) {
     sn = project_onering_rec<T, float>(cent, md.ring, md.nV, md.vf_off, knnv, kKProj);
   } else {
@@ -572,9 +590,14 @@ constexpr int kVertexRingLimit = 4;
 
 // Everything after the centroid; false when the 5-NN search was deferred
 // (the site is then listed in a.far and finished by k_site_far).
-template <int PROF>
+template <int PROF, int PROJ>
 __device__ __forceinline__ bool site_proj(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g, SiteOut& o) {
   using T = typename PT<PROF>::T;
+  if (PROJ == 1) {
+    const int none[kKProj] = {-1, -1, -1, -1, -1};
+    site_finish<PROF, 1>(a, parity, g, none, o);
+    return true;
+  }
   const int s = __ldg(a.site_seg + g);
   const SegDev& sd = a.segs[s];
   const MeshDev& md = a.meshes[sd.mesh];
@@ -597,7 +620,7 @@ __device__ __forceinline__ bool site_proj(const EngineArgs<typename PT<PROF>::T>
 #pragma unroll
     for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];
   }
-  site_finish<PROF>(a, parity, g, knnv, o);
+  site_finish<PROF, 0>(a, parity, g, knnv, o);
   return true;
 }
 
@@ -665,7 +688,7 @@ __device__ __forceinline__ void stats_stage_flush(int* stats, const SegDev* segs
   atomicMax(reinterpret_cast<unsigned*>(sl + 4), stage.v[4]);
 }
 
-template <int PROF, int BS>
+template <int PROF, int BS, int PROJ>
 __global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
   __shared__ StatsStage stage;
   stats_stage_init(stage);
@@ -673,7 +696,7 @@ __global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::
   const int t = blockIdx.x * BS + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   SiteOut o{-1, 0, 0, 0, 0, 0.f};
-  if (t < n_grid) site_proj<PROF>(a, parity, (int)a.sorted[t].id, o);
+  if (t < n_grid) site_proj<PROF, PROJ>(a, parity, (int)a.sorted[t].id, o);
   stats_flush(a.stats, a.segs, o, stage);
   __syncthreads();
   stats_stage_flush(a.stats, a.segs, stage);
@@ -741,7 +764,7 @@ __global__ void __launch_bounds__(128) k_site_far(EngineArgs<typename PT<PROF>::
 #pragma unroll
       for (int j = 0; j < kKProj; ++j) { knnv[j] = (int)KeyOps<T>::idx(all.k[j]); kv[j] = knnv[j]; }
       SiteOut o{-1, 0, 0, 0, 0, 0.f};
-      site_finish<PROF>(a, parity, g, knnv, o);
+      site_finish<PROF, 0>(a, parity, g, knnv, o);
       stats_atomic(a.stats, a.segs, o);
     }
     __syncthreads();

@@ -9,21 +9,13 @@
 
 namespace cvt {
 
-// 40-byte node, layout of evaluate.cuh:15-22
-struct BVHNode {
-  float bmin[3], bmax[3];
-  int left, right, triStart, triCount;
-};
-
 // The tree is the reference's (bounds from the triangle boxes, leaf <= 8
 // triangles, otherwise the centroid-sorted list split at its middle, nodes in
 // pre-order, evaluate.cuh:114-201); it is built on the device, cvt_ingest.cuh.
 
 // Per-probe closest squared distance to the BVH surface.  Near-first
 // traversal: of two children the nearer box is visited first, which only
-// changes the order, not the minimum.  The stack holds at most one pending
-// sibling per level (depth <= 2*log2(nF) for the median split).
-constexpr int kBvhStack = 96;
+// changes the order, not the minimum (stack: kBvhStack, cvt_math.cuh).
 
 __device__ __forceinline__ float bvh_closest_d2(V3<float> p, const BVHNode* __restrict__ nodes,
                                                 const int* __restrict__ tri, const float* __restrict__ V,

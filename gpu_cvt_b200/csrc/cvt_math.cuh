@@ -68,6 +68,61 @@ template <class T> __device__ __forceinline__ Frame<T> frame_from_normal(V3<T> n
 }
 
 // --------------------------------------------------------------------------
+// PCA normal of a site's neighbourhood (frame option; the reference builds
+// every frame from the nearest vertex normal, site_normals.cuh:69-110).
+// The eigenvector of the smallest eigenvalue of the covariance C of the
+// listed neighbours' offsets, found by power iteration on the adjugate of C,
+// which has the same eigenvectors with the order reversed (error shrinks by
+// l1 / l2 per step: fast wherever the neighbourhood is a surface patch, even
+// a narrow one).  The iteration starts from the reference normal n0 and runs
+// a fixed kPcaSteps steps; its sign is then chosen to agree with n0.  Fewer
+// than 3 neighbours, a zero spread, or a non-finite result give n0 back.
+// Only IEEE-rounded arithmetic with an explicit operation order, so a CPU
+// restatement reproduces the bits.
+// --------------------------------------------------------------------------
+constexpr int kPcaSteps = 8;
+
+template <class T>
+__device__ __forceinline__ V3<T> pca_normal(const T* __restrict__ S, long site_base, int n_sites,
+                                            const uint32_t* __restrict__ row, int K, V3<T> si, V3<T> n0) {
+  T sx = 0, sy = 0, sz = 0, xx = 0, xy = 0, xz = 0, yy = 0, yz = 0, zz = 0;
+  int m = 0;
+  for (int t = 0; t < K; ++t) {
+    const uint32_t j = __ldg(row + t);
+    if (j >= (uint32_t)n_sites) continue;
+    const V3<T> d = sub3(ld3(S, site_base + (long)j), si);
+    sx = sx + d.x; sy = sy + d.y; sz = sz + d.z;
+    xx = fmaT(d.x, d.x, xx); xy = fmaT(d.x, d.y, xy); xz = fmaT(d.x, d.z, xz);
+    yy = fmaT(d.y, d.y, yy); yz = fmaT(d.y, d.z, yz); zz = fmaT(d.z, d.z, zz);
+    ++m;
+  }
+  if (m < 3) return n0;
+  const T im = divT((T)1, (T)m);
+  const T mx = sx * im, my = sy * im, mz = sz * im;
+  // C = sum d d^T - m mean mean^T = sum d d^T - s mean^T
+  const T cxx = fmaT(-sx, mx, xx), cxy = fmaT(-sx, my, xy), cxz = fmaT(-sx, mz, xz);
+  const T cyy = fmaT(-sy, my, yy), cyz = fmaT(-sy, mz, yz), czz = fmaT(-sz, mz, zz);
+  const T tr = (cxx + cyy) + czz;
+  if (!(tr > (T)1e-30)) return n0;
+  // adjugate of C: eigenvalues l2 l3, l1 l3, l1 l2 for C's l1 <= l2 <= l3,
+  // so the normal's (l1) direction dominates by the factor l2 / l1
+  const T axx = fmaT(cyy, czz, -(cyz * cyz)), axy = fmaT(cxz, cyz, -(cxy * czz)), axz = fmaT(cxy, cyz, -(cxz * cyy));
+  const T ayy = fmaT(cxx, czz, -(cxz * cxz)), ayz = fmaT(cxy, cxz, -(cxx * cyz)), azz = fmaT(cxx, cyy, -(cxy * cxy));
+  V3<T> v = n0;
+  for (int it = 0; it < kPcaSteps; ++it) {
+    const V3<T> w{fmaT(axz, v.z, fmaT(axy, v.y, axx * v.x)), fmaT(ayz, v.z, fmaT(ayy, v.y, axy * v.x)),
+                  fmaT(azz, v.z, fmaT(ayz, v.y, axz * v.x))};
+    const T nw = sqrtT(dot3(w, w));
+    if (!(nw > (T)1e-30)) return n0;
+    const T inv = divT((T)1, nw);
+    v = {w.x * inv, w.y * inv, w.z * inv};
+  }
+  if (!finite3(v)) return n0;
+  if (dot3(v, n0) < (T)0) v = {-v.x, -v.y, -v.z};
+  return v;
+}
+
+// --------------------------------------------------------------------------
 // centroid of the clipped polygon (2dClip.cuh:55-80); Neumaier compensation
 // in the MIXED profile.
 // --------------------------------------------------------------------------
@@ -309,6 +364,12 @@ __device__ __forceinline__ V3<T> project_onering_rec(V3<T> c, const float4* __re
 // --------------------------------------------------------------------------
 // evaluation primitives (evaluate.cuh:44-104)
 // --------------------------------------------------------------------------
+// 40-byte BVH node, layout of evaluate.cuh:15-22
+struct BVHNode {
+  float bmin[3], bmax[3];
+  int left, right, triStart, triCount;
+};
+
 __device__ __forceinline__ float aabb_d2(V3<float> p, const float* bmin, const float* bmax) {
   float d = 0.f;
   float q[3] = {p.x, p.y, p.z};
@@ -357,6 +418,78 @@ __device__ __forceinline__ float point_tri_d2(V3<float> p, V3<float> a, V3<float
   V3<float> pr{a.x + fmaT(ab.x, v, ac.x * w), a.y + fmaT(ab.y, v, ac.y * w), a.z + fmaT(ab.z, v, ac.z * w)};
   V3<float> d = sub3(p, pr);
   return dot3(d, d);
+}
+
+// Traversal stack: at most one pending sibling per level; the median-split
+// tree is at most 2 log2(nF) deep.
+constexpr int kBvhStack = 96;
+
+// Closest point on the whole mesh through the BVH (projection option; the
+// reference projects onto the one-rings of the KPROJ nearest vertices,
+// near_project.cuh:149-189).  Near-first traversal; a box is entered only
+// when its FP32 squared distance to c is below the best squared distance so
+// far, and a face replaces the best only with a strictly smaller squared
+// distance, so ties keep the first face met in traversal order.  `best`
+// starts at bound2, an upper bound of the answer (the caller's distance to a
+// point on the mesh, with margin); if no face beats it the search is rerun
+// without the bound.  Q is the barycentric arithmetic type.  The traversal
+// order and every comparison are fixed, so a CPU restatement that walks the
+// same tree returns the same bits.  A non-finite c is returned unchanged.
+template <class T, class Q>
+__device__ __forceinline__ V3<T> project_bvh(V3<T> c, const BVHNode* __restrict__ nodes, const int* __restrict__ tri,
+                                             const float* __restrict__ V, const int* __restrict__ F, Q bound2,
+                                             int* overflow) {
+  if (!finite3(c)) return c;
+  const V3<Q> cq = cvt3<Q>(c);
+  const V3<float> cf = cvt3<float>(c);
+  V3<Q> bp = cq;
+  int stack[kBvhStack];
+  for (int pass = 0; pass < 2; ++pass) {
+    Q best = pass == 0 ? bound2 : (Q)1e30;
+    bool found = false;
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+      const BVHNode nd = nodes[stack[--sp]];
+      if ((Q)aabb_d2(cf, nd.bmin, nd.bmax) >= best) continue;
+      if (nd.triCount > 0) {
+        for (int k = 0; k < nd.triCount; ++k) {
+          const int t = __ldg(tri + nd.triStart + k);
+          const int ia = __ldg(F + 3 * t), ib = __ldg(F + 3 * t + 1), ic = __ldg(F + 3 * t + 2);
+          const V3<Q> A = {(Q)__ldg(V + 3 * ia), (Q)__ldg(V + 3 * ia + 1), (Q)__ldg(V + 3 * ia + 2)};
+          const V3<Q> B = {(Q)__ldg(V + 3 * ib), (Q)__ldg(V + 3 * ib + 1), (Q)__ldg(V + 3 * ib + 2)};
+          const V3<Q> C = {(Q)__ldg(V + 3 * ic), (Q)__ldg(V + 3 * ic + 1), (Q)__ldg(V + 3 * ic + 2)};
+          const V3<Q> p = closest_point_tri(cq, A, B, C);
+          const V3<Q> dd = sub3(p, cq);
+          const Q d2 = dot3(dd, dd);
+          if (d2 < best) { best = d2; bp = p; found = true; }
+        }
+      } else {
+        const BVHNode L = nodes[nd.left], R = nodes[nd.right];
+        const Q dl = (Q)aabb_d2(cf, L.bmin, L.bmax), dr = (Q)aabb_d2(cf, R.bmin, R.bmax);
+        if (sp + 2 > kBvhStack) { atomicAdd(overflow, 1); continue; }
+        if (dl < dr) {
+          if (dr < best) stack[sp++] = nd.right;
+          if (dl < best) stack[sp++] = nd.left;
+        } else {
+          if (dl < best) stack[sp++] = nd.left;
+          if (dr < best) stack[sp++] = nd.right;
+        }
+      }
+    }
+    if (found) break;
+  }
+  return cvt3<T>(bp);
+}
+
+// Upper bound of the squared distance from c to the mesh, given a point s on
+// the mesh (up to rounding): (|c - s| (1 + 1e-4) + 1e-5 max|coordinate|)^2.
+template <class T>
+__device__ __forceinline__ double bvh_bound2(V3<T> c, V3<T> s) {
+  const double dx = (double)c.x - (double)s.x, dy = (double)c.y - (double)s.y, dz = (double)c.z - (double)s.z;
+  const double m = fmax(fmax(fabs((double)s.x), fabs((double)s.y)), fabs((double)s.z));
+  const double d = __dsqrt_rn(__fma_rn(dz, dz, __fma_rn(dy, dy, dx * dx))) * 1.0001 + 1e-5 * m;
+  return isfinite(d) ? d * d : 1e30;
 }
 
 }  // namespace cvt

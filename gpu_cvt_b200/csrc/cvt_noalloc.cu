@@ -21,7 +21,11 @@
 //     (different streams, or different host threads without ordering) race
 //     and corrupt each other's results -- order them on one stream;
 //   * the first call on a device looks the array's device address up
-//     (cudaGetSymbolAddress); make that first call before any stream capture.
+//     (cudaGetSymbolAddress); make that first call before any stream capture;
+//   * the address is cached per device ordinal for the life of the process:
+//     cudaDeviceReset (or any other teardown of the device's primary
+//     context) leaves it stale, so a program that resets a device must not
+//     call this entry point afterwards.
 
 #include <mutex>
 

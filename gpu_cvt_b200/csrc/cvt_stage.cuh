@@ -179,6 +179,22 @@ __global__ void k_stage_frames(const float* __restrict__ N0, const int* __restri
   st3(Vv, i, fr.v);
 }
 
+// frames from the PCA normal of each site's listed neighbours (pca_normal),
+// started from the normal of the vertex knnV[i * kproj] -- the frame option
+// of the engine (frame_mode 1)
+__global__ void k_stage_frames_pca(const float* __restrict__ S, int n, const uint32_t* __restrict__ knn, int K,
+                                   const float* __restrict__ N0, const int* __restrict__ knnV, int kproj,
+                                   float* __restrict__ U, float* __restrict__ Vv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int nn = knnV[(size_t)i * kproj];
+  if (nn < 0) { st3(U, i, V3<float>{1, 0, 0}); st3(Vv, i, V3<float>{0, 1, 0}); return; }
+  const V3<float> nrm = pca_normal<float>(S, 0, n, knn + (size_t)i * K, K, ld3(S, i), ld3(N0, nn));
+  Frame<float> fr = frame_from_normal(nrm);
+  st3(U, i, fr.u);
+  st3(Vv, i, fr.v);
+}
+
 // clip + centroid for every site; overflowing polygons go to the fallback
 template <int PROF, int BLOCK, int CAP>
 __global__ void __launch_bounds__(BLOCK) k_stage_clip(const float* __restrict__ S, const float* __restrict__ U,
@@ -250,6 +266,22 @@ __global__ void k_stage_project(const float* __restrict__ cent, const float* __r
   V3<float> r = (PROF == PROF_REF) ? project_onering<float, float>(c, V, nV, F, nF, off, fcs, kv, min(kproj, 16))
                                    : project_onering<float, double>(c, V, nV, F, nF, off, fcs, kv, min(kproj, 16));
   st3(Snew, i, r);
+}
+
+// exact closest point on the mesh through its BVH (project_bvh), the
+// projection option of the engine (proj_mode 1); Sold (may be NULL) bounds
+// the search and, in MIXED, replaces a non-finite centroid
+template <int PROF>
+__global__ void k_stage_project_bvh(const float* __restrict__ cent, int nQ, const BVHNode* __restrict__ nodes,
+                                    const int* __restrict__ tri, const float* __restrict__ V, const int* __restrict__ F,
+                                    const float* __restrict__ Sold, float* __restrict__ Snew, int* ovf) {
+  using Q = typename PT<PROF>::Q;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nQ) return;
+  V3<float> c = ld3(cent, i);
+  if (PROF == PROF_MIXED && !finite3(c)) { st3(Snew, i, ld3(Sold, i)); return; }
+  const Q bound2 = Sold ? (Q)bvh_bound2(c, ld3(Sold, i)) : (Q)1e30;
+  st3(Snew, i, project_bvh<float, Q>(c, nodes, tri, V, F, bound2, ovf));
 }
 
 struct FreezeTable { float thr2[6]; int need[6]; };

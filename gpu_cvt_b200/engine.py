@@ -25,8 +25,16 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
+PROJ = {"onering": 0, "bvh": 1}
+FRAME = {"vertex": 0, "pca": 1}
+
+
 def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1, use_graph=True,
-           knn_block=0, clip_block=0, proj_block=0) -> Params:
+           knn_block=0, clip_block=0, proj_block=0, proj="onering", frame="vertex") -> Params:
+    """Engine parameters.  proj: "onering" (the reference's projection onto
+    the one-rings of the 5 nearest vertices) or "bvh" (exact closest point
+    through the mesh's BVH); frame: "vertex" (the nearest vertex normal, as
+    the reference) or "pca" (PCA normal of the site's neighbours)."""
     p = Params()
     _lib.load().cvt_params_default(C.byref(p))
     p.k = int(k)
@@ -37,6 +45,8 @@ def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1,
     p.cell_factor = float(cell_factor)
     p.use_graph = int(bool(use_graph))
     p.knn_block, p.clip_block, p.proj_block = int(knn_block), int(clip_block), int(proj_block)
+    p.proj_mode = PROJ[proj] if isinstance(proj, str) else int(proj)
+    p.frame_mode = FRAME[frame] if isinstance(frame, str) else int(frame)
     return p
 
 
@@ -303,3 +313,34 @@ def remesh(V, F, sites, k=24, mode=0, profile="ref", iters=50, ex_quirk=True, ce
     call("cvt_remesh", _ptr(V), V.shape[0], _ptr(F), F.shape[0], _ptr(S), S.shape[0], C.byref(p), int(iters),
          _ptr(out), _ptr(counts))
     return (out, counts[:iters]) if with_counts else out
+
+
+def _host_ptr(a):
+    """Address of a host array: a C-contiguous numpy array, or a CPU torch
+    tensor (e.g. pinned with .pin_memory())."""
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda or not a.is_contiguous():
+            raise ValueError("remesh_batch takes contiguous host arrays")
+        return a.data_ptr()
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("remesh_batch takes contiguous host arrays")
+    return a.ctypes.data
+
+
+def remesh_batch(Vs, Fs, sites, prm: Params, iters: int, outs=None):
+    """Many meshes in one call through ``cvt_remesh_batch`` (host arrays in
+    and out; float32 V/sites, int32 F, numpy or CPU torch tensors).  Returns
+    the list of output site arrays (``outs`` when given, else new float32
+    numpy arrays)."""
+    n = len(Vs)
+    if not (len(Fs) == n == len(sites)) or n == 0:
+        raise ValueError("remesh_batch: one V, F and site array per mesh")
+    if outs is None:
+        outs = [np.zeros((int(S.shape[0]), 3), np.float32) for S in sites]
+    P = C.c_void_p * n
+    I = C.c_int * n
+    vp_, fp_, sp_, op_ = P(*[_host_ptr(v) for v in Vs]), P(*[_host_ptr(f) for f in Fs]), \
+        P(*[_host_ptr(s) for s in sites]), P(*[_host_ptr(o) for o in outs])
+    nv, nf, ns = I(*[int(v.shape[0]) for v in Vs]), I(*[int(f.shape[0]) for f in Fs]), I(*[int(s.shape[0]) for s in sites])
+    call("cvt_remesh_batch", n, vp_, nv, fp_, nf, sp_, ns, C.byref(prm), int(iters), op_)
+    return outs

@@ -61,9 +61,10 @@ def run_batched(meshes, k=24, mode=0, profile="ref", iters=100, stream=None, prm
     return e0.elapsed_time(e1) / 1e3, eng, segs, M
 
 
-def run_plain_loop(meshes, k=24, mode=0, profile="ref", iters=100, prm=None):
+def run_plain_loop(meshes, k=24, mode=0, profile="ref", iters=100, prm=None, per_mesh=False):
     """One mesh at a time through one engine sized for the largest; every
-    mesh's 100 iterations replayed from the same CUDA graphs."""
+    mesh's 100 iterations replayed from the same CUDA graphs.  Returns
+    (total seconds, final sites per mesh[, device seconds per mesh])."""
     import torch
     M = [E.Mesh(V, F) for _, V, F, _ in meshes]
     nmax = max(S.shape[0] for *_, S in meshes)
@@ -75,7 +76,7 @@ def run_plain_loop(meshes, k=24, mode=0, profile="ref", iters=100, prm=None):
     _sync()
     eng.remove(g)
     total = 0.0
-    finals = []
+    finals, each = [], []
     for m, (*_, S) in zip(M, meshes):
         g = eng.add(m, S)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -83,13 +84,14 @@ def run_plain_loop(meshes, k=24, mode=0, profile="ref", iters=100, prm=None):
         eng.run(iters, C_stream(st))
         e1.record(st)
         e1.synchronize()
-        total += e0.elapsed_time(e1) / 1e3
+        each.append(e0.elapsed_time(e1) / 1e3)
+        total += each[-1]
         finals.append(eng.sites(g))
         eng.remove(g)
     eng.close()
     for m in M:
         m.close()
-    return total, finals
+    return (total, finals, each) if per_mesh else (total, finals)
 
 
 def C_stream(st):

@@ -71,7 +71,10 @@ cvt_status_t cvt_knn_sites(const float* pts, int n, int kk, const uint8_t* froze
  * frees nothing.  At most CVT_NOALLOC_MAX_POINTS points (larger n returns
  * CVT_ERR_CAPACITY).  All calls share the array: calls that overlap on the
  * GPU race; keep them ordered on one stream.  The first call on a device
- * looks up the array's address; make it before any stream capture. */
+ * looks up the array's address; make it before any stream capture.  The
+ * address is kept for the life of the process: after cudaDeviceReset (or
+ * anything else that destroys the device's primary context) it is stale, so
+ * a program that resets a device must not call this entry point again. */
 #define CVT_NOALLOC_MAX_POINTS 131072
 cvt_status_t cvt_knn_sites_noalloc(const float* pts, int n, int kk, const uint8_t* frozen,
                                    uint32_t* knn, float* dist, void* stream);
@@ -108,6 +111,14 @@ cvt_status_t cvt_vertex_normals(const float* V, int nV, const int* F, int nF, co
  * frame of site i from the normal of vertex knnV[i*kproj]. */
 cvt_status_t cvt_frames(const float* N0, const int* knnV, int kproj, int n, float* U, float* V,
                         void* stream);
+/* Option beside uv_from_nearest_vertex_normal (site_normals.cuh:69-110):
+ * frame of site i from the PCA normal of its K listed neighbours (knn: n*K
+ * local indices into S) -- the eigenvector of the smallest eigenvalue of
+ * their covariance, by a fixed power iteration started from the normal of
+ * vertex knnV[i*kproj] and oriented like it; fewer than 3 neighbours keep
+ * that vertex normal.  The engine's frame_mode CVT_FRAME_PCA. */
+cvt_status_t cvt_frames_pca(const float* S, int n, const uint32_t* knn, int K, const float* N0, const int* knnV,
+                            int kproj, float* U, float* V, void* stream);
 
 /* Replaces centroids_tangent_voronoi (2dClip.cuh:82-135): clip [-R,R]^2 by the
  * bisectors of the K listed neighbours (list order), area centroid mapped back
@@ -215,6 +226,16 @@ cvt_status_t cvt_mesh_get_bvh(cvt_mesh_t m, void* nodes, int nodes_cap, int* tri
  * max of the two sides; a_to_b / b_to_a (may be NULL) are the one-sided
  * distances.  Synchronous. */
 cvt_status_t cvt_hausdorff_meshes(cvt_mesh_t a, cvt_mesh_t b, float* out, float* a_to_b, float* b_to_a, void* stream);
+/* Option beside project_centroids_to_mesh (near_project.cuh:149-189): the
+ * exact closest point on the whole mesh to each of the n centroids (device
+ * arrays, n*3 floats), through the mesh's BVH (built on first use): the
+ * face with the smallest squared distance, first met in the BVH's near-first
+ * order on ties.  Sold (the sites before the step; may be NULL except in
+ * MIXED) bounds the search; in MIXED a non-finite centroid keeps its old
+ * site.  profile REF or MIXED (FP64 barycentrics).  The engine's proj_mode
+ * CVT_PROJ_BVH.  Synchronous (checks the traversal stack). */
+cvt_status_t cvt_project_bvh(cvt_mesh_t m, const float* cent, int n, int profile, const float* Sold, float* Snew,
+                             void* stream);
 /* n area-uniform points on the mesh (device out, n*3 floats): a face drawn by
  * area, then the square-root barycentric map, three uniforms per point from
  * a counter hash of (seed, i).  New (the reference starts from the vertices,
@@ -238,7 +259,24 @@ typedef struct {
    * knn_block 64|128|256 (one warp per site), clip_block 64|128 (FP64
    * profile: 32|64), proj_block 64|128|256; 0 = default. */
   int knn_block, clip_block, proj_block;
+  /* options beyond the reference (defaults reproduce it):
+   * proj_mode  CVT_PROJ_ONERING (0): the closest point over the one-rings of
+   *            the kproj nearest vertices (near_project.cuh:149-189);
+   *            CVT_PROJ_BVH (1): the exact closest point on the whole mesh
+   *            through its BVH (built when the first segment is placed).
+   *            Frozen sites then keep the frame vertex of the last iteration
+   *            they were active (no vertex list is kept).
+   * frame_mode CVT_FRAME_VERTEX_NORMAL (0): the frame from the normal of the
+   *            site's nearest vertex (site_normals.cuh:69-110);
+   *            CVT_FRAME_PCA (1): from the PCA normal of the site's K
+   *            neighbours (the smallest-eigenvalue eigenvector of their
+   *            covariance, oriented like the vertex normal). */
+  int proj_mode, frame_mode;
 } cvt_params_t;
+#define CVT_PROJ_ONERING 0
+#define CVT_PROJ_BVH 1
+#define CVT_FRAME_VERTEX_NORMAL 0
+#define CVT_FRAME_PCA 1
 
 void cvt_params_default(cvt_params_t* p);
 /* Launch-shape autotuner: times every candidate block size of the site KNN,
@@ -333,6 +371,16 @@ cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n);
  * NULL) receives {same, low, both, newly frozen} per iteration. */
 cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF, const float* sites_in, int n_sites,
                         const cvt_params_t* p, int iters, float* sites_out, int* counts);
+/* Many meshes in one call, HOST buffers (the main.cu driver run once per
+ * mesh, main.cu:369-1073, replaced by one batched run): mesh i is V[i]
+ * (nV[i]*3 floats), F[i] (nF[i]*3 ints) with sites_in[i] (n_sites[i]*3
+ * floats); every mesh is a segment of one engine, so each Lloyd iteration
+ * of all meshes is one pass of the iteration's kernels.  sites_out[i]
+ * receives mesh i's sites after `iters` iterations -- the same values
+ * cvt_remesh returns for that mesh alone.  Synchronous. */
+cvt_status_t cvt_remesh_batch(int n_meshes, const float* const* V, const int* nV, const int* const* F, const int* nF,
+                              const float* const* sites_in, const int* n_sites, const cvt_params_t* p, int iters,
+                              float* const* sites_out);
 
 #ifdef __cplusplus
 }

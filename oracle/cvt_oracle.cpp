@@ -748,172 +748,9 @@ void oracle_tiers(int mode, int n, int K, const float* site_normal, const uint32
 }  // extern "C"
 
 // ===========================================================================
-// Lloyd loop (main.cu:640-881), generalised to nSites != nV
+// BVH (evaluate.cuh:106-201), used by the Hausdorff evaluation and by the
+// BVH projection option
 // ===========================================================================
-namespace {
-
-struct RunParams {
-  int K;          // neighbours after dropping self (K_NEIGH)
-  int mode;       // 0 freezing off, 1 five tiers, 2 six tiers
-  int profile;    // P_REF / P_MIXED / P_FP64
-  int iters;
-  int kproj;      // nearest mesh vertices for the projection one-rings (5)
-  int ex_quirk;   // mode 0: skip vertex index == site index in centroid->mesh KNN
-  float R;        // clip square half size (input mesh max bbox edge)
-};
-
-const int kStreak1[6] = {5, 10, 15, 20, 25, 25};
-const int kStreak2[6] = {5, 10, 15, 20, 25, 10};
-
-template <class T>
-void lloyd_run(const float* V, int nV, const int* F, int nF, const float* N, T* S, int n,
-               const RunParams& p, int* counts, double* maxdisp, unsigned char* frozen_out,
-               unsigned char* tier_out, uint32_t* knn_out, int* knnv_out, float* cent_out) {
-  const int K = p.K, KK = p.K + 1, KP = p.kproj;
-  std::vector<int> off(nV + 1), fcs(3 * (size_t)nF);
-  oracle_build_vf(nV, nF, F, off.data(), fcs.data());
-  PGrid<float> vg;
-  vg.build(V, nV, 4.0);
-  std::vector<uint32_t> raw((size_t)n * KK), knn((size_t)n * K, 0u), prev((size_t)n * K, 0u);
-  std::vector<int> knnv((size_t)n * KP, -1);
-  std::vector<unsigned char> frozen(n, 0), streak(n, 0), cand(n, 0), tier(n, 0);
-  std::vector<T> Snew((size_t)3 * n);
-  float thr2 = ((0.01f * p.R) * 0.01f) * p.R;
-  float thr2_tier[6];
-  int need[6];
-  for (int t = 0; t < 6; ++t) {
-    thr2_tier[t] = thr2;
-    int s = p.mode == 0 ? 5 : (p.mode == 1 ? kStreak1[t] : kStreak2[t]);
-    need[t] = std::max(1, s - 1);
-  }
-  auto site_knn = [&](const unsigned char* fr) {
-    PGrid<T> g;
-    g.build(S, n, 2.0 * KK);
-#pragma omp parallel for schedule(dynamic, 256)
-    for (int i = 0; i < n; ++i) {
-      if (fr && fr[i]) continue;
-      TopK<T> top(KK);
-      g.knn(S + 3 * (size_t)i, top, [](uint32_t) { return true; });
-      uint32_t* r = raw.data() + (size_t)i * KK;
-      for (int t = 0; t < KK; ++t) r[t] = t < top.n ? top.c[t].i : 0xFFFFFFFFu;
-      // drop self (site_knn.cuh:79-103)
-      uint32_t* d = knn.data() + (size_t)i * K;
-      int w = 0;
-      for (int t = 0; t < KK && w < K; ++t) {
-        if ((int)r[t] == i) continue;
-        d[w++] = r[t];
-      }
-      if (w == 0) for (int k = 0; k < K; ++k) d[k] = (uint32_t)i;
-      else { uint32_t fill = d[w - 1]; for (; w < K; ++w) d[w] = fill; }
-    }
-  };
-  auto nearest_vertex = [&](V3<T> q) { int o; vertex_knn<T>(&vg, V, nV, q, 1, -1, &o); return o; };
-
-  if (p.mode != 0) {
-    // tier pre-pass (main.cu:640-667): KNN of the initial sites, site normal =
-    // normal of the site's nearest mesh vertex (= vertex i when sites are the
-    // vertices, as in the reference).
-    site_knn(nullptr);
-    std::vector<float> sn((size_t)3 * n);
-    for (int i = 0; i < n; ++i) {
-      int v = nearest_vertex(ld3(S, i));
-      V3<float> nn = v >= 0 ? ld3(N, v) : V3<float>{0, 0, 0};
-      st3(sn.data(), i, nn);
-    }
-    oracle_tiers(p.mode, n, K, sn.data(), knn.data(), tier.data(), nullptr, nullptr);
-  }
-
-  for (int it = 0; it < p.iters; ++it) {
-    site_knn(frozen.data());
-    for (int i = 0; i < n; ++i)
-      if (frozen[i]) std::memcpy(&knn[(size_t)i * K], &prev[(size_t)i * K], sizeof(uint32_t) * K);
-    const int skip_mode0 = (p.mode == 0 && p.ex_quirk);
-#pragma omp parallel for schedule(dynamic, 64)
-    for (int i = 0; i < n; ++i) {
-      V3<T> si = ld3(S, i);
-      int nn = frozen[i] ? knnv[(size_t)i * KP] : nearest_vertex(si);
-      Frame<T> fr;
-      if (nn < 0) fr = {{1, 0, 0}, {0, 1, 0}};
-      else fr = frame_from_normal(cvt3<T>(ld3(N, nn)));
-      V3<T> c = cell_centroid<T>(S, n, i, &knn[(size_t)i * K], K, fr, (T)p.R, p.profile, nullptr);
-      if (cent_out) st3(cent_out, i, cvt3<float>(c));
-      if (!frozen[i]) vertex_knn<T>(&vg, V, nV, c, KP, skip_mode0 ? i : -1, &knnv[(size_t)i * KP]);
-      bool finite = std::isfinite((double)c.x) && std::isfinite((double)c.y) && std::isfinite((double)c.z);
-      V3<T> sn = (p.profile != P_REF && !finite)
-                     ? si
-                     : project_point<T>(c, V, nV, F, nF, off.data(), fcs.data(), &knnv[(size_t)i * KP], KP,
-                                        p.profile == P_MIXED ? P_MIXED : P_REF);
-      st3(Snew.data(), i, sn);
-    }
-    int cnt[4] = {0, 0, 0, 0};
-    double md = 0.0;
-    for (int i = 0; i < n; ++i) {
-      double dd = (double)dist2(ld3(Snew.data(), i), ld3(S, i));
-      if (dd > md) md = dd;
-    }
-    if (it == 0) {
-      for (int i = 0; i < n; ++i) { streak[i] = 0; cand[i] = 0; }
-    } else {
-      for (int i = 0; i < n; ++i) {
-        int t = std::min<int>(tier[i], 5);
-        bool same = std::memcmp(&knn[(size_t)i * K], &prev[(size_t)i * K], sizeof(uint32_t) * K) == 0;
-        T d2 = dist2(ld3(Snew.data(), i), ld3(S, i));
-        bool low = d2 <= (T)thr2_tier[t];
-        bool both = same && low;
-        cnt[0] += same; cnt[1] += low; cnt[2] += both;
-        unsigned char s = streak[i];
-        s = both ? (unsigned char)(s < 255 ? s + 1 : s) : 0;
-        streak[i] = s;
-        cand[i] = (s >= need[t]) ? 1 : 0;
-      }
-      for (int i = 0; i < n; ++i)
-        if (cand[i] && !frozen[i]) { frozen[i] = 1; cnt[3]++; }
-    }
-    if (p.mode == 0) {
-      std::fill(frozen.begin(), frozen.end(), 0);
-      std::fill(streak.begin(), streak.end(), 0);
-    }
-    if (counts) for (int a = 0; a < 4; ++a) counts[4 * it + a] = cnt[a];
-    if (maxdisp) maxdisp[it] = std::sqrt(md);
-    prev = knn;
-    std::memcpy(S, Snew.data(), sizeof(T) * 3 * (size_t)n);
-  }
-  if (frozen_out) std::memcpy(frozen_out, frozen.data(), n);
-  if (tier_out) std::memcpy(tier_out, tier.data(), n);
-  if (knn_out) std::memcpy(knn_out, knn.data(), sizeof(uint32_t) * (size_t)n * K);
-  if (knnv_out) std::memcpy(knnv_out, knnv.data(), sizeof(int) * (size_t)n * KP);
-}
-
-}  // namespace
-
-extern "C" {
-
-// One full remesh run.  S (n*3) is updated in place.  counts: iters*4 ints
-// {same, low, both, newly}; maxdisp: iters doubles (max site motion).  The
-// optional outputs give the final frozen mask, tiers, site KNN (n*K) and
-// vertex KNN (n*kproj).  cent_out (n*3 floats) receives the centroids of the
-// last iteration.  profile 0/1: float state.
-void oracle_lloyd_run(const float* V, int nV, const int* F, int nF, const float* N, float* S, int n, int K,
-                      int mode, int profile, int iters, int kproj, int ex_quirk, float R, int* counts,
-                      double* maxdisp, unsigned char* frozen_out, unsigned char* tier_out, uint32_t* knn_out,
-                      int* knnv_out, float* cent_out) {
-  RunParams p{K, mode, profile == P_FP64 ? P_REF : profile, iters, kproj, ex_quirk, R};
-  lloyd_run<float>(V, nV, F, nF, N, S, n, p, counts, maxdisp, frozen_out, tier_out, knn_out, knnv_out, cent_out);
-}
-
-// The FP64 oracle: the same loop with double state and arithmetic.
-void oracle_lloyd_run_f64(const float* V, int nV, const int* F, int nF, const float* N, double* S, int n, int K,
-                          int mode, int iters, int kproj, int ex_quirk, float R, int* counts, double* maxdisp,
-                          unsigned char* frozen_out, unsigned char* tier_out, uint32_t* knn_out, int* knnv_out) {
-  RunParams p{K, mode, P_REF, iters, kproj, ex_quirk, R};
-  lloyd_run<double>(V, nV, F, nF, N, S, n, p, counts, maxdisp, frozen_out, tier_out, knn_out, knnv_out, nullptr);
-}
-
-// ===========================================================================
-// evaluation: BVH (evaluate.cuh:106-201), Hausdorff (evaluate.cuh:203-383),
-// quality (evaluate.cuh:388-462)
-// ===========================================================================
-
 // point->AABB squared distance (evaluate.cuh:44-51)
 static inline float aabb_d2(V3<float> p, const float* bmin, const float* bmax) {
   float d = 0.f;
@@ -923,47 +760,6 @@ static inline float aabb_d2(V3<float> p, const float* bmin, const float* bmax) {
     else if (q[a] > bmax[a]) { float t = q[a] - bmax[a]; d = std::fma(t, t, d); }
   }
   return d;
-}
-
-// point->triangle squared distance (evaluate.cuh:54-104)
-float oracle_point_tri_d2(const float* P, const float* A, const float* B, const float* C) {
-  V3<float> p = ld3(P, 0), a = ld3(A, 0), b = ld3(B, 0), c = ld3(C, 0);
-  V3<float> ab = sub3(b, a), ac = sub3(c, a), ap = sub3(p, a);
-  float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
-  if (d1 <= 0.f && d2 <= 0.f) return dot3(ap, ap);
-  V3<float> bp = sub3(p, b);
-  float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
-  if (d3 >= 0.f && d4 <= d3) return dot3(bp, bp);
-  float vc = std::fma(d1, d4, -(d3 * d2));
-  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
-    float v = d1 / (d1 - d3);
-    V3<float> pr{std::fma(ab.x, v, a.x), std::fma(ab.y, v, a.y), std::fma(ab.z, v, a.z)};
-    V3<float> d = sub3(p, pr);
-    return dot3(d, d);
-  }
-  V3<float> cp = sub3(p, c);
-  float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
-  if (d6 >= 0.f && d5 <= d6) return dot3(cp, cp);
-  float vb = std::fma(d5, d2, -(d1 * d6));
-  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
-    float w = d2 / (d2 - d6);
-    V3<float> pr{std::fma(ac.x, w, a.x), std::fma(ac.y, w, a.y), std::fma(ac.z, w, a.z)};
-    V3<float> d = sub3(p, pr);
-    return dot3(d, d);
-  }
-  float va = std::fma(d3, d6, -(d5 * d4));
-  if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
-    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-    V3<float> bc = sub3(c, b);
-    V3<float> pr{std::fma(bc.x, w, b.x), std::fma(bc.y, w, b.y), std::fma(bc.z, w, b.z)};
-    V3<float> d = sub3(p, pr);
-    return dot3(d, d);
-  }
-  float denom = 1.f / ((va + vb) + vc);
-  float v = vb * denom, w = vc * denom;
-  V3<float> pr{a.x + std::fma(ab.x, v, ac.x * w), a.y + std::fma(ab.y, v, ac.y * w), a.z + std::fma(ab.z, v, ac.z * w)};
-  V3<float> d = sub3(p, pr);
-  return dot3(d, d);
 }
 
 // BVH node layout as in evaluate.cuh:15-22 (40 bytes)
@@ -1022,6 +818,379 @@ static void obvh_build(const float* V, const int* F, int nF, int leaf, std::vect
   std::vector<int> tids(nF);
   for (int i = 0; i < nF; ++i) tids[i] = i;
   if (nF > 0) obvh_rec(nodes, tri, info, tids, leaf);
+}
+
+// ===========================================================================
+// options beyond the reference: PCA frames and the BVH projection.  Each
+// restates the device routine of the same name in gpu_cvt_b200/csrc/
+// cvt_math.cuh operation for operation, so the results agree bit for bit.
+// ===========================================================================
+namespace {
+
+constexpr int kPcaSteps = 8;
+
+// normal of the neighbourhood: eigenvector of the smallest eigenvalue of the
+// covariance of the listed neighbours' offsets, by power iteration on the
+// adjugate of C from n0, oriented like n0; n0 itself when fewer than 3
+// neighbours, zero spread or a non-finite result
+template <class T>
+V3<T> pca_normal(const T* S, long ns, const uint32_t* row, int K, V3<T> si, V3<T> n0) {
+  T sx = 0, sy = 0, sz = 0, xx = 0, xy = 0, xz = 0, yy = 0, yz = 0, zz = 0;
+  int m = 0;
+  for (int t = 0; t < K; ++t) {
+    const uint32_t j = row[t];
+    if (j >= (uint32_t)ns) continue;
+    const V3<T> d = sub3(ld3(S, (long)j), si);
+    sx = sx + d.x; sy = sy + d.y; sz = sz + d.z;
+    xx = fmaT(d.x, d.x, xx); xy = fmaT(d.x, d.y, xy); xz = fmaT(d.x, d.z, xz);
+    yy = fmaT(d.y, d.y, yy); yz = fmaT(d.y, d.z, yz); zz = fmaT(d.z, d.z, zz);
+    ++m;
+  }
+  if (m < 3) return n0;
+  const T im = (T)1 / (T)m;
+  const T mx = sx * im, my = sy * im, mz = sz * im;
+  const T cxx = fmaT(-sx, mx, xx), cxy = fmaT(-sx, my, xy), cxz = fmaT(-sx, mz, xz);
+  const T cyy = fmaT(-sy, my, yy), cyz = fmaT(-sy, mz, yz), czz = fmaT(-sz, mz, zz);
+  const T tr = (cxx + cyy) + czz;
+  if (!(tr > (T)1e-30)) return n0;
+  // adjugate of C: eigenvalues l2 l3, l1 l3, l1 l2 for C's l1 <= l2 <= l3,
+  // so the normal's (l1) direction dominates by the factor l2 / l1
+  const T axx = fmaT(cyy, czz, -(cyz * cyz)), axy = fmaT(cxz, cyz, -(cxy * czz)), axz = fmaT(cxy, cyz, -(cxz * cyy));
+  const T ayy = fmaT(cxx, czz, -(cxz * cxz)), ayz = fmaT(cxy, cxz, -(cxx * cyz)), azz = fmaT(cxx, cyy, -(cxy * cxy));
+  V3<T> v = n0;
+  for (int it = 0; it < kPcaSteps; ++it) {
+    const V3<T> w{fmaT(axz, v.z, fmaT(axy, v.y, axx * v.x)), fmaT(ayz, v.z, fmaT(ayy, v.y, axy * v.x)),
+                  fmaT(azz, v.z, fmaT(ayz, v.y, axz * v.x))};
+    const T nw = std::sqrt(dot3(w, w));
+    if (!(nw > (T)1e-30)) return n0;
+    const T inv = (T)1 / nw;
+    v = {w.x * inv, w.y * inv, w.z * inv};
+  }
+  if (!(std::isfinite((double)v.x) && std::isfinite((double)v.y) && std::isfinite((double)v.z))) return n0;
+  if (dot3(v, n0) < (T)0) v = {-v.x, -v.y, -v.z};
+  return v;
+}
+
+// (|c - s| (1 + 1e-4) + 1e-5 max|s|)^2 in double: an upper bound of the
+// squared distance from c to the mesh when s lies on it
+template <class T> double bvh_bound2(V3<T> c, V3<T> s) {
+  const double dx = (double)c.x - (double)s.x, dy = (double)c.y - (double)s.y, dz = (double)c.z - (double)s.z;
+  const double m = std::fmax(std::fmax(std::fabs((double)s.x), std::fabs((double)s.y)), std::fabs((double)s.z));
+  const double d = std::sqrt(std::fma(dz, dz, std::fma(dy, dy, dx * dx))) * 1.0001 + 1e-5 * m;
+  return std::isfinite(d) ? d * d : 1e30;
+}
+
+// closest point on the mesh through the BVH: near-first traversal, boxes
+// entered while their FP32 squared distance is below the best so far, strict
+// '<' per face (first face in traversal order wins ties); best starts at
+// bound2 and the search reruns unbounded if nothing beats it
+template <class T, class Q>
+V3<T> project_bvh(V3<T> c, const std::vector<OBVHNode>& nodes, const std::vector<int>& tri, const float* V,
+                  const int* F, Q bound2) {
+  if (!(std::isfinite((double)c.x) && std::isfinite((double)c.y) && std::isfinite((double)c.z))) return c;
+  const V3<Q> cq = cvt3<Q>(c);
+  const V3<float> cf = cvt3<float>(c);
+  V3<Q> bp = cq;
+  if (nodes.empty()) return c;
+  std::vector<int> stack;
+  for (int pass = 0; pass < 2; ++pass) {
+    Q best = pass == 0 ? bound2 : (Q)1e30;
+    bool found = false;
+    stack.clear();
+    stack.push_back(0);
+    while (!stack.empty()) {
+      const OBVHNode nd = nodes[stack.back()];
+      stack.pop_back();
+      if ((Q)aabb_d2(cf, nd.bmin, nd.bmax) >= best) continue;
+      if (nd.triCount > 0) {
+        for (int k = 0; k < nd.triCount; ++k) {
+          const int t = tri[nd.triStart + k];
+          const V3<Q> A = cvt3<Q>(ld3(V, F[3 * t])), B = cvt3<Q>(ld3(V, F[3 * t + 1])), C = cvt3<Q>(ld3(V, F[3 * t + 2]));
+          const V3<Q> p = closest_point_tri(cq, A, B, C);
+          const V3<Q> dd = sub3(p, cq);
+          const Q d2 = dot3(dd, dd);
+          if (d2 < best) { best = d2; bp = p; found = true; }
+        }
+      } else {
+        const OBVHNode& L = nodes[nd.left];
+        const OBVHNode& R = nodes[nd.right];
+        const Q dl = (Q)aabb_d2(cf, L.bmin, L.bmax), dr = (Q)aabb_d2(cf, R.bmin, R.bmax);
+        if (dl < dr) {
+          if (dr < best) stack.push_back(nd.right);
+          if (dl < best) stack.push_back(nd.left);
+        } else {
+          if (dl < best) stack.push_back(nd.left);
+          if (dr < best) stack.push_back(nd.right);
+        }
+      }
+    }
+    if (found) break;
+  }
+  return cvt3<T>(bp);
+}
+
+}  // namespace
+
+// ===========================================================================
+// Lloyd loop (main.cu:640-881), generalised to nSites != nV
+// ===========================================================================
+namespace {
+
+struct RunParams {
+  int K;          // neighbours after dropping self (K_NEIGH)
+  int mode;       // 0 freezing off, 1 five tiers, 2 six tiers
+  int profile;    // P_REF / P_MIXED / P_FP64
+  int iters;
+  int kproj;      // nearest mesh vertices for the projection one-rings (5)
+  int ex_quirk;   // mode 0: skip vertex index == site index in centroid->mesh KNN
+  float R;        // clip square half size (input mesh max bbox edge)
+  int proj_mode;  // 0: one-ring of the kproj nearest vertices; 1: closest point through the BVH
+  int frame_mode; // 0: nearest vertex normal; 1: PCA normal of the neighbour list
+};
+
+const int kStreak1[6] = {5, 10, 15, 20, 25, 25};
+const int kStreak2[6] = {5, 10, 15, 20, 25, 10};
+
+template <class T>
+void lloyd_run(const float* V, int nV, const int* F, int nF, const float* N, T* S, int n,
+               const RunParams& p, int* counts, double* maxdisp, unsigned char* frozen_out,
+               unsigned char* tier_out, uint32_t* knn_out, int* knnv_out, float* cent_out) {
+  const int K = p.K, KK = p.K + 1, KP = p.kproj;
+  std::vector<int> off(nV + 1), fcs(3 * (size_t)nF);
+  oracle_build_vf(nV, nF, F, off.data(), fcs.data());
+  PGrid<float> vg;
+  vg.build(V, nV, 4.0);
+  std::vector<uint32_t> raw((size_t)n * KK), knn((size_t)n * K, 0u), prev((size_t)n * K, 0u);
+  std::vector<int> knnv((size_t)n * KP, -1);
+  std::vector<int> nnv(n, -1);  // frame vertex of each site's last active iteration
+  std::vector<OBVHNode> bvh_nodes;
+  std::vector<int> bvh_tri;
+  if (p.proj_mode == 1) obvh_build(V, F, nF, 8, bvh_nodes, bvh_tri);
+  std::vector<unsigned char> frozen(n, 0), streak(n, 0), cand(n, 0), tier(n, 0);
+  std::vector<T> Snew((size_t)3 * n);
+  float thr2 = ((0.01f * p.R) * 0.01f) * p.R;
+  float thr2_tier[6];
+  int need[6];
+  for (int t = 0; t < 6; ++t) {
+    thr2_tier[t] = thr2;
+    int s = p.mode == 0 ? 5 : (p.mode == 1 ? kStreak1[t] : kStreak2[t]);
+    need[t] = std::max(1, s - 1);
+  }
+  auto site_knn = [&](const unsigned char* fr) {
+    PGrid<T> g;
+    g.build(S, n, 2.0 * KK);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int i = 0; i < n; ++i) {
+      if (fr && fr[i]) continue;
+      TopK<T> top(KK);
+      g.knn(S + 3 * (size_t)i, top, [](uint32_t) { return true; });
+      uint32_t* r = raw.data() + (size_t)i * KK;
+      for (int t = 0; t < KK; ++t) r[t] = t < top.n ? top.c[t].i : 0xFFFFFFFFu;
+      // drop self (site_knn.cuh:79-103)
+      uint32_t* d = knn.data() + (size_t)i * K;
+      int w = 0;
+      for (int t = 0; t < KK && w < K; ++t) {
+        if ((int)r[t] == i) continue;
+        d[w++] = r[t];
+      }
+      if (w == 0) for (int k = 0; k < K; ++k) d[k] = (uint32_t)i;
+      else { uint32_t fill = d[w - 1]; for (; w < K; ++w) d[w] = fill; }
+    }
+  };
+  auto nearest_vertex = [&](V3<T> q) { int o; vertex_knn<T>(&vg, V, nV, q, 1, -1, &o); return o; };
+
+  if (p.mode != 0) {
+    // tier pre-pass (main.cu:640-667): KNN of the initial sites, site normal =
+    // normal of the site's nearest mesh vertex (= vertex i when sites are the
+    // vertices, as in the reference).
+    site_knn(nullptr);
+    std::vector<float> sn((size_t)3 * n);
+    for (int i = 0; i < n; ++i) {
+      int v = nearest_vertex(ld3(S, i));
+      V3<float> nn = v >= 0 ? ld3(N, v) : V3<float>{0, 0, 0};
+      st3(sn.data(), i, nn);
+    }
+    oracle_tiers(p.mode, n, K, sn.data(), knn.data(), tier.data(), nullptr, nullptr);
+  }
+
+  for (int it = 0; it < p.iters; ++it) {
+    site_knn(frozen.data());
+    for (int i = 0; i < n; ++i)
+      if (frozen[i]) std::memcpy(&knn[(size_t)i * K], &prev[(size_t)i * K], sizeof(uint32_t) * K);
+    const int skip_mode0 = (p.mode == 0 && p.ex_quirk);
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int i = 0; i < n; ++i) {
+      V3<T> si = ld3(S, i);
+      if (!frozen[i]) nnv[i] = nearest_vertex(si);
+      // frozen sites: the first entry of their kept vertex list; with the BVH
+      // projection (no vertex list) their kept frame vertex
+      int nn = (frozen[i] && p.proj_mode == 0) ? knnv[(size_t)i * KP] : nnv[i];
+      Frame<T> fr;
+      if (nn < 0) {
+        fr = {{1, 0, 0}, {0, 1, 0}};
+      } else {
+        V3<T> n0 = cvt3<T>(ld3(N, nn));
+        if (p.frame_mode == 1) n0 = pca_normal<T>(S, n, &knn[(size_t)i * K], K, si, n0);
+        fr = frame_from_normal(n0);
+      }
+      V3<T> c = cell_centroid<T>(S, n, i, &knn[(size_t)i * K], K, fr, (T)p.R, p.profile, nullptr);
+      if (cent_out) st3(cent_out, i, cvt3<float>(c));
+      bool finite = std::isfinite((double)c.x) && std::isfinite((double)c.y) && std::isfinite((double)c.z);
+      V3<T> sn;
+      if (p.profile != P_REF && !finite) {
+        sn = si;
+      } else if (p.proj_mode == 1) {
+        if (p.profile == P_MIXED) sn = project_bvh<T, double>(c, bvh_nodes, bvh_tri, V, F, bvh_bound2(c, si));
+        else sn = project_bvh<T, T>(c, bvh_nodes, bvh_tri, V, F, (T)bvh_bound2(c, si));
+      } else {
+        if (!frozen[i]) vertex_knn<T>(&vg, V, nV, c, KP, skip_mode0 ? i : -1, &knnv[(size_t)i * KP]);
+        sn = project_point<T>(c, V, nV, F, nF, off.data(), fcs.data(), &knnv[(size_t)i * KP], KP,
+                              p.profile == P_MIXED ? P_MIXED : P_REF);
+      }
+      st3(Snew.data(), i, sn);
+    }
+    int cnt[4] = {0, 0, 0, 0};
+    double md = 0.0;
+    for (int i = 0; i < n; ++i) {
+      double dd = (double)dist2(ld3(Snew.data(), i), ld3(S, i));
+      if (dd > md) md = dd;
+    }
+    if (it == 0) {
+      for (int i = 0; i < n; ++i) { streak[i] = 0; cand[i] = 0; }
+    } else {
+      for (int i = 0; i < n; ++i) {
+        int t = std::min<int>(tier[i], 5);
+        bool same = std::memcmp(&knn[(size_t)i * K], &prev[(size_t)i * K], sizeof(uint32_t) * K) == 0;
+        T d2 = dist2(ld3(Snew.data(), i), ld3(S, i));
+        bool low = d2 <= (T)thr2_tier[t];
+        bool both = same && low;
+        cnt[0] += same; cnt[1] += low; cnt[2] += both;
+        unsigned char s = streak[i];
+        s = both ? (unsigned char)(s < 255 ? s + 1 : s) : 0;
+        streak[i] = s;
+        cand[i] = (s >= need[t]) ? 1 : 0;
+      }
+      for (int i = 0; i < n; ++i)
+        if (cand[i] && !frozen[i]) { frozen[i] = 1; cnt[3]++; }
+    }
+    if (p.mode == 0) {
+      std::fill(frozen.begin(), frozen.end(), 0);
+      std::fill(streak.begin(), streak.end(), 0);
+    }
+    if (counts) for (int a = 0; a < 4; ++a) counts[4 * it + a] = cnt[a];
+    if (maxdisp) maxdisp[it] = std::sqrt(md);
+    prev = knn;
+    std::memcpy(S, Snew.data(), sizeof(T) * 3 * (size_t)n);
+  }
+  if (frozen_out) std::memcpy(frozen_out, frozen.data(), n);
+  if (tier_out) std::memcpy(tier_out, tier.data(), n);
+  if (knn_out) std::memcpy(knn_out, knn.data(), sizeof(uint32_t) * (size_t)n * K);
+  if (knnv_out) std::memcpy(knnv_out, knnv.data(), sizeof(int) * (size_t)n * KP);
+}
+
+}  // namespace
+
+extern "C" {
+
+// One full remesh run.  S (n*3) is updated in place.  counts: iters*4 ints
+// {same, low, both, newly}; maxdisp: iters doubles (max site motion).  The
+// optional outputs give the final frozen mask, tiers, site KNN (n*K) and
+// vertex KNN (n*kproj).  cent_out (n*3 floats) receives the centroids of the
+// last iteration.  profile 0/1: float state.
+void oracle_lloyd_run(const float* V, int nV, const int* F, int nF, const float* N, float* S, int n, int K,
+                      int mode, int profile, int iters, int kproj, int ex_quirk, float R, int* counts,
+                      double* maxdisp, unsigned char* frozen_out, unsigned char* tier_out, uint32_t* knn_out,
+                      int* knnv_out, float* cent_out, int proj_mode, int frame_mode) {
+  RunParams p{K, mode, profile == P_FP64 ? P_REF : profile, iters, kproj, ex_quirk, R, proj_mode, frame_mode};
+  lloyd_run<float>(V, nV, F, nF, N, S, n, p, counts, maxdisp, frozen_out, tier_out, knn_out, knnv_out, cent_out);
+}
+
+// The FP64 oracle: the same loop with double state and arithmetic.
+void oracle_lloyd_run_f64(const float* V, int nV, const int* F, int nF, const float* N, double* S, int n, int K,
+                          int mode, int iters, int kproj, int ex_quirk, float R, int* counts, double* maxdisp,
+                          unsigned char* frozen_out, unsigned char* tier_out, uint32_t* knn_out, int* knnv_out,
+                          int proj_mode, int frame_mode) {
+  RunParams p{K, mode, P_REF, iters, kproj, ex_quirk, R, proj_mode, frame_mode};
+  lloyd_run<double>(V, nV, F, nF, N, S, n, p, counts, maxdisp, frozen_out, tier_out, knn_out, knnv_out, nullptr);
+}
+
+// frames from the PCA normal of each site's listed neighbours, started from
+// the normal of vertex nearest[i] (cvt_frames_pca)
+void oracle_pca_frames(const float* S, int n, const uint32_t* knn, int K, const float* N, const int* nearest,
+                       float* U, float* Vv) {
+  for (int i = 0; i < n; ++i) {
+    int nn = nearest[i];
+    if (nn < 0) { st3(U, i, V3<float>{1, 0, 0}); st3(Vv, i, V3<float>{0, 1, 0}); continue; }
+    V3<float> nrm = pca_normal<float>(S, n, knn + (size_t)i * K, K, ld3(S, i), ld3(N, nn));
+    Frame<float> fr = frame_from_normal(nrm);
+    st3(U, i, fr.u); st3(Vv, i, fr.v);
+  }
+}
+
+// closest point on the mesh through its BVH for every centroid
+// (cvt_project_bvh); Sold may be NULL except in MIXED
+void oracle_project_bvh(const float* cent, int n, const float* V, int nV, const int* F, int nF, int profile,
+                        const float* Sold, float* Snew) {
+  (void)nV;
+  std::vector<OBVHNode> nodes;
+  std::vector<int> tri;
+  obvh_build(V, F, nF, 8, nodes, tri);
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < n; ++i) {
+    V3<float> c = ld3(cent, i);
+    bool finite = std::isfinite(c.x) && std::isfinite(c.y) && std::isfinite(c.z);
+    if (profile == P_MIXED && !finite) { st3(Snew, i, ld3(Sold, i)); continue; }
+    double b2 = Sold ? bvh_bound2(c, ld3(Sold, i)) : 1e30;
+    V3<float> r = profile == P_MIXED ? project_bvh<float, double>(c, nodes, tri, V, F, b2)
+                                     : project_bvh<float, float>(c, nodes, tri, V, F, (float)b2);
+    st3(Snew, i, r);
+  }
+}
+
+// ===========================================================================
+// evaluation: BVH (evaluate.cuh:106-201), Hausdorff (evaluate.cuh:203-383),
+// quality (evaluate.cuh:388-462)
+// ===========================================================================
+
+// point->triangle squared distance (evaluate.cuh:54-104)
+float oracle_point_tri_d2(const float* P, const float* A, const float* B, const float* C) {
+  V3<float> p = ld3(P, 0), a = ld3(A, 0), b = ld3(B, 0), c = ld3(C, 0);
+  V3<float> ab = sub3(b, a), ac = sub3(c, a), ap = sub3(p, a);
+  float d1 = dot3(ab, ap), d2 = dot3(ac, ap);
+  if (d1 <= 0.f && d2 <= 0.f) return dot3(ap, ap);
+  V3<float> bp = sub3(p, b);
+  float d3 = dot3(ab, bp), d4 = dot3(ac, bp);
+  if (d3 >= 0.f && d4 <= d3) return dot3(bp, bp);
+  float vc = std::fma(d1, d4, -(d3 * d2));
+  if (vc <= 0.f && d1 >= 0.f && d3 <= 0.f) {
+    float v = d1 / (d1 - d3);
+    V3<float> pr{std::fma(ab.x, v, a.x), std::fma(ab.y, v, a.y), std::fma(ab.z, v, a.z)};
+    V3<float> d = sub3(p, pr);
+    return dot3(d, d);
+  }
+  V3<float> cp = sub3(p, c);
+  float d5 = dot3(ab, cp), d6 = dot3(ac, cp);
+  if (d6 >= 0.f && d5 <= d6) return dot3(cp, cp);
+  float vb = std::fma(d5, d2, -(d1 * d6));
+  if (vb <= 0.f && d2 >= 0.f && d6 <= 0.f) {
+    float w = d2 / (d2 - d6);
+    V3<float> pr{std::fma(ac.x, w, a.x), std::fma(ac.y, w, a.y), std::fma(ac.z, w, a.z)};
+    V3<float> d = sub3(p, pr);
+    return dot3(d, d);
+  }
+  float va = std::fma(d3, d6, -(d5 * d4));
+  if (va <= 0.f && (d4 - d3) >= 0.f && (d5 - d6) >= 0.f) {
+    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    V3<float> bc = sub3(c, b);
+    V3<float> pr{std::fma(bc.x, w, b.x), std::fma(bc.y, w, b.y), std::fma(bc.z, w, b.z)};
+    V3<float> d = sub3(p, pr);
+    return dot3(d, d);
+  }
+  float denom = 1.f / ((va + vb) + vc);
+  float v = vb * denom, w = vc * denom;
+  V3<float> pr{a.x + std::fma(ab.x, v, ac.x * w), a.y + std::fma(ab.y, v, ac.y * w), a.z + std::fma(ab.z, v, ac.z * w)};
+  V3<float> d = sub3(p, pr);
+  return dot3(d, d);
 }
 
 int oracle_bvh_node_count(const float* V, const int* F, int nF, int leaf) {

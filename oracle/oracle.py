@@ -60,9 +60,11 @@ def _declare(L):
         "oracle_freeze": ([vp, vp, i32, vp, vp, i32, i32, vp, vp, vp, vp, vp, vp, vp], None),
         "oracle_tiers": ([i32, i32, i32, vp, vp, vp, vp, vp], None),
         "oracle_lloyd_run": ([vp, i32, vp, i32, vp, vp, i32, i32, i32, i32, i32, i32, i32, f32,
-                              vp, vp, vp, vp, vp, vp, vp], None),
+                              vp, vp, vp, vp, vp, vp, vp, i32, i32], None),
         "oracle_lloyd_run_f64": ([vp, i32, vp, i32, vp, vp, i32, i32, i32, i32, i32, i32, f32,
-                                  vp, vp, vp, vp, vp, vp], None),
+                                  vp, vp, vp, vp, vp, vp, i32, i32], None),
+        "oracle_pca_frames": ([vp, i32, vp, i32, vp, vp, vp, vp], None),
+        "oracle_project_bvh": ([vp, i32, vp, i32, vp, i32, i32, vp, vp], None),
         "oracle_point_tri_d2": ([vp, vp, vp, vp], f32),
         "oracle_bvh_node_count": ([vp, vp, i32, i32], i32),
         "oracle_bvh_build": ([vp, vp, i32, i32, vp, vp], None),
@@ -199,8 +201,16 @@ def freeze(S, Snew, knn, prev, has_prev, tier, thr2_tier, need_tier, streak, fro
     return cand, counts
 
 
-def lloyd_run(V, F, S0, K, mode, iters, profile=P_REF, kproj=5, ex_quirk=True, R=None, N=None):
-    """Full remesh run; returns dict(S, counts, maxdisp, frozen, tier, knn, knnv, cent)."""
+PROJ = {"onering": 0, "bvh": 1}
+FRAME = {"vertex": 0, "pca": 1}
+
+
+def lloyd_run(V, F, S0, K, mode, iters, profile=P_REF, kproj=5, ex_quirk=True, R=None, N=None, proj="onering",
+              frame="vertex"):
+    """Full remesh run; returns dict(S, counts, maxdisp, frozen, tier, knn, knnv, cent).
+    proj "bvh" / frame "pca" select the engine's projection and frame options."""
+    pm = PROJ[proj] if isinstance(proj, str) else int(proj)
+    fm = FRAME[frame] if isinstance(frame, str) else int(frame)
     V, F = _f32(V), _i32(F)
     nV, nF = V.shape[0], F.shape[0]
     if N is None:
@@ -219,16 +229,35 @@ def lloyd_run(V, F, S0, K, mode, iters, profile=P_REF, kproj=5, ex_quirk=True, R
         S = np.ascontiguousarray(S0, dtype=np.float64).copy()
         lib().oracle_lloyd_run_f64(_p(V), nV, _p(F), nF, _p(_f32(N)), _p(S), n, K, mode, iters, kproj,
                                    int(ex_quirk), float(R), _p(counts), _p(maxdisp), _p(frozen), _p(tier),
-                                   _p(knn), _p(knnv))
+                                   _p(knn), _p(knnv), pm, fm)
         cent = None
     else:
         S = _f32(S0).copy()
         cent = np.zeros((n, 3), np.float32)
         lib().oracle_lloyd_run(_p(V), nV, _p(F), nF, _p(_f32(N)), _p(S), n, K, mode, profile, iters, kproj,
                                int(ex_quirk), float(R), _p(counts), _p(maxdisp), _p(frozen), _p(tier),
-                               _p(knn), _p(knnv), _p(cent))
+                               _p(knn), _p(knnv), _p(cent), pm, fm)
     return dict(S=S, counts=counts[:iters], maxdisp=maxdisp[:iters], frozen=frozen, tier=tier, knn=knn,
                 knnv=knnv, cent=cent)
+
+
+def pca_frames(S, knn, N, nearest):
+    """Frames from the PCA normal of each site's neighbours (cvt_frames_pca)."""
+    S, knn, N, nearest = _f32(S), _u32(knn), _f32(N), _i32(nearest)
+    n, K = knn.shape
+    U = np.zeros((n, 3), np.float32)
+    Vv = np.zeros((n, 3), np.float32)
+    lib().oracle_pca_frames(_p(S), n, _p(knn), K, _p(N), _p(nearest), _p(U), _p(Vv))
+    return U, Vv
+
+
+def project_bvh(cent, V, F, profile=P_REF, Sold=None):
+    """Closest point on the mesh through its BVH (cvt_project_bvh)."""
+    cent, V, F = _f32(cent), _f32(V), _i32(F)
+    Snew = np.zeros_like(cent)
+    lib().oracle_project_bvh(_p(cent), cent.shape[0], _p(V), V.shape[0], _p(F), F.shape[0], int(profile),
+                             _p(None if Sold is None else _f32(Sold)), _p(Snew))
+    return Snew
 
 
 def point_tri_d2(P, A, B, Cc) -> float:

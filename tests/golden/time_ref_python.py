@@ -92,4 +92,7 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("GPU_CVT_REF")
+    if not ref:
+        sys.exit(f"usage: {sys.argv[0]} <reference checkout>  (or set GPU_CVT_REF)")
+    main(ref)

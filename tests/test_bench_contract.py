@@ -1,19 +1,19 @@
 """bench.py's JSON contract where it runs without a GPU: the reference arm
 (the oracle port of the reference's CPU path, timed on the host cores) on a
-bounded sample, and the issue-roofline arithmetic."""
+bounded sample of the batched workload, its configuration identical to the
+GPU arm's, and the issue-roofline arithmetic."""
 import json
 import os
 import subprocess
 import sys
 
-import pytest
-
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+sys.path.insert(0, ROOT)
 
 
 def test_reference_arm_prints_contract_line():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1",
-                        "--warmup", "0", "--ref-seconds", "1"],
+                        "--warmup", "0", "--ref-seconds", "1", "--meshes", "6"],
                        capture_output=True, text=True, timeout=600, cwd=ROOT)
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads(r.stdout.strip().splitlines()[-1])
@@ -21,50 +21,58 @@ def test_reference_arm_prints_contract_line():
     assert line["metric"].startswith("sites")
     assert line["unit"] == "sites*iters/s" and line["higher_is_better"] is True
     assert line["value"] > 0 and line["steps"] == 1 and line["n_gpus"] == 1
-    assert line["config"]["workload"] == "torus_100k" and line["config"]["sites"] == 100_000
+    cfg = line["config"]
+    assert cfg["workload"] == "batched_6_meshes" and cfg["meshes"] == 6 and cfg["iters"] == 100 and cfg["k"] == 24
     cb = line["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"] and cb["sample"]
+    assert "whole remeshes" in cb["sample"]
     e2e = line["e2e"]
     assert e2e["value"] == line["value"] and e2e["unit"] == line["unit"]
     assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
 
 
+def test_both_arms_share_one_config():
+    """The GPU arm and the reference arm build their config dicts with the
+    same function, so the dicts are identical for the same flags."""
+    import bench
+    _, a, _ = bench.batched_workload(4, 1)
+    _, b, _ = bench.batched_workload(4, 1)
+    assert a == b and a["parallelism"] == "single GPU"
+    assert "tiles" not in a                       # run-dependent values stay outside config
+    _, c, _ = bench.batched_workload(4, 2)
+    assert c["parallelism"] != a["parallelism"]
+
+
 def test_issue_roofline_arithmetic():
-    sys.path.insert(0, ROOT)
     import bench
     with open(os.path.join(ROOT, "profiles", "instructions.json")) as fh:
-        counts = json.load(fh)["warp_instructions_per_remesh"]
+        rec = json.load(fh)["workloads"]["torus_100k"]
+    counts = rec["warp_instructions_per_remesh"]
     prof = {"grid": 0.03, "knn": 0.08, "clip": 0.06, "proj": 0.1}
-    out = bench.issue_roofline(prof, 100, 1965.0, sms=148)
+    out = bench.issue_roofline("torus_100k", prof, 100, 1965.0, sms=148)
     assert out["bound"] == "issue" and out["peak"] == 148 * 4 * 1965e6
+    assert "recorded" in out["counts"]
     for kernel, group in (("k_site_knn", "knn"), ("k_site_clip", "clip"), ("k_site_proj", "proj")):
         k = out["kernels"][kernel]
         assert abs(k["achieved"] - counts[kernel] / (prof[group] * 1e-3 * 100)) < 1e-6 * k["achieved"]
         assert abs(k["frac"] - k["achieved"] / out["peak"]) < 1e-12
         assert 0.0 < k["frac"] < 1.0
-    assert bench.issue_roofline(prof, 100, None, sms=148) is None
+    assert bench.issue_roofline("torus_100k", prof, 100, None, sms=148) is None
+    assert bench.issue_roofline("no_such_workload", prof, 100, 1965.0, sms=148) is None
 
 
-@pytest.mark.gpu
-def test_main_arm_prints_contract_line():
-    """One short run of the benchmark's own arm on the GPU: every key the
-    JSON contract asks for, with consistent values."""
-    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--steps", "1", "--warmup", "3", "--no-cpu",
-                        "--no-accuracy"], capture_output=True, text=True, timeout=900, cwd=ROOT)
-    assert r.returncode == 0, r.stderr[-2000:]
-    line = json.loads(r.stdout.strip().splitlines()[-1])
-    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
-                "scaling", "vs_baseline", "dtype", "data", "config", "e2e", "gpu_launches", "roofline",
-                "issue_roofline", "cpu_baseline", "clocks"):
-        assert key in line, key
-    assert line["n_gpus"] == 1 and line["steps"] == 1 and line["warmup"] == 3 and line["scaling"] == "weak"
-    n, iters = line["config"]["sites"], line["config"]["iters"]
-    assert abs(line["value"] - n * iters / (line["ms_per_step"] / 1e3)) < 1e-6 * line["value"]
-    assert line["gpu_launches"] >= 10 * iters
-    e2e = line["e2e"]
-    assert e2e["value"] > 0 and e2e["h2d_bytes_per_step"] > 0 and e2e["d2h_bytes_per_step"] > 0
-    assert e2e["same_sites_as_engine"] is True
-    rf = line["roofline"]
-    assert rf["bound"] == "hbm" and rf["unit"] == "GB/s" and abs(rf["frac"] - rf["achieved"] / rf["peak"]) < 1e-9
-    assert set(line["issue_roofline"]["kernels"]) == {"k_site_knn", "k_site_clip", "k_site_proj"}
-    assert set(line["config"]["tiles"]) == {"knn_block", "clip_block", "proj_block"}
+def test_clock_fallback_without_samples(monkeypatch):
+    """A timed region shorter than the sampling period still reports a clock
+    (one-shot queries around it), never None when any source answers."""
+    import bench
+    c = bench.Clocks(0)
+    c.before = (1965.0, 1965.0)
+    monkeypatch.setattr(bench, "_smi_once", lambda gpu: (1950.0, 1965.0))
+    out = c.stop()
+    assert out["samples"] == 0 and out["sm_mhz"] == (1965.0 + 1950.0) / 2 and out["sm_max_mhz"] == 1965.0
+    assert "one-shot" in out["source"]
+    c2 = bench.Clocks(0)
+    monkeypatch.setattr(bench, "_smi_once", lambda gpu: None)
+    monkeypatch.setattr(bench, "_nvml_max_clock", lambda gpu: 1965.0)
+    out2 = c2.stop()
+    assert out2["sm_mhz"] is None and out2["sm_max_mhz"] == 1965.0 and "NVML" in out2["source"]

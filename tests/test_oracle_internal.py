@@ -218,3 +218,45 @@ def test_face_skip_bound_is_sound(oracle):
             checked += 1
     assert checked > 5000
     assert worst >= 1.0, f"bound above the computed distance: d2 / lb^2 = {worst}"
+
+
+def test_bvh_projection_is_the_closest_point(oracle):
+    """The oracle's BVH projection finds the closest point on the whole mesh:
+    its distance equals a scan of every face."""
+    from gpu_cvt_b200 import meshgen as mg
+    m = mg.superellipsoid(8.0, 4_000, 0.01, 1e-3, seed=2)
+    rng = np.random.default_rng(1)
+    P = (m.V[rng.integers(0, m.nV, 150)] + rng.normal(0, 0.05, (150, 3))).astype(np.float32)
+    for prof in (oracle.P_REF, oracle.P_MIXED):
+        Q = oracle.project_bvh(P, m.V, m.F, profile=prof)
+        d = np.linalg.norm(Q.astype(np.float64) - P, axis=1)
+        A, B, Cc = m.V[m.F[:, 0]], m.V[m.F[:, 1]], m.V[m.F[:, 2]]
+        for i in range(0, 150, 5):
+            dmin = np.sqrt(min(oracle.point_tri_d2(P[i], A[f], B[f], Cc[f]) for f in range(m.nF)))
+            assert abs(d[i] - dmin) <= 1e-6 * (1 + dmin)
+
+
+def test_pca_frames_recover_plane_and_sphere_normals(oracle):
+    """On a plane the PCA normal is the plane's normal whatever the start
+    vertex normal; on a finely sampled sphere it is close to radial."""
+    from gpu_cvt_b200 import meshgen as mg
+    rng = np.random.default_rng(2)
+    P = np.c_[rng.random((500, 2)), np.zeros(500)].astype(np.float32)
+    tilt = np.array([[1, 0, 0], [0, 0.8, -0.6], [0, 0.6, 0.8]], np.float32)
+    P = P @ tilt.T
+    knn, _ = oracle.knn_points(P, 13, method="bf")
+    knn = oracle.drop_self(knn, 12)
+    N = np.tile(np.array([[0.3, 0.1, 0.95]], np.float32), (1, 1))
+    U, V = oracle.pca_frames(P, knn, N / np.linalg.norm(N), np.zeros(500, np.int32))
+    nrm = np.cross(U, V)
+    assert np.abs(np.abs(nrm @ tilt[:, 2]) - 1).max() < 1e-5
+    m = mg.icosphere(5)
+    S = mg.sample_sites(m.V, m.F, 4000, seed=3)
+    knn, _ = oracle.knn_points(S, 21, method="grid")
+    knn = oracle.drop_self(knn, 20)
+    N = oracle.vertex_normals(m.V, m.F)
+    near = oracle.knn_vertices(m.V, S, 1)[:, 0]
+    U, V = oracle.pca_frames(S, knn, N, near)
+    nrm = np.cross(U, V)
+    radial = S / np.linalg.norm(S, axis=1, keepdims=True)
+    assert np.median(np.abs((nrm * radial).sum(1))) > 0.9999

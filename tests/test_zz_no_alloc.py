@@ -50,6 +50,27 @@ def test_noalloc_knn_matches_allocating_knn_twice_in_a_row():
         assert np.array_equal(a_d, b_d)
 
 
+def test_noalloc_knn_allocates_no_device_memory():
+    """The point of the entry point: a warm call takes no device memory.  The
+    library's own pool is trimmed first, the outputs are allocated before the
+    measurement, and the device's free memory must not move across the call."""
+    from gpu_cvt_b200 import _lib, meshgen as mg
+    m = mg.icosphere(4)
+    P = torch.from_numpy(mg.sample_sites(m.V, m.F, 20_000, seed=5)).cuda()
+    _knn("cvt_knn_sites_noalloc", P, 16)            # warm: symbol address, module load
+    _lib.call("cvt_release_cached_memory")
+    knn = torch.zeros((P.shape[0], 16), dtype=torch.int32, device="cuda")
+    dist = torch.zeros((P.shape[0], 16), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.call("cvt_knn_sites_noalloc", C.c_void_p(P.data_ptr()), P.shape[0], 16, None, C.c_void_p(knn.data_ptr()),
+              C.c_void_p(dist.data_ptr()), st)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
 def test_noalloc_knn_rejects_oversized_input():
     from gpu_cvt_b200 import _lib
     n = 131072 + 1
