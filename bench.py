@@ -754,6 +754,8 @@ def run_serve(args):
     served = srv.run(reqs)
     srv.close()
     plain = server.serve_plain(srv.M, plain_reqs, prm=prm)
+    classes = server.size_classes(plain_reqs)
+    ceiling = server.batching_ceiling(plain_reqs, plain["makespan_s"])
     line = {"metric": METRIC, "value": served["sites_iters_per_s"], "unit": UNIT, "n_gpus": 1, "steps": 1,
             "warmup": 1, "ms_per_step": served["makespan_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -766,6 +768,7 @@ def run_serve(args):
                           "mean": served["latency_mean_s"]},
             "served": served, "plain_fifo": plain,
             "served_over_plain": served["sites_iters_per_s"] / plain["sites_iters_per_s"],
+            "plain_by_request_size": classes, "batching_ceiling": ceiling,
             "request_generation_s": gen_s}
     print(json.dumps(line), flush=True)
     return 0

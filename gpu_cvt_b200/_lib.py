@@ -30,7 +30,7 @@ class MeshInfo(C.Structure):
 class Params(C.Structure):
     _fields_ = [("k", i32), ("mode", i32), ("profile", i32), ("kproj", i32), ("ex_quirk", i32),
                 ("cell_factor", f32), ("use_graph", i32), ("knn_block", i32), ("clip_block", i32),
-                ("proj_block", i32), ("proj_mode", i32), ("frame_mode", i32)]
+                ("proj_block", i32), ("proj_mode", i32), ("frame_mode", i32), ("knn_reuse", i32)]
 
 
 class EvalOut(C.Structure):

@@ -957,6 +957,7 @@ extern "C" void cvt_params_default(cvt_params_t* p) {
   p->knn_block = p->clip_block = p->proj_block = 0;
   p->proj_mode = CVT_PROJ_ONERING;
   p->frame_mode = CVT_FRAME_VERTEX_NORMAL;
+  p->knn_reuse = 1;
 }
 
 // launch shapes the tiles may take (cvt_params_t knn_block / clip_block /
@@ -1068,6 +1069,9 @@ struct cvt_engine {
                                   // [2] BVH stack overflows of the projection (never expected)
   int num_sms = 148;
   void* d_cent = nullptr;
+  uint32_t* d_cand = nullptr;   // candidate lists (knn_reuse): cand_len(K) global ids per site
+  float* d_cand_r2 = nullptr;
+  double* d_cand_cum = nullptr;
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   // fork / join of the frame-vertex search, which runs on a second stream
@@ -1087,10 +1091,11 @@ struct cvt_engine {
 // destroys them.
 struct GraphKey {
   int dev, profile, k, knn_block, clip_block, proj_block, proj_mode, frame_mode;
+  bool knn_reuse;
   bool operator==(const GraphKey& o) const {
     return dev == o.dev && profile == o.profile && k == o.k && knn_block == o.knn_block &&
            clip_block == o.clip_block && proj_block == o.proj_block && proj_mode == o.proj_mode &&
-           frame_mode == o.frame_mode;
+           frame_mode == o.frame_mode && knn_reuse == o.knn_reuse;
   }
 };
 constexpr size_t kGraphCacheMax = 16;
@@ -1099,7 +1104,7 @@ static std::vector<std::pair<GraphKey, cudaGraphExec_t>> g_graph_cache;
 
 static GraphKey graph_key(const cvt_engine* e) {
   return {e->dev, e->p.profile, e->K, e->p.knn_block, e->p.clip_block, e->p.proj_block, e->p.proj_mode,
-          e->p.frame_mode};
+          e->p.frame_mode, e->p.knn_reuse != 0};
 }
 
 static cudaGraphExec_t graph_cache_take(const GraphKey& k) {
@@ -1148,6 +1153,11 @@ static void engine_free(cvt_engine* e) {
   dev_free_sync(e->arena);
   delete e;
 }
+
+// candidate list length for the site KNN's list reuse: K + 16, even, <= 64
+// (the longer the list, the longer it survives the sites' motion, and the
+// more a refresh costs)
+static constexpr int cand_len(int k) { return k + 16 > 64 ? 64 : k + 16; }
 
 static bool k_supported(int k) { return k == 8 || k == 12 || k == 16 || k == 20 || k == 24 || k == 32; }
 
@@ -1223,6 +1233,11 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   ar.add(&e->d_far, ns + 1);
   ar.add(&e->d_tickets, 3);  // scan ticket, bookkeeping ticket, BVH stack overflows
   ar.add(reinterpret_cast<char**>(&e->d_cent), tsz * 3 * ns);
+  if (q.knn_reuse) {
+    ar.add(&e->d_cand, (size_t)cand_len(e->K) * ns);
+    ar.add(&e->d_cand_r2, ns);
+    ar.add(&e->d_cand_cum, ns);
+  }
   ECK(ar.commit(&e->arena));
   e->bytes = ar.size;
   ECK(cudaMemset(e->arena, 0, ar.size));
@@ -1319,6 +1334,10 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   CK(cudaMemsetAsync(e->d_same + base, 0, n, st));
   k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_kth) + base, n, (int)0xbf800000);  // -1.0f
   CKLAUNCH();
+  if (e->d_cand_r2) {  // no candidate lists yet
+    k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_cand_r2) + base, n, (int)0xbf800000);
+    CKLAUNCH();
+  }
   CK(cudaMemsetAsync(e->d_stats + (size_t)s * kStatsRing * kStatsWords, 0, sizeof(int) * kStatsRing * kStatsWords, st));
   CK(cudaMemcpyAsync(e->d_active + s, &e->active[s], sizeof(int), cudaMemcpyHostToDevice, st));
   // the host mirrors above are read by the async copies; keep them stable
@@ -1353,16 +1372,23 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
   a.stats = e->d_stats; a.ovf = e->d_ovf; a.far = e->d_far; a.cent = (T*)e->d_cent; a.K = e->K;
   a.proj_mode = e->p.proj_mode; a.bvh_ovf = reinterpret_cast<int*>(e->d_tickets + 2);
+  a.cand = e->d_cand; a.cand_r2 = e->d_cand_r2; a.cand_cum = e->d_cand_cum;
   return a;
 }
 
-template <class T, int KK>
-static void launch_site_knn(const EngineArgs<T>& a, int nsites, int bs, cudaStream_t st) {
+template <class T, int KK, int MM>
+static void launch_site_knn_m(const EngineArgs<T>& a, int parity, int nsites, int bs, cudaStream_t st) {
   // one warp per site
   const int nb = cdiv((long)nsites * 32, bs);
-  if (bs == 64) k_site_knn<T, KK, 64><<<nb, 64, 0, st>>>(a);
-  else if (bs == 256) k_site_knn<T, KK, 256><<<nb, 256, 0, st>>>(a);
-  else k_site_knn<T, KK, 128><<<nb, 128, 0, st>>>(a);
+  if (bs == 64) k_site_knn<T, KK, MM, 64><<<nb, 64, 0, st>>>(a, parity);
+  else if (bs == 256) k_site_knn<T, KK, MM, 256><<<nb, 256, 0, st>>>(a, parity);
+  else k_site_knn<T, KK, MM, 128><<<nb, 128, 0, st>>>(a, parity);
+}
+
+template <class T, int KK>
+static void launch_site_knn(const EngineArgs<T>& a, int parity, int nsites, int bs, bool reuse, cudaStream_t st) {
+  if (reuse) launch_site_knn_m<T, KK, cand_len(KK)>(a, parity, nsites, bs, st);
+  else launch_site_knn_m<T, KK, 0>(a, parity, nsites, bs, st);
 }
 
 template <int PROF, int FRAME>
@@ -1442,13 +1468,14 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   CK(cudaEventRecord(br.join, br.side));
   L++;
   if (ev) CK(cudaEventRecord(ev[1], st));
+  const bool reuse = e->p.knn_reuse != 0;
   switch (e->K) {
-    case 8: launch_site_knn<T, 8>(a, ns, e->p.knn_block, st); break;
-    case 12: launch_site_knn<T, 12>(a, ns, e->p.knn_block, st); break;
-    case 16: launch_site_knn<T, 16>(a, ns, e->p.knn_block, st); break;
-    case 20: launch_site_knn<T, 20>(a, ns, e->p.knn_block, st); break;
-    case 24: launch_site_knn<T, 24>(a, ns, e->p.knn_block, st); break;
-    default: launch_site_knn<T, 32>(a, ns, e->p.knn_block, st); break;
+    case 8: launch_site_knn<T, 8>(a, parity, ns, e->p.knn_block, reuse, st); break;
+    case 12: launch_site_knn<T, 12>(a, parity, ns, e->p.knn_block, reuse, st); break;
+    case 16: launch_site_knn<T, 16>(a, parity, ns, e->p.knn_block, reuse, st); break;
+    case 20: launch_site_knn<T, 20>(a, parity, ns, e->p.knn_block, reuse, st); break;
+    case 24: launch_site_knn<T, 24>(a, parity, ns, e->p.knn_block, reuse, st); break;
+    default: launch_site_knn<T, 32>(a, parity, ns, e->p.knn_block, reuse, st); break;
   }
   L++;
   if (ev) CK(cudaEventRecord(ev[2], st));

@@ -72,6 +72,7 @@ struct SegDev {
   int stop_iters;      // stop after this many iterations (0: never)
   float thr2_tier[6];
   int need_tier[6];
+  double cum_motion;   // sum of the per-iteration maximum site motions so far
 };
 
 template <int PROF> struct PT;
@@ -106,6 +107,9 @@ template <class T> struct EngineArgs {
   int K;
   int proj_mode;  // 0: one-ring of the KPROJ nearest vertices; 1: closest point through the BVH
   int* bvh_ovf;   // BVH traversal stack overflows (never expected: the tree depth is bounded)
+  uint32_t* cand;    // candidate list per site (global ids), MM entries (k_site_knn)
+  float* cand_r2;    // its MM-th squared distance when it was built (< 0: no list; inf: every other site)
+  double* cand_cum;  // the segment's cum_motion when it was built
 };
 
 // polygon storage: vertex k at p[k * stride] (shared memory: thread-
@@ -391,10 +395,23 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
 // read (for the freeze test's equality) and written coalesced.
 // Sets same[g] (new list == stored list) and kth[g].
 // ---------------------------------------------------------------------------
-template <class T, int KK, int BS>
-__global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
+// Candidate lists (MM > 0): besides its K neighbours, a site keeps the MM
+// nearest other sites of the last full search (ids, the MM-th squared
+// distance r2b, and the segment's cumulative motion at that iteration).
+// While every site has moved by at most D in total since then (D = the sum
+// of the segment's per-iteration maximum motions), a site outside the list
+// is still farther than sqrt(r2b) - 2 D, so when the K-th nearest of the
+// re-keyed list is closer than that, the list's first K are exactly the K
+// nearest of all: the same keys as a full search, at a fraction of its
+// work.  Otherwise (and in a segment's first iteration) the full search
+// runs for MM neighbours and refreshes the list.  Margins of 1e-4 cover the
+// rounding of the distances and of the accumulated motion.
+template <class T, int KK, int MM, int BS>
+__global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
   static_assert(KK <= 32, "one list entry per lane");
+  static_assert(MM == 0 || (MM > KK && MM <= 64 && MM % 2 == 0), "candidate list of KK < MM <= 64 (even) entries");
   using O = KeyOps<T>;
+  using Key = typename O::Key;
   const int lane = threadIdx.x & 31;
   const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
   if (w >= __ldg(a.act_count)) return;  // whole warp
@@ -408,21 +425,79 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a) {
   // the same K points), and the K-th distance equals the (K+1)-th with self.
   constexpr int K = KK;
   const V3<T> q{me.x, me.y, me.z};
-  const GridGeom G = a.geom[s];
   const float kp = a.kth[g];
-  // candidates beyond 1.1x the last K-th squared distance are skipped; sites
-  // move little between iterations, and a bound that proves too tight
-  // restarts the search without it (swept 1.02-1.5: 1.05-1.1 fastest)
-  const T thr0 = kp >= 0.f ? (T)kp * (T)1.1 : (T)sd.kth_est;
-  constexpr int R = (KK + 31) / 32;
-  typename O::Key key[R];
   const uint32_t self = (uint32_t)g;
-  warp_knn<T, T, KK>(G, a.cell_start, a.sorted, q, thr0, lane, [self](uint32_t id) { return id != self; }, key);
-  const auto kth = shfl_key(key[(KK - 1) / 32], (KK - 1) % 32);
+  Key key;  // lane j: entry j of the K-list
+  bool have = false;
+  if constexpr (MM > 0) {
+    const float r2b = a.cand_r2[g];
+    if (r2b >= 0.f) {
+      // re-key the list at the current positions and put it in order
+      // (element e = 2 lane + r)
+      const uint32_t* cr = a.cand + (size_t)g * MM;
+      const T* S = a.S[parity];
+      Key k2[2];
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int e = 2 * lane + r;
+        k2[r] = O::empty();
+        if (e < MM) {
+          const uint32_t id = __ldg(cr + e);
+          if (id != 0xffffffffu) k2[r] = O::make(dist2(ld3(S, (long)id), q), id);
+        }
+      }
+      const bool moved = warp_order_pairs<T>(k2[0], k2[1], lane);
+      // entry j to lane j
+      const Key e0 = shfl_key(k2[0], lane >> 1), e1 = shfl_key(k2[1], lane >> 1);
+      key = (lane & 1) ? e1 : e0;
+      const Key kth = shfl_key(key, KK - 1);
+      const double D = sd.cum_motion - a.cand_cum[g];
+      const double kap = sqrt((double)O::dist(kth));
+      have = !O::is_empty(kth) &&
+             (isinf(r2b) || kap * 1.0001 + 2.0 * D * 1.0001 < sqrt((double)r2b) * 0.9999);
+      if (have && moved) {
+        // keep the list in its new order: the next iteration starts sorted
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int e = 2 * lane + r;
+          if (e < MM) a.cand[(size_t)g * MM + e] = O::idx(k2[r]);
+        }
+      }
+    }
+    if (!have) {
+      // full search for MM neighbours; its first KK are the K-list
+      constexpr int RM = (MM + 31) / 32;
+      Key mk[RM];
+      const T thrM = r2b >= 0.f && !isinf(r2b) ? (T)r2b * (T)1.2
+                     : (kp >= 0.f ? (T)kp * (T)(1.1 * (MM + 1) / (KK + 1)) : (T)sd.kth_est * (T)((MM + 1.0) / (KK + 1)));
+      warp_knn<T, T, MM>(a.geom[s], a.cell_start, a.sorted, q, thrM, lane,
+                         [self](uint32_t id) { return id != self; }, mk);
+#pragma unroll
+      for (int r = 0; r < RM; ++r)
+        if (32 * r + lane < MM) a.cand[(size_t)g * MM + 32 * r + lane] = O::idx(mk[r]);
+      const Key mth = shfl_key(mk[(MM - 1) / 32], (MM - 1) % 32);
+      if (lane == 0) {
+        a.cand_r2[g] = O::is_empty(mth) ? __int_as_float(0x7f800000) : (float)O::dist(mth);
+        a.cand_cum[g] = sd.cum_motion;
+      }
+      key = mk[0];
+    }
+  } else {
+    // candidates beyond 1.1x the last K-th squared distance are skipped; sites
+    // move little between iterations, and a bound that proves too tight
+    // restarts the search without it (swept 1.02-1.5: 1.05-1.1 fastest)
+    const T thr0 = kp >= 0.f ? (T)kp * (T)1.1 : (T)sd.kth_est;
+    Key kl[1];
+    warp_knn<T, T, KK>(a.geom[s], a.cell_start, a.sorted, q, thr0, lane,
+                       [self](uint32_t id) { return id != self; }, kl);
+    key = kl[0];
+  }
+  (void)have;
+  const Key kth = shfl_key(key, KK - 1);
   const bool full = !O::is_empty(kth);
   if (lane == 0) a.kth[g] = full ? (float)O::dist(kth) : -1.f;
   const uint32_t base = (uint32_t)sd.site_base;
-  const uint32_t gid = O::idx(key[0]);
+  const uint32_t gid = O::idx(key);
   const uint32_t out = gid == 0xffffffffu ? 0xffffffffu : gid - base;
   uint32_t* row = a.knn + (size_t)g * K;
   bool diff = false;
@@ -718,6 +793,9 @@ __device__ __forceinline__ void seg_advance(SegDev* segs, int* active, int nseg,
     int* sl = stats + ((size_t)s * kStatsRing + (nx % kStatsRing)) * kStatsWords;
     for (int w = 0; w < kStatsWords; ++w) sl[w] = 0;
     segs[s].iter = nx;
+    // motion bound of the candidate lists (a NaN motion poisons it, and the
+    // lists are then never trusted again in this segment)
+    segs[s].cum_motion += (double)sqrtf(d2) * (1.0 + 1e-6);
     const float lim = segs[s].stop_motion2;
     const int cap = segs[s].stop_iters;
     if ((lim >= 0.f && d2 <= lim) || (cap > 0 && nx >= cap)) active[s] = 2;

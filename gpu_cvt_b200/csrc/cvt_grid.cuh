@@ -315,6 +315,43 @@ __device__ __forceinline__ void warp_knn(const GridGeom& g, const int* __restric
 }
 
 // ---------------------------------------------------------------------------
+// warp-wide ordering of a short key list held two keys per lane (element e
+// = 2 lane + r, r = 0, 1): odd-even transposition passes until the list is
+// in order.  A list that is already nearly in order (a site's candidate
+// list from an earlier iteration, re-keyed at the sites' new positions)
+// needs a pass or two; 64 passes order any list.  Returns true when some
+// key moved.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long shfl_down_key(unsigned long long k, int d) {
+  return __shfl_down_sync(0xffffffffu, k, d);
+}
+__device__ __forceinline__ DKey shfl_down_key(DKey k, int d) {
+  return {__shfl_down_sync(0xffffffffu, k.d, d), __shfl_down_sync(0xffffffffu, k.i, d)};
+}
+
+template <class T>
+__device__ __forceinline__ bool warp_order_pairs(typename KeyOps<T>::Key& k0, typename KeyOps<T>::Key& k1, int lane) {
+  using O = KeyOps<T>;
+  bool moved = false;
+  for (int pass = 0; pass < 64; ++pass) {
+    // in order: k0 < k1 in every lane and k1 < the next lane's k0
+    const auto nx = shfl_down_key(k0, 1);
+    const bool ok = !O::less(k1, k0) && (lane == 31 || !O::less(nx, k1));
+    if (__all_sync(0xffffffffu, ok)) break;
+    moved = true;
+    // pairs (2l, 2l+1): inside the lane
+    const auto lo = O::kmin(k0, k1), hi = O::kmax(k0, k1);
+    k0 = lo; k1 = hi;
+    // pairs (2l+1, 2l+2): this lane's k1 with the next lane's k0
+    const auto nk0 = shfl_down_key(k0, 1);
+    const auto pk1 = shfl_up_key(k1);
+    if (lane < 31) k1 = O::kmin(k1, nk0);
+    if (lane > 0) k0 = O::kmax(k0, pk1);
+  }
+  return moved;
+}
+
+// ---------------------------------------------------------------------------
 // grid build: count -> exclusive scan -> scatter
 // ---------------------------------------------------------------------------
 struct SegGrid {           // the minimal per-point view the build needs

@@ -30,11 +30,13 @@ FRAME = {"vertex": 0, "pca": 1}
 
 
 def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1, use_graph=True,
-           knn_block=0, clip_block=0, proj_block=0, proj="onering", frame="vertex") -> Params:
+           knn_block=0, clip_block=0, proj_block=0, proj="onering", frame="vertex", knn_reuse=True) -> Params:
     """Engine parameters.  proj: "onering" (the reference's projection onto
     the one-rings of the 5 nearest vertices) or "bvh" (exact closest point
     through the mesh's BVH); frame: "vertex" (the nearest vertex normal, as
-    the reference) or "pca" (PCA normal of the site's neighbours)."""
+    the reference) or "pca" (PCA normal of the site's neighbours);
+    knn_reuse: take the K-lists from each site's kept candidate list while
+    the sites' motion proves it exact (same lists, less work)."""
     p = Params()
     _lib.load().cvt_params_default(C.byref(p))
     p.k = int(k)
@@ -47,6 +49,7 @@ def params(k=24, mode=0, profile="ref", kproj=5, ex_quirk=True, cell_factor=1.1,
     p.knn_block, p.clip_block, p.proj_block = int(knn_block), int(clip_block), int(proj_block)
     p.proj_mode = PROJ[proj] if isinstance(proj, str) else int(proj)
     p.frame_mode = FRAME[frame] if isinstance(frame, str) else int(frame)
+    p.knn_reuse = int(bool(knn_reuse))
     return p
 
 

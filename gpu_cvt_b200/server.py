@@ -43,6 +43,7 @@ class Request:
     arrival: float
     admitted: float = -1.0
     done: float = -1.0
+    service: float = -1.0   # plain loop: seconds from admission to done
     iters: int = 0
     result: np.ndarray | None = field(default=None, repr=False)
 
@@ -178,6 +179,7 @@ def serve_plain(meshes, requests, k=24, mode=1, profile="mixed", tol=1e-4, max_i
             if state[seg] == 2:
                 break
         r.done = time.perf_counter() - t0
+        r.service = r.done - r.admitted
         r.iters = int(iters[seg])
         if keep_results:
             r.result = eng.sites(seg)
@@ -191,3 +193,33 @@ def serve_plain(meshes, requests, k=24, mode=1, profile="mixed", tol=1e-4, max_i
             "sites_iters_per_s": work / makespan, "latency_p50_s": _percentile(lat, 50),
             "latency_p99_s": _percentile(lat, 99), "latency_mean_s": float(np.mean(lat)),
             "iters_mean": float(np.mean([r.iters for r in requests])), "gpu_launches": launches}
+
+
+def size_classes(requests, bounds=(20_000, 200_000)):
+    """Per request-size class of a plain (one at a time) run: requests, share
+    of the stream's site-iterations, and the sites x iterations per second
+    each class reached alone (its work over its service time)."""
+    out = []
+    lo = 0
+    for hi in list(bounds) + [None]:
+        cls = [r for r in requests if r.n >= lo and (hi is None or r.n < hi)]
+        work = sum(r.n * r.iters for r in cls)
+        svc = sum(r.service for r in cls)
+        out.append({"sites": [lo, hi], "requests": len(cls), "work_share": 0.0, "site_iters": int(work),
+                    "plain_rate": work / svc if svc > 0 else None})
+        lo = hi if hi is not None else lo
+    tot = sum(c["site_iters"] for c in out)
+    for c in out:
+        c["work_share"] = c["site_iters"] / tot if tot else 0.0
+    return out
+
+
+def batching_ceiling(requests, plain_makespan):
+    """Upper bound of the served/plain throughput ratio: even with perfect
+    overlap, the stream's work takes at least its site-iterations divided by
+    the best rate any single request reached in the plain loop (a large
+    request already fills the GPU), and no earlier than the last arrival."""
+    best = max(r.n * r.iters / r.service for r in requests if r.service > 0)
+    work = sum(r.n * r.iters for r in requests)
+    t_min = max(work / best, max(r.arrival for r in requests))
+    return {"best_single_request_rate": best, "min_makespan_s": t_min, "max_ratio": plain_makespan / t_min}

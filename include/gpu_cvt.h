@@ -272,6 +272,12 @@ typedef struct {
    *            neighbours (the smallest-eigenvalue eigenvector of their
    *            covariance, oriented like the vertex normal). */
   int proj_mode, frame_mode;
+  /* knn_reuse 1 (default): each site also keeps the K+16 nearest sites of
+   * its last full KNN search, and while the sites' accumulated motion proves
+   * that no other site can have come closer than its K-th neighbour, the
+   * K-list is taken from those candidates (same lists as a full search);
+   * 0: a full search every iteration. */
+  int knn_reuse;
 } cvt_params_t;
 #define CVT_PROJ_ONERING 0
 #define CVT_PROJ_BVH 1
