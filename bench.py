@@ -255,6 +255,14 @@ def batched_workload(n_meshes, ws):
     return meshes, cfg, gen_s
 
 
+def rank_share(meshes, ws, rank):
+    """Indices of the meshes rank `rank` of `ws` remeshes: a size-balanced
+    partition by site count, the same on every rank without communication."""
+    from gpu_cvt_b200 import replicas
+    sizes = [int(S.shape[0]) for *_, S in meshes]
+    return replicas.partition(sizes, ws, rank) if ws > 1 else list(range(len(meshes)))
+
+
 def torus_workload(ws):
     from gpu_cvt_b200 import meshgen as mg
     m, S, p = mg.workload_mesh("torus_100k")
@@ -357,14 +365,14 @@ def _barrier(ws):
 
 def run_ours_batched(args):
     import torch
-    from gpu_cvt_b200 import _lib, replicas, workloads
+    from gpu_cvt_b200 import _lib, workloads
     from gpu_cvt_b200 import engine as E
 
     ws, rank, local = dist_setup()
     _init_dist(ws, local)
     meshes_all, cfg, gen_s = batched_workload(args.meshes, ws)
     sizes = [int(S.shape[0]) for *_, S in meshes_all]
-    mine = replicas.partition(sizes, ws, rank) if ws > 1 else list(range(len(meshes_all)))
+    mine = rank_share(meshes_all, ws, rank)
     meshes = [meshes_all[i] for i in mine]
     K, mode, iters = cfg["k"], cfg["mode"], cfg["iters"]
     n_mine = sum(int(S.shape[0]) for *_, S in meshes)

@@ -454,3 +454,27 @@ def test_knn_candidate_lists_match_full_search(eng, oracle, small_torus, mode, k
     assert out[True][2] == out[False][2]
     r = oracle.lloyd_run(m.V, m.F, S0, k, mode, 40, profile=oracle.P_MIXED)
     assert np.array_equal(out[True][0], r["S"])
+
+
+@pytest.mark.parametrize("mode,k", [(0, 24), (1, 32), (2, 20)])
+def test_knn_candidate_lists_match_full_search(eng, oracle, small_torus, mode, k):
+    """Lists taken from the kept candidate lists (knn_reuse, the default) are
+    the lists a full search finds: whole runs with and without reuse agree
+    bit for bit, and with the oracle."""
+    m, S0 = small_torus
+    out = {}
+    for reuse in (True, False):
+        M = eng.Mesh(m.V, m.F)
+        e = eng.Engine(eng.params(k=k, mode=mode, profile="mixed", knn_reuse=reuse), 1, len(S0),
+                       eng.grid_cells(M, len(S0), k))
+        g = e.add(M, S0)
+        e.run(40)
+        out[reuse] = (e.sites(g), e.state(g)["knn"],
+                      [e.stats(g, i)["same"] for i in range(40)])
+        e.close()
+        M.close()
+    assert np.array_equal(out[True][0], out[False][0])
+    assert np.array_equal(out[True][1], out[False][1])
+    assert out[True][2] == out[False][2]
+    r = oracle.lloyd_run(m.V, m.F, S0, k, mode, 40, profile=oracle.P_MIXED)
+    assert np.array_equal(out[True][0], r["S"])
