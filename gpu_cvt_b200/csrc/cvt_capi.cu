@@ -1071,7 +1071,8 @@ struct cvt_engine {
   void* d_cent = nullptr;
   uint32_t* d_cand = nullptr;   // candidate lists (knn_reuse): cand_len(K) global ids per site
   float* d_cand_r2 = nullptr;
-  double* d_cand_cum = nullptr;
+  float* d_cand_D = nullptr;
+  unsigned long long* d_blockmax = nullptr;  // per cell slot: coarse-block motion of the last step
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   // fork / join of the frame-vertex search, which runs on a second stream
@@ -1236,7 +1237,8 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   if (q.knn_reuse) {
     ar.add(&e->d_cand, (size_t)cand_len(e->K) * ns);
     ar.add(&e->d_cand_r2, ns);
-    ar.add(&e->d_cand_cum, ns);
+    ar.add(&e->d_cand_D, ns);
+    ar.add(&e->d_blockmax, (size_t)max_cells);
   }
   ECK(ar.commit(&e->arena));
   e->bytes = ar.size;
@@ -1334,9 +1336,10 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   CK(cudaMemsetAsync(e->d_same + base, 0, n, st));
   k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_kth) + base, n, (int)0xbf800000);  // -1.0f
   CKLAUNCH();
-  if (e->d_cand_r2) {  // no candidate lists yet
+  if (e->d_cand_r2) {  // no candidate lists yet; no motion recorded in the segment's blocks
     k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_cand_r2) + base, n, (int)0xbf800000);
     CKLAUNCH();
+    CK(cudaMemsetAsync(e->d_blockmax + cbase, 0, sizeof(unsigned long long) * (size_t)cells, st));
   }
   CK(cudaMemsetAsync(e->d_stats + (size_t)s * kStatsRing * kStatsWords, 0, sizeof(int) * kStatsRing * kStatsWords, st));
   CK(cudaMemcpyAsync(e->d_active + s, &e->active[s], sizeof(int), cudaMemcpyHostToDevice, st));
@@ -1372,7 +1375,7 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
   a.stats = e->d_stats; a.ovf = e->d_ovf; a.far = e->d_far; a.cent = (T*)e->d_cent; a.K = e->K;
   a.proj_mode = e->p.proj_mode; a.bvh_ovf = reinterpret_cast<int*>(e->d_tickets + 2);
-  a.cand = e->d_cand; a.cand_r2 = e->d_cand_r2; a.cand_cum = e->d_cand_cum;
+  a.cand = e->d_cand; a.cand_r2 = e->d_cand_r2; a.cand_D = e->d_cand_D; a.blockmax = e->d_blockmax;
   return a;
 }
 

@@ -72,7 +72,7 @@ struct SegDev {
   int stop_iters;      // stop after this many iterations (0: never)
   float thr2_tier[6];
   int need_tier[6];
-  double cum_motion;   // sum of the per-iteration maximum site motions so far
+  float step_motion;   // largest site motion of the segment's last iteration
 };
 
 template <int PROF> struct PT;
@@ -109,8 +109,18 @@ template <class T> struct EngineArgs {
   int* bvh_ovf;   // BVH traversal stack overflows (never expected: the tree depth is bounded)
   uint32_t* cand;    // candidate list per site (global ids), MM entries (k_site_knn)
   float* cand_r2;    // its MM-th squared distance when it was built (< 0: no list; inf: every other site)
-  double* cand_cum;  // the segment's cum_motion when it was built
+  float* cand_D;     // motion bound accumulated since it was built (k_site_knn)
+  unsigned long long* blockmax;  // per coarse block (cell slots of the segment): iteration << 32 | max motion bits
 };
+
+// Coarse motion blocks of a segment: 4 x 4 x 4 grid cells, stored in the
+// first cells of the segment's cell range (there are fewer blocks than
+// cells).  Positions outside the grid fall in the edge blocks, like cells.
+template <class T>
+__device__ __forceinline__ int motion_block(const GridGeom& g, V3<T> p, int& bx, int& by, int& bz) {
+  bx = grid_coord(g, p.x, 0) >> 2; by = grid_coord(g, p.y, 1) >> 2; bz = grid_coord(g, p.z, 2) >> 2;
+  return g.cell_base + (bz * ((g.dim[1] + 3) >> 2) + by) * ((g.dim[0] + 3) >> 2) + bx;
+}
 
 // polygon storage: vertex k at p[k * stride] (shared memory: thread-
 // interleaved; local memory: stride 1)
@@ -396,16 +406,21 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
 // Sets same[g] (new list == stored list) and kth[g].
 // ---------------------------------------------------------------------------
 // Candidate lists (MM > 0): besides its K neighbours, a site keeps the MM
-// nearest other sites of the last full search (ids, the MM-th squared
-// distance r2b, and the segment's cumulative motion at that iteration).
-// While every site has moved by at most D in total since then (D = the sum
-// of the segment's per-iteration maximum motions), a site outside the list
-// is still farther than sqrt(r2b) - 2 D, so when the K-th nearest of the
-// re-keyed list is closer than that, the list's first K are exactly the K
-// nearest of all: the same keys as a full search, at a fraction of its
-// work.  Otherwise (and in a segment's first iteration) the full search
-// runs for MM neighbours and refreshes the list.  Margins of 1e-4 cover the
-// rounding of the distances and of the accumulated motion.
+// nearest other sites of its last full search (ids and the MM-th squared
+// distance r2b = rho^2) and a bound D on how much closer any other site can
+// have come since.  Every iteration adds to D the site's own last motion and
+// the largest last motion of any site in the 27 coarse blocks (4 x 4 x 4
+// cells, edge B = 4h) around the site's old position.  A site j outside the
+// list started at distance >= rho; while it is within B of site i its steps
+// are among those counted, and it cannot jump from beyond B to within rho in
+// one step as long as (largest motion of the step in the segment) + (i's
+// motion) < B - rho, which every iteration checks.  So when the K-th nearest
+// of the re-keyed list is closer than rho - D, no site outside the list is
+// closer: the list's first K are exactly the K nearest of all, the keys a
+// full search returns, at a fraction of its work.  Otherwise (and in a
+// segment's first iteration) the full search runs for MM neighbours and
+// refreshes the list.  Margins of 1e-4 cover the rounding of the distances
+// and of the accumulated motion; a NaN motion fails every test.
 template <class T, int KK, int MM, int BS>
 __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
   static_assert(KK <= 32, "one list entry per lane");
@@ -432,6 +447,28 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
   if constexpr (MM > 0) {
     const float r2b = a.cand_r2[g];
     if (r2b >= 0.f) {
+      // the motion bound of the last step: this site's own motion, the
+      // largest motion in the 27 coarse blocks around its old position
+      // (lane b < 27 reads block b), and the step condition that no site
+      // from beyond those blocks reached the list's radius in one step
+      const GridGeom G = a.geom[s];
+      const V3<T> prev = ld3(a.S[parity ^ 1], g);
+      int bx, by, bz;
+      motion_block(G, prev, bx, by, bz);
+      unsigned mbits = 0u;
+      if (lane < 27) {
+        const int x = bx + lane % 3 - 1, y = by + (lane / 3) % 3 - 1, z = bz + lane / 9 - 1;
+        const int dx = (G.dim[0] + 3) >> 2, dy = (G.dim[1] + 3) >> 2, dz = (G.dim[2] + 3) >> 2;
+        if (x >= 0 && x < dx && y >= 0 && y < dy && z >= 0 && z < dz) {
+          const unsigned long long v = a.blockmax[G.cell_base + (z * dy + y) * dx + x];
+          if ((unsigned)(v >> 32) == (unsigned)(sd.iter - 1)) mbits = (unsigned)v;
+        }
+      }
+      mbits = __reduce_max_sync(0xffffffffu, mbits);
+      const double mu_i = sqrt((double)dist2(cvt3<double>(q), cvt3<double>(prev)));
+      const double rho = sqrt((double)r2b);
+      const double D = (double)a.cand_D[g] + (mu_i + (double)__uint_as_float(mbits)) * 1.0001;
+      const bool step_ok = ((double)sd.step_motion + mu_i) * 1.0001 < (4.0 * (double)G.h - rho) * 0.9999;
       // re-key the list at the current positions and put it in order
       // (element e = 2 lane + r)
       const uint32_t* cr = a.cand + (size_t)g * MM;
@@ -451,16 +488,17 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
       const Key e0 = shfl_key(k2[0], lane >> 1), e1 = shfl_key(k2[1], lane >> 1);
       key = (lane & 1) ? e1 : e0;
       const Key kth = shfl_key(key, KK - 1);
-      const double D = sd.cum_motion - a.cand_cum[g];
       const double kap = sqrt((double)O::dist(kth));
-      have = !O::is_empty(kth) &&
-             (isinf(r2b) || kap * 1.0001 + 2.0 * D * 1.0001 < sqrt((double)r2b) * 0.9999);
-      if (have && moved) {
-        // keep the list in its new order: the next iteration starts sorted
+      have = !O::is_empty(kth) && (isinf(r2b) || (step_ok && kap * 1.0001 + D * 1.0001 < rho * 0.9999));
+      if (have) {
+        if (lane == 0) a.cand_D[g] = __double2float_ru(D);
+        if (moved) {
+          // keep the list in its new order: the next iteration starts sorted
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          const int e = 2 * lane + r;
-          if (e < MM) a.cand[(size_t)g * MM + e] = O::idx(k2[r]);
+          for (int r = 0; r < 2; ++r) {
+            const int e = 2 * lane + r;
+            if (e < MM) a.cand[(size_t)g * MM + e] = O::idx(k2[r]);
+          }
         }
       }
     }
@@ -478,7 +516,7 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
       const Key mth = shfl_key(mk[(MM - 1) / 32], (MM - 1) % 32);
       if (lane == 0) {
         a.cand_r2[g] = O::is_empty(mth) ? __int_as_float(0x7f800000) : (float)O::dist(mth);
-        a.cand_cum[g] = sd.cum_motion;
+        a.cand_D[g] = 0.f;
       }
       key = mk[0];
     }
@@ -763,6 +801,27 @@ __device__ __forceinline__ void stats_stage_flush(int* stats, const SegDev* segs
   atomicMax(reinterpret_cast<unsigned*>(sl + 4), stage.v[4]);
 }
 
+// This step's motion of site g (o from site_finish; o.seg < 0: none) into
+// its coarse block at its old position, for the next iteration's KNN:
+// warp-collective, one atomic per distinct block of the warp.  The stamp is
+// the segment's iteration, so an entry from an earlier iteration reads as
+// no motion.
+template <class T>
+__device__ __forceinline__ void motion_to_block(const EngineArgs<T>& a, int parity, int g, const SiteOut& o) {
+  int blk = -1;
+  unsigned bits = 0u, stamp = 0u;
+  if (g >= 0 && o.seg >= 0) {
+    int bx, by, bz;
+    blk = motion_block(a.geom[o.seg], ld3(a.S[parity], g), bx, by, bz);
+    bits = __float_as_uint(sqrtf(o.disp2));
+    stamp = (unsigned)a.segs[o.seg].iter;
+  }
+  const unsigned peers = __match_any_sync(0xffffffffu, blk);
+  const unsigned mb = __reduce_max_sync(peers, bits);
+  if (blk >= 0 && (int)(threadIdx.x & 31) == __ffs(peers) - 1)
+    atomicMax(a.blockmax + blk, ((unsigned long long)stamp << 32) | mb);
+}
+
 template <int PROF, int BS, int PROJ>
 __global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
   __shared__ StatsStage stage;
@@ -771,7 +830,12 @@ __global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::
   const int t = blockIdx.x * BS + threadIdx.x;
   const int n_grid = __ldg(a.cell_start + a.total_cells);
   SiteOut o{-1, 0, 0, 0, 0, 0.f};
-  if (t < n_grid) site_proj<PROF, PROJ>(a, parity, (int)a.sorted[t].id, o);
+  int g = -1;
+  if (t < n_grid) {
+    g = (int)a.sorted[t].id;
+    site_proj<PROF, PROJ>(a, parity, g, o);
+  }
+  if (a.blockmax) motion_to_block(a, parity, g, o);
   stats_flush(a.stats, a.segs, o, stage);
   __syncthreads();
   stats_stage_flush(a.stats, a.segs, stage);
@@ -793,9 +857,8 @@ __device__ __forceinline__ void seg_advance(SegDev* segs, int* active, int nseg,
     int* sl = stats + ((size_t)s * kStatsRing + (nx % kStatsRing)) * kStatsWords;
     for (int w = 0; w < kStatsWords; ++w) sl[w] = 0;
     segs[s].iter = nx;
-    // motion bound of the candidate lists (a NaN motion poisons it, and the
-    // lists are then never trusted again in this segment)
-    segs[s].cum_motion += (double)sqrtf(d2) * (1.0 + 1e-6);
+    // the step bound of the candidate lists (NaN fails every test)
+    segs[s].step_motion = sqrtf(d2);
     const float lim = segs[s].stop_motion2;
     const int cap = segs[s].stop_iters;
     if ((lim >= 0.f && d2 <= lim) || (cap > 0 && nx >= cap)) active[s] = 2;
@@ -844,6 +907,12 @@ __global__ void __launch_bounds__(128) k_site_far(EngineArgs<typename PT<PROF>::
       SiteOut o{-1, 0, 0, 0, 0, 0.f};
       site_finish<PROF, 0>(a, parity, g, knnv, o);
       stats_atomic(a.stats, a.segs, o);
+      if (a.blockmax) {
+        int bx, by, bz;
+        const int blk = motion_block(a.geom[o.seg], ld3(a.S[parity], g), bx, by, bz);
+        atomicMax(a.blockmax + blk, ((unsigned long long)(unsigned)a.segs[o.seg].iter << 32) |
+                                        __float_as_uint(sqrtf(o.disp2)));
+      }
     }
     __syncthreads();
   }

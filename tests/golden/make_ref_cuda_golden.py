@@ -117,12 +117,60 @@ def torus_100k(out):
     print(json.dumps(summ, indent=1))
 
 
+def torus_100k_iters(out, r=None, ours=None):
+    """The 100k-site torus (K=24, mode 1), iterations 1-10 by the reference's
+    kernels against the engine's ref and mixed profiles: positions at
+    iterations 1, 2, 5, 10 of every 20th site and of every site that strays
+    more than 1e-6 of the diagonal in either profile, and, for those sites,
+    whether the reference's first-iteration centroid is a projection tie
+    (the best two faces of its one-rings within 1e-3 in squared distance).
+    r / ours: results already computed (the harness run, {profile: sites per
+    iteration}); run here when None."""
+    import torch
+    from gpu_cvt_b200 import engine as E
+    from oracle import oracle as O
+    m, S, p = mg.workload_mesh("torus_100k")
+    diag = mg.bbox_diag(m.V)
+    if r is None:
+        r = ref_runner.run(m.V, m.F, S, p["k"], p["mode"], 10, dump=list(range(1, 11)))
+    if ours is None:
+        ours = {}
+        M = E.Mesh(m.V, m.F)
+        for prof in ("ref", "mixed"):
+            e = E.Engine(E.params(k=p["k"], mode=p["mode"], profile=prof), 1, S.shape[0],
+                         E.grid_cells(M, S.shape[0], p["k"]))
+            g = e.add(M, S)
+            arr = []
+            for _ in range(10):
+                e.run(1)
+                arr.append(e.sites(g))
+            ours[prof] = np.stack(arr)
+            e.close()
+        torch.cuda.synchronize()
+    far = np.zeros(S.shape[0], bool)
+    for prof in ("ref", "mixed"):
+        d = np.linalg.norm(ours[prof].astype(np.float64) - r["S"].astype(np.float64), axis=2) / diag
+        far |= (d > 1e-6).any(0)
+    idx = np.union1d(np.arange(0, S.shape[0], 20), np.flatnonzero(far)).astype(np.int32)
+    off, fcs = O.build_vf(m.nV, m.F)
+    tie = np.zeros(idx.size, bool)
+    for k, i in enumerate(idx):
+        c = r["cent0"][i]
+        d2 = sorted(float(((O.closest_point_tri(c, *m.V[m.F[f]]).astype(np.float64) - c) ** 2).sum())
+                    for f in {int(f) for v in r["knnv0"][i] if v >= 0 for f in fcs[off[v]:off[v + 1]]})
+        tie[k] = len(d2) > 1 and d2[1] - d2[0] <= 1e-3 * d2[1]
+    iters = np.array([1, 2, 5, 10], np.int32)
+    np.savez_compressed(os.path.join(out, "ref_cuda_torus100k_iters.npz"), idx=idx, iters=iters,
+                        S=r["S"][iters - 1][:, idx], tie=tie, diag=np.float64(diag))
+
+
 def main(out):
     os.makedirs(out, exist_ok=True)
     if not ref_runner.available():
         raise SystemExit("oracle/_ref/ref_harness is missing: build it with `make -C oracle ref`")
     small_cases(out)
     torus_100k(out)
+    torus_100k_iters(out)
 
 
 if __name__ == "__main__":

@@ -7,12 +7,13 @@ projection, freeze, normals, face extraction, Hausdorff) in the order of
 main.cu:669-974, with an exact brute-force site KNN in place of the hub KNN
 (whose output is corrupted on that GPU, see the first test).
 
-Bounds: identical neighbour lists and freeze counts; positions within 1e-6 of
-the bbox diagonal for the first iterations, 1e-5 after 10; after 30-50
-iterations Lloyd's sensitivity to last-bit differences (rsqrtf vs 1/sqrt, FMA
-contraction) allows an occasional flipped neighbour, so the mean stays below
-1e-6 and the max below 1e-4 of the diagonal.  Hausdorff within 1e-4 of the
-diagonal.  The libgpucvt kernels equal the oracle bit for bit (test_gpu_*), so
+Bounds (fractions of the bbox diagonal): identical neighbour lists and freeze
+counts; positions within 1e-6 up to 10 iterations; after 30-50 iterations all
+but a handful of sites within 1e-5 (Lloyd's sensitivity to last-bit
+differences -- rsqrtf vs 1/sqrt, FMA contraction -- lets an occasional site
+follow another branch: a flipped neighbour, or a centroid equidistant from
+two faces whose closest points differ, test_gpu_ref_cuda_torus100k.py), the
+mean below 1e-6.  Hausdorff within 1e-4 of the diagonal.  The libgpucvt kernels equal the oracle bit for bit (test_gpu_*), so
 the same bounds hold for them.
 """
 import os
@@ -52,10 +53,11 @@ def test_icosphere_2k_against_reference_kernels(oracle):
         r = oracle.lloyd_run(m.V, m.F, S0, 20, 0, int(it))
         d = np.linalg.norm(g["S"][k] - r["S"], axis=1) / diag
         if it <= 10:
-            assert d.max() < (1e-6 if it <= 2 else 1e-5), it
+            assert d.max() < 1e-6, it
             assert np.array_equal(g["counts"][:it], r["counts"]), it
         else:
-            assert d.mean() < 1e-6 and d.max() < 1e-4, it
+            # 50 iterations: measured max 1.1e-5 (2 of 2,000 sites above 1e-5)
+            assert d.mean() < 1e-6 and d.max() < 2e-5 and (d > 1e-5).sum() <= 2, it
     # evaluation after 50 iterations: dual mesh + one-sided Hausdorff
     r = oracle.lloyd_run(m.V, m.F, S0, 20, 0, 50)
     S = r["S"]
@@ -79,7 +81,13 @@ def test_torus_freezing_against_reference_kernels(oracle, mode):
     assert abs(int(g["frozen"].sum()) - int(r["frozen"].sum())) <= 0.01 * len(r["frozen"])
     assert (g["frozen"] == r["frozen"]).mean() > 0.99
     d = np.linalg.norm(g["S"][-1] - r["S"], axis=1) / diag
-    assert d.mean() < 1e-6 and d.max() < 1e-4
+    # 30 iterations: measured max 6.0e-6 (mode 1); 8.0e-5 with 8 of 4,000
+    # sites above 1e-5 (mode 2, whose sixth tier freezes sites on other branches)
+    assert d.mean() < 1e-6
+    if mode == 1:
+        assert d.max() < 1e-5
+    else:
+        assert d.max() < 1e-4 and (d > 1e-5).sum() <= 10
     if g["dump_iters"][0] == 1:
         r1 = oracle.lloyd_run(t.V, t.F, g["S0"], 24, mode, 1)
         assert np.linalg.norm(g["S"][0] - r1["S"], axis=1).max() / diag < 1e-6
