@@ -384,6 +384,8 @@ def run_ours_batched(args):
     # results never depend on them)
     _, Vb, Fb, Sb = max(meshes, key=lambda x: x[3].shape[0])
     prm, tune_ms = workloads.tune_for(Vb, Fb, Sb, k=K, mode=mode, profile=PROFILE)
+    if args.no_reuse:
+        prm.knn_reuse = 0
     M = [E.Mesh(V, F) for _, V, F, _ in meshes]
     cells = sum(E.grid_cells(m, S.shape[0], K) for m, (*_, S) in zip(M, meshes))
     eng = E.Engine(prm, len(M), n_mine, cells)
@@ -470,6 +472,9 @@ def run_ours_batched(args):
     # ---- per-kernel timing over one whole batched remesh ----------------
     reset()
     prof = eng.profile(iters, sp)
+    big = sorted(range(len(segs)), key=lambda j: -int(meshes[j][3].shape[0]))[:8]
+    reuse = knn_reuse_share(eng, [segs[j] for j in big], iters)
+    reuse["over"] = "the 8 meshes with the most sites, one whole remesh"
     groups = {"k_site_knn": (prof["knn"], n_mine * knn_bytes_per_site(K)),
               "k_site_clip": (prof["clip"], n_mine * clip_bytes_per_site(K)),
               "k_site_proj": (prof["proj"], n_mine * proj_bytes_per_site(K))}
@@ -512,7 +517,7 @@ def run_ours_batched(args):
     # ---- 1M sites on the jittered rounded box (rank 0) ---------------------
     c3 = None
     if rank == 0 and not args.no_c3:
-        c3 = c3_figures(peak, peak_kind)
+        c3 = c3_figures(peak, peak_kind, reuse=not args.no_reuse)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -542,7 +547,7 @@ def run_ours_batched(args):
                         "api": "cvt_remesh_batch (pinned host buffers; mesh ingest, upload, iterations, download)",
                         "same_sites_as_engine": same_as_engine},
                 "gpu_launches": int(sum(launches)),
-                "roofline": roofline, "issue_roofline": ir, "superellipsoid_1m": c3,
+                "roofline": roofline, "issue_roofline": ir, "knn_reuse": reuse, "superellipsoid_1m": c3,
                 "cpu_baseline": cpu, "accuracy": acc, "clocks": clk,
                 "tiles": E.tiles(prm), "tune_ms_per_iter": tune_ms, "mesh_generation_s": gen_s,
                 "libgpucvt_launches_total": _lib.launch_count()}
@@ -554,7 +559,19 @@ def run_ours_batched(args):
     return 0
 
 
-def c3_figures(peak, peak_kind, iters=200, k=32):
+def knn_reuse_share(eng, segs, iters):
+    """Share of the site KNN lists taken from the kept candidate lists (the
+    rest were full searches) over the segments' last `iters` iterations."""
+    r = s = 0
+    for g in segs:
+        for i in range(iters):
+            st = eng.stats(g, i)
+            r += st["knn_reused"]
+            s += st["knn_searched"]
+    return {"reused": r, "searched": s, "share": r / max(r + s, 1)}
+
+
+def c3_figures(peak, peak_kind, iters=200, k=32, reuse=True):
     """1M area-uniform sites on the rounded box |x|^8+|y|^8+|z|^8=1 (~2M
     triangles, 1% jittered by 1e-3), K=32, 200 iterations, freezing on,
     mixed profile: remesh time, KNN + clip time per iteration and its HBM
@@ -566,7 +583,7 @@ def c3_figures(peak, peak_kind, iters=200, k=32):
     n = S0.shape[0]
     M = E.Mesh(m.V, m.F)
     cells = E.grid_cells(M, n, k)
-    eng = E.Engine(E.params(k=k, mode=1, profile=PROFILE), 1, n, cells)
+    eng = E.Engine(E.params(k=k, mode=1, profile=PROFILE, knn_reuse=reuse), 1, n, cells)
     st = torch.cuda.current_stream()
     sp = st.cuda_stream
     g = eng.add(M, S0, sp)
@@ -587,6 +604,7 @@ def c3_figures(peak, peak_kind, iters=200, k=32):
     eng.remove(g)
     g = eng.add(M, S0, sp)
     whole = eng.profile(iters, sp)
+    reuse = knn_reuse_share(eng, [g], iters)
     eng.close()
     M.close()
     b = n * (knn_bytes_per_site(k) + clip_bytes_per_site(k))
@@ -599,7 +617,9 @@ def c3_figures(peak, peak_kind, iters=200, k=32):
             "knn_clip_hbm_frac_all_active": b / (kc_first * 1e-3) / 1e9 / peak,
             "knn_clip_bytes_per_site": knn_bytes_per_site(k) + clip_bytes_per_site(k),
             "peak_gbs": peak, "peak_source": peak_kind,
-            "stage_ms_per_iter_all_active": {k_: round(v, 5) for k_, v in first.items()}}
+            "stage_ms_per_iter_all_active": {k_: round(v, 5) for k_, v in first.items()},
+            "stage_ms_per_iter_run_average": {k_: round(v, 5) for k_, v in whole.items()},
+            "knn_reuse": reuse}
 
 
 def run_ours_torus(args):
@@ -814,6 +834,7 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="batched: skip the plain per-mesh loop")
     ap.add_argument("--no-c3", action="store_true", help="batched: skip the 1M-site rounded-box figures")
+    ap.add_argument("--no-reuse", action="store_true", help="full KNN searches every iteration (knn_reuse off)")
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--hbm-gb", type=int, default=4)
     args = ap.parse_args()

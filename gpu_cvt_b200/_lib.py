@@ -40,7 +40,7 @@ class EvalOut(C.Structure):
 
 class IterStats(C.Structure):
     _fields_ = [("same", i32), ("low", i32), ("both", i32), ("newly_frozen", i32), ("max_motion", f32),
-                ("iter", i32)]
+                ("iter", i32), ("knn_reused", i32), ("knn_searched", i32)]
 
 
 # name -> argtypes (all return cvt_status_t unless listed in _RESTYPES)

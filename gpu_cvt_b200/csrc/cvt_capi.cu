@@ -1073,6 +1073,9 @@ struct cvt_engine {
   float* d_cand_r2 = nullptr;
   float* d_cand_D = nullptr;
   unsigned long long* d_blockmax = nullptr;  // per cell slot: coarse-block motion of the last step
+  int* d_vcand = nullptr;                     // centroid -> vertex candidate lists (kVCand per site)
+  void* d_vcand_c = nullptr;
+  float* d_vcand_r2 = nullptr;
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   // fork / join of the frame-vertex search, which runs on a second stream
@@ -1239,6 +1242,9 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
     ar.add(&e->d_cand_r2, ns);
     ar.add(&e->d_cand_D, ns);
     ar.add(&e->d_blockmax, (size_t)max_cells);
+    ar.add(&e->d_vcand, (size_t)kVCand * ns);
+    ar.add(reinterpret_cast<char**>(&e->d_vcand_c), tsz * 3 * ns);
+    ar.add(&e->d_vcand_r2, ns);
   }
   ECK(ar.commit(&e->arena));
   e->bytes = ar.size;
@@ -1339,6 +1345,8 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   if (e->d_cand_r2) {  // no candidate lists yet; no motion recorded in the segment's blocks
     k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_cand_r2) + base, n, (int)0xbf800000);
     CKLAUNCH();
+    k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_vcand_r2) + base, n, (int)0xbf800000);
+    CKLAUNCH();
     CK(cudaMemsetAsync(e->d_blockmax + cbase, 0, sizeof(unsigned long long) * (size_t)cells, st));
   }
   CK(cudaMemsetAsync(e->d_stats + (size_t)s * kStatsRing * kStatsWords, 0, sizeof(int) * kStatsRing * kStatsWords, st));
@@ -1376,6 +1384,7 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   a.stats = e->d_stats; a.ovf = e->d_ovf; a.far = e->d_far; a.cent = (T*)e->d_cent; a.K = e->K;
   a.proj_mode = e->p.proj_mode; a.bvh_ovf = reinterpret_cast<int*>(e->d_tickets + 2);
   a.cand = e->d_cand; a.cand_r2 = e->d_cand_r2; a.cand_D = e->d_cand_D; a.blockmax = e->d_blockmax;
+  a.vcand = e->d_vcand; a.vcand_c = (T*)e->d_vcand_c; a.vcand_r2 = e->d_vcand_r2;
   return a;
 }
 
@@ -1666,6 +1675,8 @@ extern "C" cvt_status_t cvt_engine_get_stats(cvt_engine_t e, int s, int iter, cv
   std::memcpy(&d2, &w[4], sizeof(float));
   out->max_motion = std::sqrt(d2);
   out->iter = w[5];
+  out->knn_reused = w[6];
+  out->knn_searched = w[7];
   return CVT_OK;
 }
 

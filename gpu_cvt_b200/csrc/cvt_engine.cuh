@@ -34,7 +34,7 @@
 namespace cvt {
 
 constexpr int kStatsRing = 256;   // iterations of per-segment statistics kept
-constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter, -, -
+constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter, KNN lists reused, searched
 constexpr int kKProj = 5;         // KPROJ (main.cu:394)
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
 // threads per SM that k_site_clip's launch bounds ask to keep resident: it
@@ -111,6 +111,9 @@ template <class T> struct EngineArgs {
   float* cand_r2;    // its MM-th squared distance when it was built (< 0: no list; inf: every other site)
   float* cand_D;     // motion bound accumulated since it was built (k_site_knn)
   unsigned long long* blockmax;  // per coarse block (cell slots of the segment): iteration << 32 | max motion bits
+  int* vcand;        // per site: the kVCand vertices nearest to its centroid at the last full search (site_proj)
+  T* vcand_c;        // that centroid (3 values)
+  float* vcand_r2;   // the kVCand-th squared distance (< 0: no list; inf: fewer vertices than kVCand)
 };
 
 // Coarse motion blocks of a segment: 4 x 4 x 4 grid cells, stored in the
@@ -421,18 +424,18 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
 // segment's first iteration) the full search runs for MM neighbours and
 // refreshes the list.  Margins of 1e-4 cover the rounding of the distances
 // and of the accumulated motion; a NaN motion fails every test.
-template <class T, int KK, int MM, int BS>
-__global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
+// The K-list of active site w (one warp); true when it came from the
+// candidate list.  seg receives the site's segment.
+template <class T, int KK, int MM>
+__device__ __forceinline__ bool knn_site(const EngineArgs<T>& a, int parity, int w, int lane, int& seg) {
   static_assert(KK <= 32, "one list entry per lane");
   static_assert(MM == 0 || (MM > KK && MM <= 64 && MM % 2 == 0), "candidate list of KK < MM <= 64 (even) entries");
   using O = KeyOps<T>;
   using Key = typename O::Key;
-  const int lane = threadIdx.x & 31;
-  const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-  if (w >= __ldg(a.act_count)) return;  // whole warp
   const Pt4<T> me = a.sorted[a.act[w]];
   const int g = (int)me.id;
   const int s = __ldg(a.site_seg + g);
+  seg = s;
   const SegDev& sd = a.segs[s];
   // The K nearest other sites: the reference's K+1 nearest with self dropped
   // (site_knn.cuh:79-103) are exactly these, also when duplicates of the site
@@ -545,6 +548,39 @@ __global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
   }
   const unsigned changed = __ballot_sync(0xffffffffu, diff);
   if (lane == 0) a.same[g] = changed ? 0 : 1;
+  return have;
+}
+
+// One warp per active site; the block then adds its lists taken from the
+// candidate lists and its full searches to the segments' statistics (words
+// 6 and 7 of the iteration's slot), one atomic per run of warps of the same
+// segment.
+template <class T, int KK, int MM, int BS>
+__global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
+  __shared__ int wseg[BS / 32];
+  __shared__ int wuse[BS / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  int seg = -1;
+  bool reused = false;
+  if (w < __ldg(a.act_count)) reused = knn_site<T, KK, MM>(a, parity, w, lane, seg);
+  if (lane == 0) { wseg[wid] = seg; wuse[wid] = reused ? 1 : 0; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int cur = -1, nr = 0, ns = 0;
+    auto flush = [&]() {
+      if (cur < 0) return;
+      int* sl = a.stats + ((size_t)cur * kStatsRing + (a.segs[cur].iter % kStatsRing)) * kStatsWords;
+      if (nr) atomicAdd(sl + 6, nr);
+      if (ns) atomicAdd(sl + 7, ns);
+    };
+    for (int i = 0; i < BS / 32; ++i) {
+      if (wseg[i] < 0) continue;
+      if (wseg[i] != cur) { flush(); cur = wseg[i]; nr = ns = 0; }
+      if (wuse[i]) ++nr; else ++ns;
+    }
+    flush();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -700,6 +736,8 @@ __device__ __forceinline__ void site_finish(const EngineArgs<typename PT<PROF>::
 // is handed to k_site_far (a centroid far off the surface, e.g. of a cell
 // that the neighbours leave almost unbounded in the first iteration).
 constexpr int kVertexRingLimit = 4;
+// vertices kept per site for the centroid -> vertex search (knn_reuse)
+constexpr int kVCand = 8;
 
 // Everything after the centroid; false when the 5-NN search was deferred
 // (the site is then listed in a.far and finished by k_site_far).
@@ -720,15 +758,65 @@ __device__ __forceinline__ bool site_proj(const EngineArgs<typename PT<PROF>::T>
   int knnv[kKProj];
   if (!fz) {
     const int skip = (sd.mode == 0 && sd.ex_quirk) ? g - sd.site_base : -1;
-    TopK<T, kKProj> top;
-    if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, ld3((const T*)a.cent, g), top,
-                                    [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
-      const int k = atomicAdd(a.far, 1);
-      a.far[1 + k] = g;
-      return false;
-    }
+    const V3<T> c = ld3((const T*)a.cent, g);
+    bool have = false;
+    if (a.vcand) {
+      // the kVCand vertices nearest to the centroid of the last full search:
+      // mesh vertices do not move, so one outside that list is still
+      // farther than rho - |c - c_build|; when the 5th nearest of the list
+      // is closer than that, the list's first 5 are the 5 nearest of all
+      // (the same keys as the grid search; 1e-4 margins for rounding)
+      const float r2b = a.vcand_r2[g];
+      if (r2b >= 0.f && finite3(c)) {
+        TopK<T, kKProj> top;
+        const int* vc = a.vcand + (size_t)g * kVCand;
 #pragma unroll
-    for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
+        for (int k = 0; k < kVCand; ++k) {
+          const int v = __ldg(vc + k);
+          if (v < 0) continue;
+          const T d = dist2(V3<T>{(T)__ldg(md.V + 3 * v), (T)__ldg(md.V + 3 * v + 1), (T)__ldg(md.V + 3 * v + 2)}, c);
+          if (d <= top.worst_d()) top.insert(KeyOps<T>::make(d, (uint32_t)v));
+        }
+        const V3<T> cb = ld3((const T*)a.vcand_c, g);
+        const double delta = sqrt((double)dist2(cvt3<double>(c), cvt3<double>(cb)));
+        const double k5 = sqrt((double)top.worst_d());
+        have = top.full() && (isinf(r2b) || k5 * 1.0001 + delta * 1.0001 < sqrt((double)r2b) * 0.9999);
+        if (have) {
+#pragma unroll
+          for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
+        }
+      }
+    }
+    if (!have && a.vcand) {
+      // full search for kVCand vertices; refreshes the list
+      TopK<T, kVCand> top;
+      if (!grid_knn<T, float, kVCand>(md.vg, md.vcell_start, md.vsorted, c, top,
+                                      [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
+        a.vcand_r2[g] = -1.f;
+        const int k = atomicAdd(a.far, 1);
+        a.far[1 + k] = g;
+        return false;
+      }
+      int* vc = a.vcand + (size_t)g * kVCand;
+#pragma unroll
+      for (int k = 0; k < kVCand; ++k) {
+        const int v = KeyOps<T>::is_empty(top.k[k]) ? -1 : (int)KeyOps<T>::idx(top.k[k]);
+        vc[k] = v;
+        if (k < kKProj) { knnv[k] = v; kv[k] = v; }
+      }
+      st3((T*)a.vcand_c, g, c);
+      a.vcand_r2[g] = top.full() ? (float)top.worst_d() : __int_as_float(0x7f800000);
+    } else if (!have) {
+      TopK<T, kKProj> top;
+      if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, c, top,
+                                      [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
+        const int k = atomicAdd(a.far, 1);
+        a.far[1 + k] = g;
+        return false;
+      }
+#pragma unroll
+      for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
+    }
   } else {
 #pragma unroll
     for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];

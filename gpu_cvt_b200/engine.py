@@ -195,7 +195,7 @@ class Engine:
         s = IterStats()
         call("cvt_engine_get_stats", self.handle, int(seg), int(it), C.byref(s), None)
         return dict(same=s.same, low=s.low, both=s.both, newly_frozen=s.newly_frozen, max_motion=s.max_motion,
-                    iter=s.iter)
+                    iter=s.iter, knn_reused=s.knn_reused, knn_searched=s.knn_searched)
 
     def iters(self, seg: int) -> int:
         v = C.c_int()

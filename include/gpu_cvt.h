@@ -296,11 +296,14 @@ cvt_status_t cvt_autotune(cvt_mesh_t mesh, const float* sites, int n_sites, int 
 typedef struct cvt_engine* cvt_engine_t;
 
 /* Per-segment statistics of one iteration (freezetest.cuh counts +
- * motion).  max_motion is the largest site displacement (not squared). */
+ * motion).  max_motion is the largest site displacement (not squared).
+ * knn_reused / knn_searched: site KNN lists taken from the kept candidate
+ * lists / found by a full search (knn_reuse). */
 typedef struct {
   int same, low, both, newly_frozen;
   float max_motion;
   int iter;
+  int knn_reused, knn_searched;
 } cvt_iter_stats_t;
 
 /* Grid cells a segment of n_sites sites on `mesh` reserves with params p

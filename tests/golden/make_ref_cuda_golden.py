@@ -164,6 +164,40 @@ def torus_100k_iters(out, r=None, ours=None):
                         S=r["S"][iters - 1][:, idx], tie=tie, diag=np.float64(diag))
 
 
+def superellipsoid_1m(out, iters=10):
+    """The 1M-site rounded box (K=32, mode 1): iterations 1..iters by the
+    reference's kernels against the engine's ref and mixed profiles (per
+    iteration max / p99 / mean drift and sites above 1e-5 of the diagonal)
+    and the one-sided Hausdorff figure after them; added to
+    ref_cuda_summary.json as "superellipsoid_1m"."""
+    from gpu_cvt_b200 import engine as E
+    m = mg.superellipsoid(8.0, 2_000_000, 0.01, 1e-3, seed=2)
+    S = mg.sample_sites(m.V, m.F, 1_000_000, seed=2)
+    diag = mg.bbox_diag(m.V)
+    r = ref_runner.run(m.V, m.F, S, 32, 1, iters, dump=list(range(1, iters + 1)), timeout=3000)
+    M = E.Mesh(m.V, m.F)
+    res = {"sites": int(S.shape[0]), "k": 32, "mode": 1, "iters": iters,
+           "reference_cuda_dH_rel": r["dH"] / diag, "reference_frozen_end": int(r["frozen"].sum())}
+    for prof in ("ref", "mixed"):
+        e = E.Engine(E.params(k=32, mode=1, profile=prof), 1, S.shape[0], E.grid_cells(M, S.shape[0], 32))
+        g = e.add(M, S)
+        rows = []
+        for it in range(iters):
+            e.run(1)
+            d = np.linalg.norm(e.sites(g).astype(np.float64) - r["S"][it].astype(np.float64), axis=1) / diag
+            d = d[np.isfinite(d)]
+            rows.append({"iter": it + 1, "max": float(d.max()), "p99": float(np.percentile(d, 99)),
+                         "mean": float(d.mean()), "n_over_1e-5": int((d > 1e-5).sum())})
+        res[prof] = {"drift_vs_reference_cuda": rows, "dH_rel": e.evaluate(g)["dH_rel"],
+                     "frozen_end": int(e.state(g)["frozen"].sum())}
+        e.close()
+    path = os.path.join(out, "ref_cuda_summary.json")
+    summ = json.load(open(path)) if os.path.exists(path) else {}
+    summ["superellipsoid_1m"] = res
+    with open(path, "w") as fh:
+        json.dump(summ, fh, indent=1)
+
+
 def main(out):
     os.makedirs(out, exist_ok=True)
     if not ref_runner.available():
@@ -171,6 +205,7 @@ def main(out):
     small_cases(out)
     torus_100k(out)
     torus_100k_iters(out)
+    superellipsoid_1m(out)
 
 
 if __name__ == "__main__":
