@@ -475,7 +475,7 @@ def run_ours_batched(args):
     big = sorted(range(len(segs)), key=lambda j: -int(meshes[j][3].shape[0]))[:8]
     reuse = knn_reuse_share(eng, [segs[j] for j in big], iters)
     reuse["over"] = "the 8 meshes with the most sites, one whole remesh"
-    groups = {"k_site_knn": (prof["knn"], n_mine * knn_bytes_per_site(K)),
+    groups = {"site_knn (k_knn_verify + k_knn_search)": (prof["knn"], n_mine * knn_bytes_per_site(K)),
               "k_site_clip": (prof["clip"], n_mine * clip_bytes_per_site(K)),
               "k_site_proj": (prof["proj"], n_mine * proj_bytes_per_site(K))}
     dom = max(groups, key=lambda g: groups[g][0])

@@ -1070,12 +1070,12 @@ struct cvt_engine {
   int num_sms = 148;
   void* d_cent = nullptr;
   uint32_t* d_cand = nullptr;   // candidate lists (knn_reuse): cand_len(K) global ids per site
-  float* d_cand_r2 = nullptr;
+  float* d_cand_rho = nullptr;
   float* d_cand_D = nullptr;
+  int* d_srch = nullptr;          // sites left for a full KNN search, srch_cap slots per verify warp
+  int* d_srch_n = nullptr;
+  int srch_cap = 0;
   unsigned long long* d_blockmax = nullptr;  // per cell slot: coarse-block motion of the last step
-  int* d_vcand = nullptr;                     // centroid -> vertex candidate lists (kVCand per site)
-  void* d_vcand_c = nullptr;
-  float* d_vcand_r2 = nullptr;
   // graphs
   cudaGraphExec_t gexec[2] = {nullptr, nullptr};
   // fork / join of the frame-vertex search, which runs on a second stream
@@ -1239,12 +1239,12 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
   ar.add(reinterpret_cast<char**>(&e->d_cent), tsz * 3 * ns);
   if (q.knn_reuse) {
     ar.add(&e->d_cand, (size_t)cand_len(e->K) * ns);
-    ar.add(&e->d_cand_r2, ns);
+    ar.add(&e->d_cand_rho, ns);
     ar.add(&e->d_cand_D, ns);
+    e->srch_cap = (int)cdiv((long)ns, (long)e->num_sms * kKnnVerifyWarpsPerSM);
+    ar.add(&e->d_srch, (size_t)e->srch_cap * e->num_sms * kKnnVerifyWarpsPerSM);
+    ar.add(&e->d_srch_n, (size_t)e->num_sms * kKnnVerifyWarpsPerSM);
     ar.add(&e->d_blockmax, (size_t)max_cells);
-    ar.add(&e->d_vcand, (size_t)kVCand * ns);
-    ar.add(reinterpret_cast<char**>(&e->d_vcand_c), tsz * 3 * ns);
-    ar.add(&e->d_vcand_r2, ns);
   }
   ECK(ar.commit(&e->arena));
   e->bytes = ar.size;
@@ -1342,10 +1342,8 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   CK(cudaMemsetAsync(e->d_same + base, 0, n, st));
   k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_kth) + base, n, (int)0xbf800000);  // -1.0f
   CKLAUNCH();
-  if (e->d_cand_r2) {  // no candidate lists yet; no motion recorded in the segment's blocks
-    k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_cand_r2) + base, n, (int)0xbf800000);
-    CKLAUNCH();
-    k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_vcand_r2) + base, n, (int)0xbf800000);
+  if (e->d_cand_rho) {  // no candidate lists yet; no motion recorded in the segment's blocks
+    k_fill_int<<<cdiv(n, 256), 256, 0, st>>>(reinterpret_cast<int*>(e->d_cand_rho) + base, n, (int)0xbf800000);
     CKLAUNCH();
     CK(cudaMemsetAsync(e->d_blockmax + cbase, 0, sizeof(unsigned long long) * (size_t)cells, st));
   }
@@ -1383,24 +1381,39 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
   a.stats = e->d_stats; a.ovf = e->d_ovf; a.far = e->d_far; a.cent = (T*)e->d_cent; a.K = e->K;
   a.proj_mode = e->p.proj_mode; a.bvh_ovf = reinterpret_cast<int*>(e->d_tickets + 2);
-  a.cand = e->d_cand; a.cand_r2 = e->d_cand_r2; a.cand_D = e->d_cand_D; a.blockmax = e->d_blockmax;
-  a.vcand = e->d_vcand; a.vcand_c = (T*)e->d_vcand_c; a.vcand_r2 = e->d_vcand_r2;
+  a.cand = e->d_cand; a.cand_rho = e->d_cand_rho; a.cand_D = e->d_cand_D; a.srch = e->d_srch; a.srch_n = e->d_srch_n; a.srch_cap = e->srch_cap; a.blockmax = e->d_blockmax;
   return a;
 }
 
+// the site KNN: with candidate lists, the check (one warp per active site)
+// and then the full searches of the sites it left (a grid-stride kernel);
+// without, the full searches of every active site.  Returns the launches.
+template <class T, int KK, int MM, int BS>
+static int launch_site_knn_b(const EngineArgs<T>& a, int parity, int nsites, int nsm, cudaStream_t st) {
+  (void)nsites;
+  const int vgrid = nsm * (kKnnVerifyWarpsPerSM * 32 / BS);  // the shape a.srch_cap is sized for
+  int L = 0;
+  if constexpr (MM > 0) {
+    k_knn_verify<T, KK, MM, BS><<<vgrid, BS, 0, st>>>(a, parity);
+    L++;
+  }
+  k_knn_search<T, KK, MM, BS><<<nsm * (kKnnSearchWarpsPerSM * 32 / BS), BS, 0, st>>>(a, parity,
+                                                                                    nsm * kKnnVerifyWarpsPerSM);
+  return L + 1;
+}
+
 template <class T, int KK, int MM>
-static void launch_site_knn_m(const EngineArgs<T>& a, int parity, int nsites, int bs, cudaStream_t st) {
-  // one warp per site
-  const int nb = cdiv((long)nsites * 32, bs);
-  if (bs == 64) k_site_knn<T, KK, MM, 64><<<nb, 64, 0, st>>>(a, parity);
-  else if (bs == 256) k_site_knn<T, KK, MM, 256><<<nb, 256, 0, st>>>(a, parity);
-  else k_site_knn<T, KK, MM, 128><<<nb, 128, 0, st>>>(a, parity);
+static int launch_site_knn_m(const EngineArgs<T>& a, int parity, int nsites, int bs, int nsm, cudaStream_t st) {
+  if (bs == 64) return launch_site_knn_b<T, KK, MM, 64>(a, parity, nsites, nsm, st);
+  if (bs == 256) return launch_site_knn_b<T, KK, MM, 256>(a, parity, nsites, nsm, st);
+  return launch_site_knn_b<T, KK, MM, 128>(a, parity, nsites, nsm, st);
 }
 
 template <class T, int KK>
-static void launch_site_knn(const EngineArgs<T>& a, int parity, int nsites, int bs, bool reuse, cudaStream_t st) {
-  if (reuse) launch_site_knn_m<T, KK, cand_len(KK)>(a, parity, nsites, bs, st);
-  else launch_site_knn_m<T, KK, 0>(a, parity, nsites, bs, st);
+static int launch_site_knn(const EngineArgs<T>& a, int parity, int nsites, int bs, bool reuse, int nsm,
+                           cudaStream_t st) {
+  if (reuse) return launch_site_knn_m<T, KK, cand_len(KK)>(a, parity, nsites, bs, nsm, st);
+  return launch_site_knn_m<T, KK, 0>(a, parity, nsites, bs, nsm, st);
 }
 
 template <int PROF, int FRAME>
@@ -1481,15 +1494,15 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   L++;
   if (ev) CK(cudaEventRecord(ev[1], st));
   const bool reuse = e->p.knn_reuse != 0;
+  const int nsm = e->num_sms;
   switch (e->K) {
-    case 8: launch_site_knn<T, 8>(a, parity, ns, e->p.knn_block, reuse, st); break;
-    case 12: launch_site_knn<T, 12>(a, parity, ns, e->p.knn_block, reuse, st); break;
-    case 16: launch_site_knn<T, 16>(a, parity, ns, e->p.knn_block, reuse, st); break;
-    case 20: launch_site_knn<T, 20>(a, parity, ns, e->p.knn_block, reuse, st); break;
-    case 24: launch_site_knn<T, 24>(a, parity, ns, e->p.knn_block, reuse, st); break;
-    default: launch_site_knn<T, 32>(a, parity, ns, e->p.knn_block, reuse, st); break;
+    case 8: L += launch_site_knn<T, 8>(a, parity, ns, e->p.knn_block, reuse, nsm, st); break;
+    case 12: L += launch_site_knn<T, 12>(a, parity, ns, e->p.knn_block, reuse, nsm, st); break;
+    case 16: L += launch_site_knn<T, 16>(a, parity, ns, e->p.knn_block, reuse, nsm, st); break;
+    case 20: L += launch_site_knn<T, 20>(a, parity, ns, e->p.knn_block, reuse, nsm, st); break;
+    case 24: L += launch_site_knn<T, 24>(a, parity, ns, e->p.knn_block, reuse, nsm, st); break;
+    default: L += launch_site_knn<T, 32>(a, parity, ns, e->p.knn_block, reuse, nsm, st); break;
   }
-  L++;
   if (ev) CK(cudaEventRecord(ev[2], st));
   CK(cudaStreamWaitEvent(st, br.join, 0));
   launch_site_clip<PROF>(a, parity, ns, e->p.clip_block, e->p.frame_mode, e->num_sms, st);

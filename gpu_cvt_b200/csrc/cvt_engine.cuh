@@ -5,10 +5,12 @@
 //   k_active_list  the non-frozen sites
 //   k_frame_vertex the mesh vertex nearest to each of them (its normal
 //                gives the frame, main.cu:685-700), on a second stream
-//                while k_site_knn runs
-//   k_site_knn   per active site (one warp): exact (K+1)-NN in its segment,
-//                drop self (site_knn.cuh:79); frozen sites keep the
-//                previous list (main.cu:678)
+//                while the site KNN runs
+//   k_knn_verify per active site (one warp): the K-list from the site's
+//                candidate list where its motion bound proves it exact
+//   k_knn_search the other active sites (one warp each): exact (K+1)-NN in
+//                the segment, drop self (site_knn.cuh:79); frozen sites
+//                keep the previous list (main.cu:678)
 //   k_site_clip  per site (one thread): frame (site_normals.cuh:69; or,
 //                as an option, from the PCA normal of the neighbours),
 //                tangent-plane clip and centroid (2dClip.cuh:82)
@@ -107,14 +109,19 @@ template <class T> struct EngineArgs {
   int K;
   int proj_mode;  // 0: one-ring of the KPROJ nearest vertices; 1: closest point through the BVH
   int* bvh_ovf;   // BVH traversal stack overflows (never expected: the tree depth is bounded)
-  uint32_t* cand;    // candidate list per site (global ids), MM entries (k_site_knn)
-  float* cand_r2;    // its MM-th squared distance when it was built (< 0: no list; inf: every other site)
-  float* cand_D;     // motion bound accumulated since it was built (k_site_knn)
+  uint32_t* cand;    // candidate list per site (global ids), MM entries (k_knn_verify / k_knn_search)
+  float* cand_rho;   // its MM-th distance when it was built, rounded down (< 0: no list; inf: every other site)
+  float* cand_D;     // motion bound accumulated since it was built (k_knn_verify)
+  int* srch;         // per verify warp: srch_cap slots of sorted positions left for a full search
+  int* srch_n;       // per verify warp: slots used
+  int srch_cap;
   unsigned long long* blockmax;  // per coarse block (cell slots of the segment): iteration << 32 | max motion bits
-  int* vcand;        // per site: the kVCand vertices nearest to its centroid at the last full search (site_proj)
-  T* vcand_c;        // that centroid (3 values)
-  float* vcand_r2;   // the kVCand-th squared distance (< 0: no list; inf: fewer vertices than kVCand)
 };
+
+__device__ __forceinline__ float f32_ru(float x) { return x; }
+__device__ __forceinline__ float f32_ru(double x) { return __double2float_ru(x); }
+__device__ __forceinline__ float f32_rd(float x) { return x; }
+__device__ __forceinline__ float f32_rd(double x) { return __double2float_rd(x); }
 
 // Coarse motion blocks of a segment: 4 x 4 x 4 grid cells, stored in the
 // first cells of the segment's cell range (there are fewer blocks than
@@ -386,7 +393,7 @@ __global__ void __launch_bounds__(kActiveListThreads) k_active_list(EngineArgs<T
 // k_frame_vertex: each listed site's nearest mesh vertex (the frame vertex,
 // main.cu:685-700), one thread per site: the same exact grid search and key
 // order as any other, so the same vertex.  Runs on a second stream while
-// k_site_knn runs; k_site_clip is the first kernel to read a.nnv.
+// site KNN runs; k_site_clip is the first kernel to read a.nnv.
 // ---------------------------------------------------------------------------
 template <class T>
 __global__ void k_frame_vertex(EngineArgs<T> a) {
@@ -402,11 +409,11 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
-// k_site_knn: one warp per active site.  Exact K nearest other sites within
-// its segment (the reference's K+1 nearest with self dropped,
-// site_knn.cuh:79-103); lane j holds the j-th neighbour, so the list row is
-// read (for the freeze test's equality) and written coalesced.
-// Sets same[g] (new list == stored list) and kth[g].
+// Site KNN (k_knn_verify + k_knn_search): exact K nearest other sites
+// within the site's segment (the reference's K+1 nearest with self dropped,
+// site_knn.cuh:79-103), one warp per site; lane j holds the j-th neighbour,
+// so the list row is read (for the freeze test's equality) and written
+// coalesced.  Sets same[g] (new list == stored list) and kth[g].
 // ---------------------------------------------------------------------------
 // Candidate lists (MM > 0): besides its K neighbours, a site keeps the MM
 // nearest other sites of its last full search (ids and the MM-th squared
@@ -424,15 +431,109 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
 // segment's first iteration) the full search runs for MM neighbours and
 // refreshes the list.  Margins of 1e-4 cover the rounding of the distances
 // and of the accumulated motion; a NaN motion fails every test.
-// The K-list of active site w (one warp); true when it came from the
-// candidate list.  seg receives the site's segment.
+// The K-list of site g: lane j holds entry j (its key); writes the list
+// (local indices; only entries that changed), the K-th squared distance
+// (the next search's bound) and the `same` flag (list unchanged).
+template <class T, int KK>
+__device__ __forceinline__ void knn_store(const EngineArgs<T>& a, int g, const SegDev& sd,
+                                          typename KeyOps<T>::Key key, int lane) {
+  using O = KeyOps<T>;
+  const auto kth = shfl_key(key, KK - 1);
+  if (lane == 0) a.kth[g] = O::is_empty(kth) ? -1.f : (float)O::dist(kth);
+  const uint32_t gid = O::idx(key);
+  const uint32_t out = gid == 0xffffffffu ? 0xffffffffu : gid - (uint32_t)sd.site_base;
+  uint32_t* row = a.knn + (size_t)g * KK;
+  bool diff = false;
+  if (lane < KK) {
+    diff = row[lane] != out;
+    if (diff) row[lane] = out;
+  }
+  const unsigned changed = __ballot_sync(0xffffffffu, diff);
+  if (lane == 0) a.same[g] = changed ? 0 : 1;
+}
+
+// Candidate-list check of active site w (one warp): true when the K-list
+// came from the list (and is stored); false when the site needs a full
+// search.  seg receives the site's segment.
 template <class T, int KK, int MM>
-__device__ __forceinline__ bool knn_site(const EngineArgs<T>& a, int parity, int w, int lane, int& seg) {
+__device__ __forceinline__ bool knn_verify_site(const EngineArgs<T>& a, int parity, int w, int lane, int& seg) {
   static_assert(KK <= 32, "one list entry per lane");
-  static_assert(MM == 0 || (MM > KK && MM <= 64 && MM % 2 == 0), "candidate list of KK < MM <= 64 (even) entries");
+  static_assert(MM > KK && MM <= 64 && MM % 2 == 0, "candidate list of KK < MM <= 64 (even) entries");
   using O = KeyOps<T>;
   using Key = typename O::Key;
   const Pt4<T> me = a.sorted[a.act[w]];
+  const int g = (int)me.id;
+  const int s = __ldg(a.site_seg + g);
+  seg = s;
+  const float rho = a.cand_rho[g];
+  if (!(rho >= 0.f)) return false;
+  const SegDev& sd = a.segs[s];
+  const V3<T> q{me.x, me.y, me.z};
+  // the motion bound of the last step: this site's own motion, the largest
+  // motion in the 27 coarse blocks around its old position (lane b < 27
+  // reads block b), and the step condition that no site from beyond those
+  // blocks reached the list's radius in one step
+  const GridGeom G = a.geom[s];
+  const V3<T> prev = ld3(a.S[parity ^ 1], g);
+  int bx, by, bz;
+  motion_block(G, prev, bx, by, bz);
+  unsigned mbits = 0u;
+  if (lane < 27) {
+    const int x = bx + lane % 3 - 1, y = by + (lane / 3) % 3 - 1, z = bz + lane / 9 - 1;
+    const int dx = (G.dim[0] + 3) >> 2, dy = (G.dim[1] + 3) >> 2, dz = (G.dim[2] + 3) >> 2;
+    if (x >= 0 && x < dx && y >= 0 && y < dy && z >= 0 && z < dz) {
+      const unsigned long long v = a.blockmax[G.cell_base + (z * dy + y) * dx + x];
+      if ((unsigned)(v >> 32) == (unsigned)(sd.iter - 1)) mbits = (unsigned)v;
+    }
+  }
+  mbits = __reduce_max_sync(0xffffffffu, mbits);
+  // FP32 with upward rounding; the 1e-4 margins below are far above it
+  const float mu_i = __fsqrt_ru(f32_ru(dist2(q, prev)));
+  const float D = __fadd_ru(a.cand_D[g], __fadd_ru(mu_i, __uint_as_float(mbits)));
+  const bool step_ok = __fadd_ru(sd.step_motion, mu_i) * 1.0001f < (4.f * G.h - rho) * 0.9999f;
+  if (!isinf(rho) && !step_ok) return false;
+  // re-key the list at the current positions and select its KK smallest
+  // in order (element e = 2 lane + r)
+  const uint32_t* cr = a.cand + (size_t)g * MM;
+  const T* S = a.S[parity];
+  Key k2[2];
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int e = 2 * lane + r;
+    k2[r] = O::empty();
+    if (e < MM) {
+      const uint32_t id = __ldg(cr + e);
+      if (id != 0xffffffffu) k2[r] = O::make(dist2(ld3(S, (long)id), q), id);
+    }
+  }
+  const bool moved = warp_select_pairs<T, KK>(k2[0], k2[1], lane);
+  // entry j to lane j
+  const Key e0 = shfl_key(k2[0], lane >> 1), e1 = shfl_key(k2[1], lane >> 1);
+  const Key key = (lane & 1) ? e1 : e0;
+  const Key kth = shfl_key(key, KK - 1);
+  const float kap = __fsqrt_ru(f32_ru(O::dist(kth)));
+  if (O::is_empty(kth) || !(isinf(rho) || kap * 1.0001f + D * 1.0001f < rho * 0.9999f)) return false;
+  if (lane == 0) a.cand_D[g] = D;
+  if (moved) {
+    // keep the list in its new order: the next iteration starts nearly sorted
+#pragma unroll
+    for (int r = 0; r < 2; ++r) {
+      const int e = 2 * lane + r;
+      if (e < MM) a.cand[(size_t)g * MM + e] = O::idx(k2[r]);
+    }
+  }
+  knn_store<T, KK>(a, g, sd, key, lane);
+  return true;
+}
+
+// Full search of the site at sorted position t (one warp): the K nearest
+// (MM = 0), or the MM nearest, which refresh its candidate list and whose
+// first K are the K-list.  seg receives the site's segment.
+template <class T, int KK, int MM>
+__device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, int lane, int& seg) {
+  using O = KeyOps<T>;
+  using Key = typename O::Key;
+  const Pt4<T> me = a.sorted[t];
   const int g = (int)me.id;
   const int s = __ldg(a.site_seg + g);
   seg = s;
@@ -441,146 +542,117 @@ __device__ __forceinline__ bool knn_site(const EngineArgs<T>& a, int parity, int
   // (site_knn.cuh:79-103) are exactly these, also when duplicates of the site
   // with smaller indices push self out of the K+1 (then the first K are kept,
   // the same K points), and the K-th distance equals the (K+1)-th with self.
-  constexpr int K = KK;
   const V3<T> q{me.x, me.y, me.z};
   const float kp = a.kth[g];
   const uint32_t self = (uint32_t)g;
-  Key key;  // lane j: entry j of the K-list
-  bool have = false;
+  Key key;
   if constexpr (MM > 0) {
-    const float r2b = a.cand_r2[g];
-    if (r2b >= 0.f) {
-      // the motion bound of the last step: this site's own motion, the
-      // largest motion in the 27 coarse blocks around its old position
-      // (lane b < 27 reads block b), and the step condition that no site
-      // from beyond those blocks reached the list's radius in one step
-      const GridGeom G = a.geom[s];
-      const V3<T> prev = ld3(a.S[parity ^ 1], g);
-      int bx, by, bz;
-      motion_block(G, prev, bx, by, bz);
-      unsigned mbits = 0u;
-      if (lane < 27) {
-        const int x = bx + lane % 3 - 1, y = by + (lane / 3) % 3 - 1, z = bz + lane / 9 - 1;
-        const int dx = (G.dim[0] + 3) >> 2, dy = (G.dim[1] + 3) >> 2, dz = (G.dim[2] + 3) >> 2;
-        if (x >= 0 && x < dx && y >= 0 && y < dy && z >= 0 && z < dz) {
-          const unsigned long long v = a.blockmax[G.cell_base + (z * dy + y) * dx + x];
-          if ((unsigned)(v >> 32) == (unsigned)(sd.iter - 1)) mbits = (unsigned)v;
-        }
-      }
-      mbits = __reduce_max_sync(0xffffffffu, mbits);
-      const double mu_i = sqrt((double)dist2(cvt3<double>(q), cvt3<double>(prev)));
-      const double rho = sqrt((double)r2b);
-      const double D = (double)a.cand_D[g] + (mu_i + (double)__uint_as_float(mbits)) * 1.0001;
-      const bool step_ok = ((double)sd.step_motion + mu_i) * 1.0001 < (4.0 * (double)G.h - rho) * 0.9999;
-      // re-key the list at the current positions and put it in order
-      // (element e = 2 lane + r)
-      const uint32_t* cr = a.cand + (size_t)g * MM;
-      const T* S = a.S[parity];
-      Key k2[2];
+    constexpr int RM = (MM + 31) / 32;
+    Key mk[RM];
+    const float rho = a.cand_rho[g];
+    const T thrM = rho >= 0.f && !isinf(rho) ? (T)rho * (T)rho * (T)1.2
+                   : (kp >= 0.f ? (T)kp * (T)(1.1 * (MM + 1) / (KK + 1)) : (T)sd.kth_est * (T)((MM + 1.0) / (KK + 1)));
+    warp_knn<T, T, MM>(a.geom[s], a.cell_start, a.sorted, q, thrM, lane, [self](uint32_t id) { return id != self; },
+                       mk);
 #pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int e = 2 * lane + r;
-        k2[r] = O::empty();
-        if (e < MM) {
-          const uint32_t id = __ldg(cr + e);
-          if (id != 0xffffffffu) k2[r] = O::make(dist2(ld3(S, (long)id), q), id);
-        }
-      }
-      const bool moved = warp_order_pairs<T>(k2[0], k2[1], lane);
-      // entry j to lane j
-      const Key e0 = shfl_key(k2[0], lane >> 1), e1 = shfl_key(k2[1], lane >> 1);
-      key = (lane & 1) ? e1 : e0;
-      const Key kth = shfl_key(key, KK - 1);
-      const double kap = sqrt((double)O::dist(kth));
-      have = !O::is_empty(kth) && (isinf(r2b) || (step_ok && kap * 1.0001 + D * 1.0001 < rho * 0.9999));
-      if (have) {
-        if (lane == 0) a.cand_D[g] = __double2float_ru(D);
-        if (moved) {
-          // keep the list in its new order: the next iteration starts sorted
-#pragma unroll
-          for (int r = 0; r < 2; ++r) {
-            const int e = 2 * lane + r;
-            if (e < MM) a.cand[(size_t)g * MM + e] = O::idx(k2[r]);
-          }
-        }
-      }
+    for (int r = 0; r < RM; ++r)
+      if (32 * r + lane < MM) a.cand[(size_t)g * MM + 32 * r + lane] = O::idx(mk[r]);
+    const Key mth = shfl_key(mk[(MM - 1) / 32], (MM - 1) % 32);
+    if (lane == 0) {
+      a.cand_rho[g] = O::is_empty(mth) ? __int_as_float(0x7f800000) : __fsqrt_rd(f32_rd(O::dist(mth)));
+      a.cand_D[g] = 0.f;
     }
-    if (!have) {
-      // full search for MM neighbours; its first KK are the K-list
-      constexpr int RM = (MM + 31) / 32;
-      Key mk[RM];
-      const T thrM = r2b >= 0.f && !isinf(r2b) ? (T)r2b * (T)1.2
-                     : (kp >= 0.f ? (T)kp * (T)(1.1 * (MM + 1) / (KK + 1)) : (T)sd.kth_est * (T)((MM + 1.0) / (KK + 1)));
-      warp_knn<T, T, MM>(a.geom[s], a.cell_start, a.sorted, q, thrM, lane,
-                         [self](uint32_t id) { return id != self; }, mk);
-#pragma unroll
-      for (int r = 0; r < RM; ++r)
-        if (32 * r + lane < MM) a.cand[(size_t)g * MM + 32 * r + lane] = O::idx(mk[r]);
-      const Key mth = shfl_key(mk[(MM - 1) / 32], (MM - 1) % 32);
-      if (lane == 0) {
-        a.cand_r2[g] = O::is_empty(mth) ? __int_as_float(0x7f800000) : (float)O::dist(mth);
-        a.cand_D[g] = 0.f;
-      }
-      key = mk[0];
-    }
+    key = mk[0];
   } else {
     // candidates beyond 1.1x the last K-th squared distance are skipped; sites
     // move little between iterations, and a bound that proves too tight
     // restarts the search without it (swept 1.02-1.5: 1.05-1.1 fastest)
     const T thr0 = kp >= 0.f ? (T)kp * (T)1.1 : (T)sd.kth_est;
     Key kl[1];
-    warp_knn<T, T, KK>(a.geom[s], a.cell_start, a.sorted, q, thr0, lane,
-                       [self](uint32_t id) { return id != self; }, kl);
+    warp_knn<T, T, KK>(a.geom[s], a.cell_start, a.sorted, q, thr0, lane, [self](uint32_t id) { return id != self; },
+                       kl);
     key = kl[0];
   }
-  (void)have;
-  const Key kth = shfl_key(key, KK - 1);
-  const bool full = !O::is_empty(kth);
-  if (lane == 0) a.kth[g] = full ? (float)O::dist(kth) : -1.f;
-  const uint32_t base = (uint32_t)sd.site_base;
-  const uint32_t gid = O::idx(key);
-  const uint32_t out = gid == 0xffffffffu ? 0xffffffffu : gid - base;
-  uint32_t* row = a.knn + (size_t)g * K;
-  bool diff = false;
-  if (lane < K) {
-    diff = row[lane] != out;
-    if (diff) row[lane] = out;
-  }
-  const unsigned changed = __ballot_sync(0xffffffffu, diff);
-  if (lane == 0) a.same[g] = changed ? 0 : 1;
-  return have;
+  knn_store<T, KK>(a, g, sd, key, lane);
 }
 
-// One warp per active site; the block then adds its lists taken from the
-// candidate lists and its full searches to the segments' statistics (words
-// 6 and 7 of the iteration's slot), one atomic per run of warps of the same
-// segment.
-template <class T, int KK, int MM, int BS>
-__global__ void __launch_bounds__(BS) k_site_knn(EngineArgs<T> a, int parity) {
-  __shared__ int wseg[BS / 32];
-  __shared__ int wuse[BS / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int w = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-  int seg = -1;
-  bool reused = false;
-  if (w < __ldg(a.act_count)) reused = knn_site<T, KK, MM>(a, parity, w, lane, seg);
-  if (lane == 0) { wseg[wid] = seg; wuse[wid] = reused ? 1 : 0; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int cur = -1, nr = 0, ns = 0;
-    auto flush = [&]() {
-      if (cur < 0) return;
-      int* sl = a.stats + ((size_t)cur * kStatsRing + (a.segs[cur].iter % kStatsRing)) * kStatsWords;
-      if (nr) atomicAdd(sl + 6, nr);
-      if (ns) atomicAdd(sl + 7, ns);
-    };
-    for (int i = 0; i < BS / 32; ++i) {
-      if (wseg[i] < 0) continue;
-      if (wseg[i] != cur) { flush(); cur = wseg[i]; nr = ns = 0; }
-      if (wuse[i]) ++nr; else ++ns;
-    }
-    flush();
+// Per-warp running count of one statistics word for the segment it is on:
+// added to the segment's slot when the segment changes and at the end.
+template <class T>
+struct SegCounter {
+  int cur = -1, n = 0;
+  __device__ __forceinline__ void add(const EngineArgs<T>& a, int seg, int word, int lane) {
+    if (seg != cur) { flush(a, word, lane); cur = seg; n = 0; }
+    ++n;
   }
+  __device__ __forceinline__ void flush(const EngineArgs<T>& a, int word, int lane) {
+    if (lane == 0 && cur >= 0 && n)
+      atomicAdd(a.stats + ((size_t)cur * kStatsRing + (a.segs[cur].iter % kStatsRing)) * kStatsWords + word, n);
+  }
+};
+
+// Site KNN, two persistent kernels, each launched with the warps its launch
+// bounds keep resident on every SM (so no block waits for a second wave):
+// k_knn_verify's warp i takes active positions i, i + nw, i + 2 nw, ...,
+// takes each site's K-list from its candidate list where the motion bound
+// proves it exact, and appends the other sites to its own part of a.srch
+// (no atomics: every verify warp owns a.srch_cap slots); k_knn_search's warp
+// j searches, in full, the sites of verify warps j, j + nws, ...  Without
+// candidate lists (MM = 0) only k_knn_search runs, over every active site.
+// The reused lists and the full searches are added to the segments'
+// statistics (words 6 and 7 of the iteration's slot).
+constexpr int kKnnVerifyWarpsPerSM = 48;
+constexpr int kKnnSearchWarpsPerSM = 32;
+
+template <class T, int KK, int MM, int BS>
+__global__ void __launch_bounds__(BS, kKnnVerifyWarpsPerSM * 32 / BS) k_knn_verify(EngineArgs<T> a, int parity) {
+  const int lane = threadIdx.x & 31;
+  const int wi = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+  const int n = __ldg(a.act_count);
+  int* mine = a.srch + (size_t)wi * a.srch_cap;
+  int cnt = 0;
+  SegCounter<T> reused;
+  for (int w = wi; w < n; w += nw) {
+    int seg;
+    if (knn_verify_site<T, KK, MM>(a, parity, w, lane, seg)) {
+      reused.add(a, seg, 6, lane);
+    } else {
+      if (lane == 0) mine[cnt] = a.act[w];
+      ++cnt;
+    }
+  }
+  reused.flush(a, 6, lane);
+  if (lane == 0) a.srch_n[wi] = cnt;
+}
+
+template <class T, int KK, int MM, int BS>
+__global__ void __launch_bounds__(BS, kKnnSearchWarpsPerSM * 32 / BS) k_knn_search(EngineArgs<T> a, int parity,
+                                                                                   int n_lists) {
+  (void)parity;
+  const int lane = threadIdx.x & 31;
+  const int wi = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int nw = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
+  SegCounter<T> searched;
+  if constexpr (MM > 0) {
+    for (int l = wi; l < n_lists; l += nw) {
+      const int* list = a.srch + (size_t)l * a.srch_cap;
+      const int n = a.srch_n[l];
+      for (int k = 0; k < n; ++k) {
+        int seg;
+        knn_search_site<T, KK, MM>(a, list[k], lane, seg);
+        searched.add(a, seg, 7, lane);
+      }
+    }
+  } else {
+    const int n = __ldg(a.act_count);
+    for (int w = wi; w < n; w += nw) {
+      int seg;
+      knn_search_site<T, KK, MM>(a, a.act[w], lane, seg);
+      searched.add(a, seg, 7, lane);
+    }
+  }
+  searched.flush(a, 7, lane);
 }
 
 // ---------------------------------------------------------------------------
@@ -736,8 +808,6 @@ __device__ __forceinline__ void site_finish(const EngineArgs<typename PT<PROF>::
 // is handed to k_site_far (a centroid far off the surface, e.g. of a cell
 // that the neighbours leave almost unbounded in the first iteration).
 constexpr int kVertexRingLimit = 4;
-// vertices kept per site for the centroid -> vertex search (knn_reuse)
-constexpr int kVCand = 8;
 
 // Everything after the centroid; false when the 5-NN search was deferred
 // (the site is then listed in a.far and finished by k_site_far).
@@ -758,65 +828,15 @@ __device__ __forceinline__ bool site_proj(const EngineArgs<typename PT<PROF>::T>
   int knnv[kKProj];
   if (!fz) {
     const int skip = (sd.mode == 0 && sd.ex_quirk) ? g - sd.site_base : -1;
-    const V3<T> c = ld3((const T*)a.cent, g);
-    bool have = false;
-    if (a.vcand) {
-      // the kVCand vertices nearest to the centroid of the last full search:
-      // mesh vertices do not move, so one outside that list is still
-      // farther than rho - |c - c_build|; when the 5th nearest of the list
-      // is closer than that, the list's first 5 are the 5 nearest of all
-      // (the same keys as the grid search; 1e-4 margins for rounding)
-      const float r2b = a.vcand_r2[g];
-      if (r2b >= 0.f && finite3(c)) {
-        TopK<T, kKProj> top;
-        const int* vc = a.vcand + (size_t)g * kVCand;
-#pragma unroll
-        for (int k = 0; k < kVCand; ++k) {
-          const int v = __ldg(vc + k);
-          if (v < 0) continue;
-          const T d = dist2(V3<T>{(T)__ldg(md.V + 3 * v), (T)__ldg(md.V + 3 * v + 1), (T)__ldg(md.V + 3 * v + 2)}, c);
-          if (d <= top.worst_d()) top.insert(KeyOps<T>::make(d, (uint32_t)v));
-        }
-        const V3<T> cb = ld3((const T*)a.vcand_c, g);
-        const double delta = sqrt((double)dist2(cvt3<double>(c), cvt3<double>(cb)));
-        const double k5 = sqrt((double)top.worst_d());
-        have = top.full() && (isinf(r2b) || k5 * 1.0001 + delta * 1.0001 < sqrt((double)r2b) * 0.9999);
-        if (have) {
-#pragma unroll
-          for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
-        }
-      }
+    TopK<T, kKProj> top;
+    if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, ld3((const T*)a.cent, g), top,
+                                    [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
+      const int k = atomicAdd(a.far, 1);
+      a.far[1 + k] = g;
+      return false;
     }
-    if (!have && a.vcand) {
-      // full search for kVCand vertices; refreshes the list
-      TopK<T, kVCand> top;
-      if (!grid_knn<T, float, kVCand>(md.vg, md.vcell_start, md.vsorted, c, top,
-                                      [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
-        a.vcand_r2[g] = -1.f;
-        const int k = atomicAdd(a.far, 1);
-        a.far[1 + k] = g;
-        return false;
-      }
-      int* vc = a.vcand + (size_t)g * kVCand;
 #pragma unroll
-      for (int k = 0; k < kVCand; ++k) {
-        const int v = KeyOps<T>::is_empty(top.k[k]) ? -1 : (int)KeyOps<T>::idx(top.k[k]);
-        vc[k] = v;
-        if (k < kKProj) { knnv[k] = v; kv[k] = v; }
-      }
-      st3((T*)a.vcand_c, g, c);
-      a.vcand_r2[g] = top.full() ? (float)top.worst_d() : __int_as_float(0x7f800000);
-    } else if (!have) {
-      TopK<T, kKProj> top;
-      if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, c, top,
-                                      [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
-        const int k = atomicAdd(a.far, 1);
-        a.far[1 + k] = g;
-        return false;
-      }
-#pragma unroll
-      for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
-    }
+    for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
   } else {
 #pragma unroll
     for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];

@@ -315,12 +315,13 @@ __device__ __forceinline__ void warp_knn(const GridGeom& g, const int* __restric
 }
 
 // ---------------------------------------------------------------------------
-// warp-wide ordering of a short key list held two keys per lane (element e
-// = 2 lane + r, r = 0, 1): odd-even transposition passes until the list is
-// in order.  A list that is already nearly in order (a site's candidate
-// list from an earlier iteration, re-keyed at the sites' new positions)
-// needs a pass or two; 64 passes order any list.  Returns true when some
-// key moved.
+// warp-wide selection of the KK smallest of a short key list held two keys
+// per lane (element e = 2 lane + r, r = 0, 1), in order: odd-even
+// transposition passes until the first KK elements are in order and every
+// later one is above the KK-th (the order among the later ones does not
+// matter).  A list that is already nearly in order (a site's candidate list
+// from an earlier iteration, re-keyed at the sites' new positions) needs a
+// pass or two; 64 passes order any list.  Returns true when some key moved.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ unsigned long long shfl_down_key(unsigned long long k, int d) {
   return __shfl_down_sync(0xffffffffu, k, d);
@@ -329,14 +330,21 @@ __device__ __forceinline__ DKey shfl_down_key(DKey k, int d) {
   return {__shfl_down_sync(0xffffffffu, k.d, d), __shfl_down_sync(0xffffffffu, k.i, d)};
 }
 
-template <class T>
-__device__ __forceinline__ bool warp_order_pairs(typename KeyOps<T>::Key& k0, typename KeyOps<T>::Key& k1, int lane) {
+template <class T, int KK>
+__device__ __forceinline__ bool warp_select_pairs(typename KeyOps<T>::Key& k0, typename KeyOps<T>::Key& k1,
+                                                  int lane) {
   using O = KeyOps<T>;
+  constexpr int KL = (KK - 1) >> 1, KR = (KK - 1) & 1;  // lane and register of element KK-1
+  const int e0 = 2 * lane, e1 = 2 * lane + 1;
   bool moved = false;
   for (int pass = 0; pass < 64; ++pass) {
-    // in order: k0 < k1 in every lane and k1 < the next lane's k0
     const auto nx = shfl_down_key(k0, 1);
-    const bool ok = !O::less(k1, k0) && (lane == 31 || !O::less(nx, k1));
+    const auto kth = shfl_key(KR ? k1 : k0, KL);
+    bool ok = true;
+    if (e0 + 1 <= KK - 1) ok = ok && O::less(k0, k1);
+    if (e1 + 1 <= KK - 1) ok = ok && O::less(k1, nx);
+    if (e0 >= KK) ok = ok && O::less(kth, k0);
+    if (e1 >= KK) ok = ok && O::less(kth, k1);
     if (__all_sync(0xffffffffu, ok)) break;
     moved = true;
     // pairs (2l, 2l+1): inside the lane
