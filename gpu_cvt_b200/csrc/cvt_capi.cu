@@ -1163,6 +1163,11 @@ static void engine_free(cvt_engine* e) {
 // more a refresh costs)
 static constexpr int cand_len(int k) { return k + 16 > 64 ? 64 : k + 16; }
 
+// Neighbours a site-grid cell is sized for (times cell_factor): K+1.  (Cells
+// sized for the candidate list's length made its full searches cheaper but
+// the coarse motion blocks coarser, which kept fewer lists: slower overall.)
+static double grid_neighbours(const cvt_params_t& p) { return (double)(p.k + 1); }
+
 static bool k_supported(int k) { return k == 8 || k == 12 || k == 16 || k == 20 || k == 24 || k == 32; }
 
 extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segments, int max_sites, int max_cells,
@@ -1241,7 +1246,7 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
     ar.add(&e->d_cand, (size_t)cand_len(e->K) * ns);
     ar.add(&e->d_cand_rho, ns);
     ar.add(&e->d_cand_D, ns);
-    e->srch_cap = (int)cdiv((long)ns, (long)e->num_sms * kKnnVerifyWarpsPerSM);
+    e->srch_cap = (int)cdiv((long)ns, (long)e->num_sms * kKnnVerifyWarpsPerSM) + 2;  // two sites per warp step
     ar.add(&e->d_srch, (size_t)e->srch_cap * e->num_sms * kKnnVerifyWarpsPerSM);
     ar.add(&e->d_srch_n, (size_t)e->num_sms * kKnnVerifyWarpsPerSM);
     ar.add(&e->d_blockmax, (size_t)max_cells);
@@ -1278,7 +1283,7 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
     cvt_status_t bs = mesh_ensure_bvh(mesh);  // the projection walks it
     if (bs != CVT_OK) return bs;
   }
-  GridGeom g = surface_grid(mesh->lo, mesh->hi, mesh->area, n, (double)(e->K + 1), e->p.cell_factor, 4L * n + 64);
+  GridGeom g = surface_grid(mesh->lo, mesh->hi, mesh->area, n, grid_neighbours(e->p), e->p.cell_factor, 4L * n + 64);
   int cells = g.ncell + 1;
   int base = e->site_alloc.take(n);
   if (base < 0) return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: site capacity exhausted");
@@ -1707,7 +1712,7 @@ extern "C" cvt_status_t cvt_engine_last_launches(cvt_engine_t e, long long* n) {
 
 // capacity for one mesh + site set
 static void engine_caps(const cvt_mesh* m, int n, const cvt_params_t* p, int* cells) {
-  GridGeom g = surface_grid(m->lo, m->hi, m->area, n, (double)(p->k + 1), p->cell_factor, 4L * n + 64);
+  GridGeom g = surface_grid(m->lo, m->hi, m->area, n, grid_neighbours(*p), p->cell_factor, 4L * n + 64);
   *cells = g.ncell + 1;
 }
 

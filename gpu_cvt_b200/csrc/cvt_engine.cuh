@@ -123,13 +123,20 @@ __device__ __forceinline__ float f32_ru(double x) { return __double2float_ru(x);
 __device__ __forceinline__ float f32_rd(float x) { return x; }
 __device__ __forceinline__ float f32_rd(double x) { return __double2float_rd(x); }
 
-// Coarse motion blocks of a segment: 4 x 4 x 4 grid cells, stored in the
+// Coarse motion blocks of a segment: kBlockCells^3 grid cells, stored in the
 // first cells of the segment's cell range (there are fewer blocks than
 // cells).  Positions outside the grid fall in the edge blocks, like cells.
+// Larger blocks make the step condition looser but take the maximum motion
+// over more sites (measured: 4 cells kept more lists than 3 cells of a grid
+// sized for the candidate list's length).
+constexpr int kBlockCells = 4;
+__device__ __forceinline__ int block_dim(const GridGeom& g, int a) { return (g.dim[a] + kBlockCells - 1) / kBlockCells; }
+
 template <class T>
 __device__ __forceinline__ int motion_block(const GridGeom& g, V3<T> p, int& bx, int& by, int& bz) {
-  bx = grid_coord(g, p.x, 0) >> 2; by = grid_coord(g, p.y, 1) >> 2; bz = grid_coord(g, p.z, 2) >> 2;
-  return g.cell_base + (bz * ((g.dim[1] + 3) >> 2) + by) * ((g.dim[0] + 3) >> 2) + bx;
+  bx = grid_coord(g, p.x, 0) / kBlockCells; by = grid_coord(g, p.y, 1) / kBlockCells;
+  bz = grid_coord(g, p.z, 2) / kBlockCells;
+  return g.cell_base + (bz * block_dim(g, 1) + by) * block_dim(g, 0) + bx;
 }
 
 // polygon storage: vertex k at p[k * stride] (shared memory: thread-
@@ -419,8 +426,8 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
 // nearest other sites of its last full search (ids and the MM-th squared
 // distance r2b = rho^2) and a bound D on how much closer any other site can
 // have come since.  Every iteration adds to D the site's own last motion and
-// the largest last motion of any site in the 27 coarse blocks (4 x 4 x 4
-// cells, edge B = 4h) around the site's old position.  A site j outside the
+// the largest last motion of any site in the 27 coarse blocks (3 x 3 x 3
+// cells, edge B = 3h) around the site's old position.  A site j outside the
 // list started at distance >= rho; while it is within B of site i its steps
 // are among those counted, and it cannot jump from beyond B to within rho in
 // one step as long as (largest motion of the step in the segment) + (i's
@@ -450,80 +457,6 @@ __device__ __forceinline__ void knn_store(const EngineArgs<T>& a, int g, const S
   }
   const unsigned changed = __ballot_sync(0xffffffffu, diff);
   if (lane == 0) a.same[g] = changed ? 0 : 1;
-}
-
-// Candidate-list check of active site w (one warp): true when the K-list
-// came from the list (and is stored); false when the site needs a full
-// search.  seg receives the site's segment.
-template <class T, int KK, int MM>
-__device__ __forceinline__ bool knn_verify_site(const EngineArgs<T>& a, int parity, int w, int lane, int& seg) {
-  static_assert(KK <= 32, "one list entry per lane");
-  static_assert(MM > KK && MM <= 64 && MM % 2 == 0, "candidate list of KK < MM <= 64 (even) entries");
-  using O = KeyOps<T>;
-  using Key = typename O::Key;
-  const Pt4<T> me = a.sorted[a.act[w]];
-  const int g = (int)me.id;
-  const int s = __ldg(a.site_seg + g);
-  seg = s;
-  const float rho = a.cand_rho[g];
-  if (!(rho >= 0.f)) return false;
-  const SegDev& sd = a.segs[s];
-  const V3<T> q{me.x, me.y, me.z};
-  // the motion bound of the last step: this site's own motion, the largest
-  // motion in the 27 coarse blocks around its old position (lane b < 27
-  // reads block b), and the step condition that no site from beyond those
-  // blocks reached the list's radius in one step
-  const GridGeom G = a.geom[s];
-  const V3<T> prev = ld3(a.S[parity ^ 1], g);
-  int bx, by, bz;
-  motion_block(G, prev, bx, by, bz);
-  unsigned mbits = 0u;
-  if (lane < 27) {
-    const int x = bx + lane % 3 - 1, y = by + (lane / 3) % 3 - 1, z = bz + lane / 9 - 1;
-    const int dx = (G.dim[0] + 3) >> 2, dy = (G.dim[1] + 3) >> 2, dz = (G.dim[2] + 3) >> 2;
-    if (x >= 0 && x < dx && y >= 0 && y < dy && z >= 0 && z < dz) {
-      const unsigned long long v = a.blockmax[G.cell_base + (z * dy + y) * dx + x];
-      if ((unsigned)(v >> 32) == (unsigned)(sd.iter - 1)) mbits = (unsigned)v;
-    }
-  }
-  mbits = __reduce_max_sync(0xffffffffu, mbits);
-  // FP32 with upward rounding; the 1e-4 margins below are far above it
-  const float mu_i = __fsqrt_ru(f32_ru(dist2(q, prev)));
-  const float D = __fadd_ru(a.cand_D[g], __fadd_ru(mu_i, __uint_as_float(mbits)));
-  const bool step_ok = __fadd_ru(sd.step_motion, mu_i) * 1.0001f < (4.f * G.h - rho) * 0.9999f;
-  if (!isinf(rho) && !step_ok) return false;
-  // re-key the list at the current positions and select its KK smallest
-  // in order (element e = 2 lane + r)
-  const uint32_t* cr = a.cand + (size_t)g * MM;
-  const T* S = a.S[parity];
-  Key k2[2];
-#pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int e = 2 * lane + r;
-    k2[r] = O::empty();
-    if (e < MM) {
-      const uint32_t id = __ldg(cr + e);
-      if (id != 0xffffffffu) k2[r] = O::make(dist2(ld3(S, (long)id), q), id);
-    }
-  }
-  const bool moved = warp_select_pairs<T, KK>(k2[0], k2[1], lane);
-  // entry j to lane j
-  const Key e0 = shfl_key(k2[0], lane >> 1), e1 = shfl_key(k2[1], lane >> 1);
-  const Key key = (lane & 1) ? e1 : e0;
-  const Key kth = shfl_key(key, KK - 1);
-  const float kap = __fsqrt_ru(f32_ru(O::dist(kth)));
-  if (O::is_empty(kth) || !(isinf(rho) || kap * 1.0001f + D * 1.0001f < rho * 0.9999f)) return false;
-  if (lane == 0) a.cand_D[g] = D;
-  if (moved) {
-    // keep the list in its new order: the next iteration starts nearly sorted
-#pragma unroll
-    for (int r = 0; r < 2; ++r) {
-      const int e = 2 * lane + r;
-      if (e < MM) a.cand[(size_t)g * MM + e] = O::idx(k2[r]);
-    }
-  }
-  knn_store<T, KK>(a, g, sd, key, lane);
-  return true;
 }
 
 // Full search of the site at sorted position t (one warp): the K nearest
@@ -576,11 +509,110 @@ __device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, i
   knn_store<T, KK>(a, g, sd, key, lane);
 }
 
+// Candidate-list check of active site w by a half warp (16 lanes, one site
+// each half, three list entries per lane: element e = 3 hl + r), so a warp
+// checks two sites at once.  The motion bound D grows by the largest last
+// motion M in the 27 coarse blocks around the site's old position (lanes
+// hl and hl + 16 < 27 read one block each) plus the site's own motion; the
+// step condition asks that the segment's largest motion plus the site's own
+// stay below B - rho.  The list is re-keyed at the current positions and its
+// KK smallest selected in order (half_select3); it is accepted when the
+// KK-th is closer than rho - D.  `valid`: this half has a site.  Every lane
+// runs every warp-wide step; true when the half's K-list came from the list
+// (and is stored: row entries that changed, kth, same, the list's new
+// order, D).
+template <class T, int KK, int MM>
+__device__ __forceinline__ bool knn_verify_half(const EngineArgs<T>& a, int parity, int w, bool valid, int lane,
+                                                int& seg) {
+  static_assert(KK <= 32 && MM > KK && MM <= 48, "candidate list of KK < MM <= 48 entries");
+  using O = KeyOps<T>;
+  using Key = typename O::Key;
+  const int hl = lane & 15, half = lane >> 4;
+  const unsigned hmask = 0xffffu << (16 * half);
+  int g = -1, s = -1;
+  float rho = -1.f;
+  V3<T> q{0, 0, 0};
+  if (valid) {
+    const Pt4<T> me = a.sorted[a.act[w]];
+    g = (int)me.id;
+    s = __ldg(a.site_seg + g);
+    rho = a.cand_rho[g];
+    q = {me.x, me.y, me.z};
+  }
+  seg = s;
+  bool ok = valid && rho >= 0.f;
+  // motion bound: lanes hl and hl + 16 < 27 read blocks
+  unsigned mbits = 0u;
+  float D = 0.f, lim = 0.f;
+  if (ok) {
+    const SegDev& sd = a.segs[s];
+    const GridGeom G = a.geom[s];
+    int bx, by, bz;
+    motion_block(G, ld3(a.S[parity ^ 1], g), bx, by, bz);
+    const int dx = block_dim(G, 0), dy = block_dim(G, 1), dz = block_dim(G, 2);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int b = hl + 16 * k;
+      if (b < 27) {
+        const int x = bx + b % 3 - 1, y = by + (b / 3) % 3 - 1, z = bz + b / 9 - 1;
+        if (x >= 0 && x < dx && y >= 0 && y < dy && z >= 0 && z < dz) {
+          const unsigned long long v = a.blockmax[G.cell_base + (z * dy + y) * dx + x];
+          if ((unsigned)(v >> 32) == (unsigned)(sd.iter - 1)) mbits = max(mbits, (unsigned)v);
+        }
+      }
+    }
+    mbits = __reduce_max_sync(hmask, mbits);
+    // this site's own motion (also inside M, but usually far below it)
+    const float mu = __fsqrt_rn(f32_ru(dist2(q, ld3(a.S[parity ^ 1], g)))) * 1.000001f;
+    D = __fadd_ru(a.cand_D[g], __fadd_ru(__uint_as_float(mbits), mu));
+    const bool step_ok = __fadd_ru(sd.step_motion, mu) * 1.0001f < ((float)kBlockCells * G.h - rho) * 0.9999f;
+    lim = rho * 0.9999f - D * 1.0001f;
+    ok = isinf(rho) || (step_ok && lim > 0.f);
+  }
+  // re-key and select (both halves take part in every pass)
+  Key k[3];
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const int e = 3 * hl + r;
+    k[r] = O::empty();
+    if (ok && e < MM) {
+      const uint32_t id = __ldg(a.cand + (size_t)g * MM + e);
+      if (id != 0xffffffffu) k[r] = O::make(dist2(ld3(a.S[parity], (long)id), q), id);
+    }
+  }
+  bool moved;
+  half_select3<T, KK>(k, hl, half, moved);
+  constexpr int KL = (KK - 1) / 3, KR = (KK - 1) % 3;
+  const Key kth = shfl16_key(k[KR], KL);
+  ok = ok && !O::is_empty(kth) && (isinf(rho) || f32_ru(O::dist(kth)) * 1.0003f < lim * lim);
+  // store (per half: entries e < KK of this lane, the flags by lane hl 0)
+  bool diff = false;
+  if (ok) {
+    const uint32_t base = (uint32_t)a.segs[s].site_base;
+    uint32_t* row = a.knn + (size_t)g * KK;
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      const int e = 3 * hl + r;
+      if (moved && e < MM) a.cand[(size_t)g * MM + e] = O::idx(k[r]);
+      if (e < KK) {
+        const uint32_t gid = O::idx(k[r]);
+        const uint32_t out = gid == 0xffffffffu ? 0xffffffffu : gid - base;
+        if (row[e] != out) { row[e] = out; diff = true; }
+      }
+    }
+    if (hl == 0) { a.cand_D[g] = D; a.kth[g] = (float)O::dist(kth); }
+  }
+  const unsigned changed = __ballot_sync(0xffffffffu, diff) & hmask;
+  if (ok && hl == 0) a.same[g] = changed ? 0 : 1;
+  return ok;
+}
+
 // Per-warp running count of one statistics word for the segment it is on:
 // added to the segment's slot when the segment changes and at the end.
 template <class T>
 struct SegCounter {
   int cur = -1, n = 0;
+  // `lane` 0 adds for the whole warp (or half warp: pass its lane within the half)
   __device__ __forceinline__ void add(const EngineArgs<T>& a, int seg, int word, int lane) {
     if (seg != cur) { flush(a, word, lane); cur = seg; n = 0; }
     ++n;
@@ -612,17 +644,21 @@ __global__ void __launch_bounds__(BS, kKnnVerifyWarpsPerSM * 32 / BS) k_knn_veri
   const int n = __ldg(a.act_count);
   int* mine = a.srch + (size_t)wi * a.srch_cap;
   int cnt = 0;
-  SegCounter<T> reused;
-  for (int w = wi; w < n; w += nw) {
+  SegCounter<T> reused;  // per half, kept by lanes 0 and 16
+  const int hl = lane & 15, half = lane >> 4;
+  // two sites per warp: the halves take positions 2i + half, 2i + half + 2 nw, ...
+  for (int w0 = 2 * wi; w0 < n; w0 += 2 * nw) {
+    const int w = w0 + half;
     int seg;
-    if (knn_verify_site<T, KK, MM>(a, parity, w, lane, seg)) {
-      reused.add(a, seg, 6, lane);
-    } else {
-      if (lane == 0) mine[cnt] = a.act[w];
-      ++cnt;
-    }
+    const bool ok = knn_verify_half<T, KK, MM>(a, parity, w, w < n, lane, seg);
+    const bool need = w < n && !ok;
+    if (ok) reused.add(a, seg, 6, hl);
+    // the warp's list: half 0's site first, then half 1's
+    const unsigned b = __ballot_sync(0xffffffffu, need && hl == 0);
+    if (need && hl == 0) mine[cnt + (half ? (int)(b & 1u) : 0)] = a.act[w];
+    cnt += __popc(b);
   }
-  reused.flush(a, 6, lane);
+  reused.flush(a, 6, hl);
   if (lane == 0) a.srch_n[wi] = cnt;
 }
 

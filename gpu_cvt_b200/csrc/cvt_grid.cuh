@@ -315,48 +315,73 @@ __device__ __forceinline__ void warp_knn(const GridGeom& g, const int* __restric
 }
 
 // ---------------------------------------------------------------------------
-// warp-wide selection of the KK smallest of a short key list held two keys
-// per lane (element e = 2 lane + r, r = 0, 1), in order: odd-even
-// transposition passes until the first KK elements are in order and every
-// later one is above the KK-th (the order among the later ones does not
-// matter).  A list that is already nearly in order (a site's candidate list
-// from an earlier iteration, re-keyed at the sites' new positions) needs a
-// pass or two; 64 passes order any list.  Returns true when some key moved.
+// Warp-wide selection of the KK smallest keys of short lists, in order,
+// one list per half warp (16 lanes) with three keys per lane (element
+// e = 3 hl + r, hl = lane within the half): odd-even transposition passes
+// until the first KK elements are in order and every later one is above the
+// KK-th (the order among the later ones does not matter).  A list that is
+// already nearly in order (a site's candidate list from an earlier
+// iteration, re-keyed at the sites' new positions) needs a pass or two; 64
+// passes order any list.  Every pass is an odd-even transposition of the
+// half's 48 elements; both
+// halves run the same passes (the shuffles are warp-wide), a half that is
+// in order only repeats no-op exchanges.  `moved` tells whether this half's
+// keys moved.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned long long shfl_down_key(unsigned long long k, int d) {
-  return __shfl_down_sync(0xffffffffu, k, d);
+__device__ __forceinline__ unsigned long long shfl16_key(unsigned long long k, int src) {
+  return __shfl_sync(0xffffffffu, k, src, 16);
 }
-__device__ __forceinline__ DKey shfl_down_key(DKey k, int d) {
-  return {__shfl_down_sync(0xffffffffu, k.d, d), __shfl_down_sync(0xffffffffu, k.i, d)};
+__device__ __forceinline__ DKey shfl16_key(DKey k, int src) {
+  return {__shfl_sync(0xffffffffu, k.d, src, 16), __shfl_sync(0xffffffffu, k.i, src, 16)};
+}
+__device__ __forceinline__ unsigned long long shfl16_down_key(unsigned long long k) {
+  return __shfl_down_sync(0xffffffffu, k, 1, 16);
+}
+__device__ __forceinline__ DKey shfl16_down_key(DKey k) {
+  return {__shfl_down_sync(0xffffffffu, k.d, 1, 16), __shfl_down_sync(0xffffffffu, k.i, 1, 16)};
+}
+__device__ __forceinline__ unsigned long long shfl16_up_key(unsigned long long k) {
+  return __shfl_up_sync(0xffffffffu, k, 1, 16);
+}
+__device__ __forceinline__ DKey shfl16_up_key(DKey k) {
+  return {__shfl_up_sync(0xffffffffu, k.d, 1, 16), __shfl_up_sync(0xffffffffu, k.i, 1, 16)};
 }
 
 template <class T, int KK>
-__device__ __forceinline__ bool warp_select_pairs(typename KeyOps<T>::Key& k0, typename KeyOps<T>::Key& k1,
-                                                  int lane) {
+__device__ __forceinline__ void half_select3(typename KeyOps<T>::Key (&k)[3], int hl, int half, bool& moved) {
   using O = KeyOps<T>;
-  constexpr int KL = (KK - 1) >> 1, KR = (KK - 1) & 1;  // lane and register of element KK-1
-  const int e0 = 2 * lane, e1 = 2 * lane + 1;
-  bool moved = false;
+  constexpr int KL = (KK - 1) / 3, KR = (KK - 1) % 3;  // lane and register of element KK-1
+  const int e0 = 3 * hl;
+  moved = false;
   for (int pass = 0; pass < 64; ++pass) {
-    const auto nx = shfl_down_key(k0, 1);
-    const auto kth = shfl_key(KR ? k1 : k0, KL);
+    const auto nx0 = shfl16_down_key(k[0]);
+    const auto kth = shfl16_key(k[KR], KL);
+    const bool kth_empty = O::is_empty(kth);
     bool ok = true;
-    if (e0 + 1 <= KK - 1) ok = ok && O::less(k0, k1);
-    if (e1 + 1 <= KK - 1) ok = ok && O::less(k1, nx);
-    if (e0 >= KK) ok = ok && O::less(kth, k0);
-    if (e1 >= KK) ok = ok && O::less(kth, k1);
-    if (__all_sync(0xffffffffu, ok)) break;
-    moved = true;
-    // pairs (2l, 2l+1): inside the lane
-    const auto lo = O::kmin(k0, k1), hi = O::kmax(k0, k1);
-    k0 = lo; k1 = hi;
-    // pairs (2l+1, 2l+2): this lane's k1 with the next lane's k0
-    const auto nk0 = shfl_down_key(k0, 1);
-    const auto pk1 = shfl_up_key(k1);
-    if (lane < 31) k1 = O::kmin(k1, nk0);
-    if (lane > 0) k0 = O::kmax(k0, pk1);
+    if (e0 + 1 <= KK - 1) ok = ok && O::less(k[0], k[1]);
+    if (e0 + 2 <= KK - 1) ok = ok && O::less(k[1], k[2]);
+    if (e0 + 3 <= KK - 1 && hl < 15) ok = ok && O::less(k[2], nx0);
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      if (e0 + r >= KK) ok = ok && (kth_empty || O::less(kth, k[r]));
+    const unsigned b = __ballot_sync(0xffffffffu, ok);
+    if (b == 0xffffffffu) break;
+    if (((b >> (16 * half)) & 0xffffu) != 0xffffu) moved = true;
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      const auto n0 = shfl16_down_key(k[0]);
+      const auto p2 = shfl16_up_key(k[2]);
+      if ((hl & 1) == p) {
+        const auto lo = O::kmin(k[0], k[1]), hi = O::kmax(k[0], k[1]);
+        k[0] = lo; k[1] = hi;
+        if (hl < 15) k[2] = O::kmin(k[2], n0);
+      } else {
+        const auto lo = O::kmin(k[1], k[2]), hi = O::kmax(k[1], k[2]);
+        k[1] = lo; k[2] = hi;
+        if (hl > 0) k[0] = O::kmax(k[0], p2);
+      }
+    }
   }
-  return moved;
 }
 
 // ---------------------------------------------------------------------------
