@@ -819,13 +819,26 @@ def run_precision(args):
     return 0
 
 
+def run_options(args):
+    """The projection (one-ring / BVH) and frame (vertex normal / PCA)
+    options on the 100k-site torus and the 1M-site rounded box: mixed
+    profile against FP64 with the same options."""
+    import torch
+    from gpu_cvt_b200 import workloads
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    res = [workloads.options_study(c) for c in ("torus_100k", "superellipsoid_1m")]
+    print(json.dumps({"workload": "options", "studies": res}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["batched", "torus_100k", "serve", "superellipsoid_1m"], default="batched")
+    ap.add_argument("--workload", choices=["batched", "torus_100k", "serve", "superellipsoid_1m", "options"],
+                    default="batched")
     ap.add_argument("--meshes", type=int, default=256, help="batched workload: number of meshes (256)")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-seconds", type=float, default=120.0,
@@ -846,6 +859,8 @@ def main():
         return run_serve(args)
     if args.workload == "superellipsoid_1m":
         return run_precision(args)
+    if args.workload == "options":
+        return run_options(args)
     return run_ours_torus(args)
 
 

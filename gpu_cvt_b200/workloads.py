@@ -178,3 +178,52 @@ def precision_study(iters=200, k=32, mode=1, n_sites=1_000_000, tris=2_000_000, 
         out[prof]["dH_minus_fp64_rel"] = (out[prof]["dH"] - out["fp64"]["dH"]) / M.diag
     M.close()
     return out
+
+
+def options_study(case="torus_100k", combos=(("onering", "vertex"), ("bvh", "vertex"), ("onering", "pca"),
+                                             ("bvh", "pca"))):
+    """The projection and frame options on one workload: for each (proj,
+    frame) combination the mixed-profile run against the FP64 run with the
+    same options (per-site drift, Hausdorff difference), its Hausdorff and
+    time.  case: "torus_100k" (100k sites, K=24, 100 iterations, mode 1) or
+    "superellipsoid_1m" (1M sites on the jittered rounded box, K=32, 200
+    iterations, mode 1)."""
+    import torch
+    if case == "torus_100k":
+        m, S0, p = mg.workload_mesh("torus_100k")
+        k, iters = p["k"], p["iters"]
+    else:
+        m = mg.superellipsoid(8.0, 2_000_000, 0.01, 1e-3, seed=2)
+        S0 = mg.sample_sites(m.V, m.F, 1_000_000, seed=2)
+        k, iters = 32, 200
+    M = E.Mesh(m.V, m.F)
+    cells = E.grid_cells(M, S0.shape[0], k)
+    out = {"case": case, "sites": int(S0.shape[0]), "k": k, "iters": iters, "mode": 1, "rows": []}
+    for proj, frame in combos:
+        res = {}
+        for prof in ("mixed", "fp64"):
+            eng = E.Engine(E.params(k=k, mode=1, profile=prof, proj=proj, frame=frame), 1, S0.shape[0], cells)
+            g = eng.add(M, S0)
+            eng.run(1)
+            _sync()
+            eng.remove(g)
+            g = eng.add(M, S0)
+            st = torch.cuda.current_stream()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            eng.run(iters, C_stream(st))
+            e1.record(st)
+            e1.synchronize()
+            ev = eng.evaluate(g)
+            res[prof] = {"ms": e0.elapsed_time(e1), "dH": ev["dH"],
+                         "S": eng.sites_f64(g) if prof == "fp64" else eng.sites(g).astype(np.float64)}
+            eng.close()
+        d = np.linalg.norm(res["mixed"]["S"] - res["fp64"]["S"], axis=1) / M.diag
+        d = d[np.isfinite(d)]
+        out["rows"].append({"proj": proj, "frame": frame, "ms_mixed": res["mixed"]["ms"], "ms_fp64": res["fp64"]["ms"],
+                            "dH_rel_mixed": res["mixed"]["dH"] / M.diag, "dH_rel_fp64": res["fp64"]["dH"] / M.diag,
+                            "dH_minus_fp64_rel": (res["mixed"]["dH"] - res["fp64"]["dH"]) / M.diag,
+                            "drift_vs_fp64": {"mean": float(d.mean()), "p99": float(np.percentile(d, 99)),
+                                              "max": float(d.max())}})
+    M.close()
+    return out
