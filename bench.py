@@ -192,30 +192,46 @@ def _recorded(name):
         return json.load(fh)
 
 
-def traffic_recorded(workload, kernel_key, sites_in_launch):
-    """DRAM read + write bytes per launch of a kernel from a recorded ncu
-    capture (profiles/traffic.json), scaled from the captured launch's sites
-    to this launch's sites when the capture was a smaller case."""
-    d = _recorded("traffic.json")
-    w = (d or {}).get("workloads", {}).get(workload)
-    if not w or kernel_key not in w.get("bytes_per_launch", {}):
+KNN_GROUP = "site_knn (k_knn_verify + k_knn_search)"
+
+
+def _recorded_workload(name, workload):
+    """The entry of a recorded capture for a workload: its own entry, else
+    the entry recorded on a smaller case of the same family (`stands_for`
+    is the family's name prefix)."""
+    d = _recorded(name)
+    ws = (d or {}).get("workloads", {})
+    if workload in ws:
+        return ws[workload]
+    for w in ws.values():
+        if w.get("stands_for") and workload.startswith(w["stands_for"]):
+            return w
+    return None
+
+
+def traffic_recorded(workload, group, sites_in_launch):
+    """DRAM read + write bytes per launch of a kernel group from a recorded
+    ncu capture (profiles/traffic.json: dram__bytes_read.sum +
+    dram__bytes_write.sum averaged over the launches of one remesh), scaled
+    from the captured case's sites to this launch's sites.  (None, None)
+    when nothing is recorded for the workload's family."""
+    w = _recorded_workload("traffic.json", workload)
+    if not w or group not in w.get("groups", {}):
         return None, None
-    b = float(w["bytes_per_launch"][kernel_key])
-    sites = float(w.get("sites_per_launch", {}).get(kernel_key, sites_in_launch) or sites_in_launch)
-    return b * sites_in_launch / sites, f"recorded ncu capture: {w['command']} (scaled by sites per launch)"
+    b = sum(float(w["bytes_per_launch"][k]) for k in w["groups"][group])
+    return b * sites_in_launch / float(w["sites"]), \
+        f"recorded ncu capture on {w['sites']} sites: {w['command']} (scaled by sites per launch)"
 
 
-def issue_roofline(workload, prof, iters, sm_mhz, sms=None, sites_scale=1.0):
+def issue_roofline(workload, prof, iters, sm_mhz, sites, sms=None):
     """Warp-instruction issue rate of the site kernels against the B200's
     issue peak (SMs x 4 schedulers x SM clock), the bound these kernels meet
     long before HBM.  Warp instructions per remesh come from a recorded ncu
     capture (profiles/instructions.json: smsp__inst_executed.sum summed over
-    the launches of one remesh of the named workload, scaled by sites when
-    the capture was a smaller case); the kernel times come from this run's
-    CUDA events.  None when no count is recorded for the workload or no
-    clock is known."""
-    d = _recorded("instructions.json")
-    w = (d or {}).get("workloads", {}).get(workload)
+    the launches of one remesh, scaled from the captured case's sites to
+    `sites`); the kernel times come from this run's CUDA events.  None when
+    no count is recorded for the workload's family or no clock is known."""
+    w = _recorded_workload("instructions.json", workload)
     if not w or not sm_mhz:
         return None
     counts = w["warp_instructions_per_remesh"]
@@ -223,13 +239,15 @@ def issue_roofline(workload, prof, iters, sm_mhz, sms=None, sites_scale=1.0):
         import torch
         sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
     peak = sms * 4 * sm_mhz * 1e6
+    scale = sites / float(w["sites"])
     out = {"bound": "issue", "unit": "warp instructions/s", "peak": peak,
            "peak_from": f"{sms} SMs x 4 schedulers x {sm_mhz:.0f} MHz",
-           "counts": f"recorded ncu capture: {w['command']}, not this run", "kernels": {}}
-    for kernel, group in (("k_site_knn", "knn"), ("k_site_clip", "clip"), ("k_site_proj", "proj")):
-        if kernel in counts and prof.get(group, 0) > 0:
-            achieved = counts[kernel] * sites_scale / (prof[group] * 1e-3 * iters)
-            out["kernels"][kernel] = {"achieved": achieved, "frac": achieved / peak}
+           "counts": f"recorded ncu capture on {w['sites']} sites, scaled to {sites}: {w['command']}; not this run",
+           "kernels": {}}
+    for group, kernels in w["groups"].items():
+        if prof.get(group, 0) > 0:
+            achieved = sum(counts[k] for k in kernels) * scale / (prof[group] * 1e-3 * iters)
+            out["kernels"][" + ".join(kernels)] = {"achieved": achieved, "frac": achieved / peak}
     return out
 
 
@@ -475,7 +493,7 @@ def run_ours_batched(args):
     big = sorted(range(len(segs)), key=lambda j: -int(meshes[j][3].shape[0]))[:8]
     reuse = knn_reuse_share(eng, [segs[j] for j in big], iters)
     reuse["over"] = "the 8 meshes with the most sites, one whole remesh"
-    groups = {"site_knn (k_knn_verify + k_knn_search)": (prof["knn"], n_mine * knn_bytes_per_site(K)),
+    groups = {KNN_GROUP: (prof["knn"], n_mine * knn_bytes_per_site(K)),
               "k_site_clip": (prof["clip"], n_mine * clip_bytes_per_site(K)),
               "k_site_proj": (prof["proj"], n_mine * proj_bytes_per_site(K))}
     dom = max(groups, key=lambda g: groups[g][0])
@@ -492,7 +510,7 @@ def run_ours_batched(args):
                              / ((prof["knn"] + prof["clip"]) * 1e-3) / 1e9}}
     roofline["knn_clip"]["frac"] = roofline["knn_clip"]["achieved_gbs"] / peak
     sm_clock = clk.get("sm_mhz") or clk.get("sm_max_mhz")
-    ir = issue_roofline(cfg["workload"], prof, iters, sm_clock)
+    ir = issue_roofline(cfg["workload"], prof, iters, sm_clock, n_mine)
 
     # ---- accuracy: the same remesh with FP64 state and arithmetic ---------
     acc = None
@@ -698,7 +716,7 @@ def run_ours_torus(args):
     K = p["k"]
     newly = np.array([eng.stats(state["seg"], i)["newly_frozen"] for i in range(iters)], np.float64)
     active_mean = float(np.mean(n - np.concatenate([[0.0], np.cumsum(newly)[:-1]])))
-    groups = {"k_site_knn": (prof["knn"], active_mean * knn_bytes_per_site(K)),
+    groups = {KNN_GROUP: (prof["knn"], active_mean * knn_bytes_per_site(K)),
               "k_site_clip": (prof["clip"], n * clip_bytes_per_site(K)),
               "k_site_proj": (prof["proj"], n * proj_bytes_per_site(K))}
     dom = max(groups, key=lambda g: groups[g][0])
@@ -742,7 +760,7 @@ def run_ours_torus(args):
                         "same_sites_as_engine": same_as_engine},
                 "gpu_launches": int(sum(launches)),
                 "roofline": roofline,
-                "issue_roofline": issue_roofline(cfg["workload"], prof, iters, clk.get("sm_mhz") or clk.get("sm_max_mhz")),
+                "issue_roofline": issue_roofline(cfg["workload"], prof, iters, clk.get("sm_mhz") or clk.get("sm_max_mhz"), n),
                 "cpu_baseline": cpu, "accuracy": acc, "clocks": clk, "tiles": E.tiles(prm),
                 "libgpucvt_launches_total": _lib.launch_count()}
         print(json.dumps(line), flush=True)

@@ -44,21 +44,39 @@ def test_both_arms_share_one_config():
 
 
 def test_issue_roofline_arithmetic():
+    """Issue rate = recorded warp instructions of a kernel group, scaled by
+    sites from the captured case, over the group's event time per remesh."""
     import bench
     with open(os.path.join(ROOT, "profiles", "instructions.json")) as fh:
-        rec = json.load(fh)["workloads"]["torus_100k"]
+        rec = json.load(fh)["workloads"]["batched_12_meshes"]
     counts = rec["warp_instructions_per_remesh"]
-    prof = {"grid": 0.03, "knn": 0.08, "clip": 0.06, "proj": 0.1}
-    out = bench.issue_roofline("torus_100k", prof, 100, 1965.0, sms=148)
+    prof = {"grid": 0.12, "knn": 2.9, "clip": 0.9, "proj": 2.0}
+    sites = 3 * rec["sites"]
+    out = bench.issue_roofline("batched_256_meshes", prof, 100, 1965.0, sites, sms=148)
     assert out["bound"] == "issue" and out["peak"] == 148 * 4 * 1965e6
     assert "recorded" in out["counts"]
-    for kernel, group in (("k_site_knn", "knn"), ("k_site_clip", "clip"), ("k_site_proj", "proj")):
-        k = out["kernels"][kernel]
-        assert abs(k["achieved"] - counts[kernel] / (prof[group] * 1e-3 * 100)) < 1e-6 * k["achieved"]
+    assert set(out["kernels"]) == {"k_knn_verify + k_knn_search", "k_site_clip", "k_site_proj"}
+    for group, kernels in rec["groups"].items():
+        k = out["kernels"][" + ".join(kernels)]
+        want = 3 * sum(counts[x] for x in kernels) / (prof[group] * 1e-3 * 100)
+        assert abs(k["achieved"] - want) < 1e-6 * want
         assert abs(k["frac"] - k["achieved"] / out["peak"]) < 1e-12
         assert 0.0 < k["frac"] < 1.0
-    assert bench.issue_roofline("torus_100k", prof, 100, None, sms=148) is None
-    assert bench.issue_roofline("no_such_workload", prof, 100, 1965.0, sms=148) is None
+    assert bench.issue_roofline("batched_256_meshes", prof, 100, None, sites, sms=148) is None
+    assert bench.issue_roofline("no_such_workload", prof, 100, 1965.0, sites, sms=148) is None
+
+
+def test_traffic_recorded_scaling():
+    """Recorded DRAM bytes of the site-KNN group (verify + search) scale with
+    the launch's sites; unknown workloads and groups give no figure."""
+    import bench
+    with open(os.path.join(ROOT, "profiles", "traffic.json")) as fh:
+        rec = json.load(fh)["workloads"]["batched_12_meshes"]
+    b, src = bench.traffic_recorded("batched_256_meshes", bench.KNN_GROUP, 2 * rec["sites"])
+    want = 2 * (rec["bytes_per_launch"]["k_knn_verify"] + rec["bytes_per_launch"]["k_knn_search"])
+    assert abs(b - want) < 1e-6 * want and "recorded" in src
+    assert bench.traffic_recorded("torus_100k", bench.KNN_GROUP, 100000) == (None, None)
+    assert bench.traffic_recorded("batched_256_meshes", "k_frame_vertex", 100000) == (None, None)
 
 
 def test_clock_fallback_without_samples(monkeypatch):
