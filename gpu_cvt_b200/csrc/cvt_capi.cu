@@ -1073,6 +1073,7 @@ struct cvt_engine {
   float* d_cand_rho = nullptr;
   float* d_cand_D = nullptr;
   int* d_srch = nullptr;          // sites left for a full KNN search, srch_cap slots per verify warp
+  float* d_srch_thr = nullptr;    // per slot: the check's bound on the site's MM-th distance
   int* d_srch_n = nullptr;
   int srch_cap = 0;
   unsigned long long* d_blockmax = nullptr;  // per cell slot: coarse-block motion of the last step
@@ -1248,6 +1249,7 @@ extern "C" cvt_status_t cvt_engine_create(const cvt_params_t* p, int max_segment
     ar.add(&e->d_cand_D, ns);
     e->srch_cap = (int)cdiv((long)ns, (long)e->num_sms * kKnnVerifyWarpsPerSM) + 2;  // two sites per warp step
     ar.add(&e->d_srch, (size_t)e->srch_cap * e->num_sms * kKnnVerifyWarpsPerSM);
+    ar.add(&e->d_srch_thr, (size_t)e->srch_cap * e->num_sms * kKnnVerifyWarpsPerSM);
     ar.add(&e->d_srch_n, (size_t)e->num_sms * kKnnVerifyWarpsPerSM);
     ar.add(&e->d_blockmax, (size_t)max_cells);
   }
@@ -1386,7 +1388,7 @@ template <class T> static EngineArgs<T> engine_args(cvt_engine* e) {
   a.cell_start = e->d_cell_start; a.sorted = (const Pt4<T>*)e->d_sorted; a.total_cells = e->max_cells;
   a.stats = e->d_stats; a.ovf = e->d_ovf; a.far = e->d_far; a.cent = (T*)e->d_cent; a.K = e->K;
   a.proj_mode = e->p.proj_mode; a.bvh_ovf = reinterpret_cast<int*>(e->d_tickets + 2);
-  a.cand = e->d_cand; a.cand_rho = e->d_cand_rho; a.cand_D = e->d_cand_D; a.srch = e->d_srch; a.srch_n = e->d_srch_n; a.srch_cap = e->srch_cap; a.blockmax = e->d_blockmax;
+  a.cand = e->d_cand; a.cand_rho = e->d_cand_rho; a.cand_D = e->d_cand_D; a.srch = e->d_srch; a.srch_thr = e->d_srch_thr; a.srch_n = e->d_srch_n; a.srch_cap = e->srch_cap; a.blockmax = e->d_blockmax;
   return a;
 }
 

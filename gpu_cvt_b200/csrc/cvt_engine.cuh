@@ -113,6 +113,7 @@ template <class T> struct EngineArgs {
   float* cand_rho;   // its MM-th distance when it was built, rounded down (< 0: no list; inf: every other site)
   float* cand_D;     // motion bound accumulated since it was built (k_knn_verify)
   int* srch;         // per verify warp: srch_cap slots of sorted positions left for a full search
+  float* srch_thr;   // per slot: squared distance that the site's MM nearest lie within (< 0: unknown)
   int* srch_n;       // per verify warp: slots used
   int srch_cap;
   unsigned long long* blockmax;  // per coarse block (cell slots of the segment): iteration << 32 | max motion bits
@@ -461,9 +462,16 @@ __device__ __forceinline__ void knn_store(const EngineArgs<T>& a, int g, const S
 
 // Full search of the site at sorted position t (one warp): the K nearest
 // (MM = 0), or the MM nearest, which refresh its candidate list and whose
-// first K are the K-list.  seg receives the site's segment.
+// first K are the K-list.  seg receives the site's segment.  With candidate
+// lists the search is first tried as one radius query (warp_radius_knn,
+// scratch buf of 64 keys): within bound tb when the check left one (the
+// largest re-keyed distance of the site's complete old list, so at least MM
+// sites lie within it), else within a squared distance expected to hold
+// about (MM + 64) / 2 sites; when the count falls outside [MM, 64] the ring
+// search runs instead.  Both return the MM smallest (distance, index) keys.
 template <class T, int KK, int MM>
-__device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, int lane, int& seg) {
+__device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, float tb, int lane, int& seg,
+                                                typename KeyOps<T>::Key* buf) {
   using O = KeyOps<T>;
   using Key = typename O::Key;
   const Pt4<T> me = a.sorted[t];
@@ -478,17 +486,32 @@ __device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, i
   const V3<T> q{me.x, me.y, me.z};
   const float kp = a.kth[g];
   const uint32_t self = (uint32_t)g;
+  auto not_self = [self](uint32_t id) { return id != self; };
   Key key;
   if constexpr (MM > 0) {
-    constexpr int RM = (MM + 31) / 32;
-    Key mk[RM];
+    static_assert(MM <= 64, "at most 64 candidates");
+    Key mk[2];
     const float rho = a.cand_rho[g];
-    const T thrM = rho >= 0.f && !isinf(rho) ? (T)rho * (T)rho * (T)1.2
-                   : (kp >= 0.f ? (T)kp * (T)(1.1 * (MM + 1) / (KK + 1)) : (T)sd.kth_est * (T)((MM + 1.0) / (KK + 1)));
-    warp_knn<T, T, MM>(a.geom[s], a.cell_start, a.sorted, q, thrM, lane, [self](uint32_t id) { return id != self; },
-                       mk);
+    const GridGeom G = a.geom[s];
+    const T base = kp >= 0.f ? (T)kp : (T)sd.kth_est;
+    const T thr_r = tb >= 0.f ? (T)tb : base * (T)((MM + 64) / 2.0 / (KK + 1));
+    const float qm = fmaxf(fabsf((float)q.x), fmaxf(fabsf((float)q.y), fabsf((float)q.z)));
+    const float rad = __fsqrt_ru(f32_ru(thr_r)) * 1.0001f + 1e-3f * G.h + 4e-7f * qm;
+    if (!warp_radius_knn<T, T, MM>(G, a.cell_start, a.sorted, q, thr_r, rad, lane, not_self, buf, mk)) {
+      const T thrM = tb >= 0.f ? (T)tb
+                     : rho >= 0.f && !isinf(rho) ? (T)rho * (T)rho * (T)1.2
+                     : (kp >= 0.f ? (T)kp * (T)(1.1 * (MM + 1) / (KK + 1)) : (T)sd.kth_est * (T)((MM + 1.0) / (KK + 1)));
+      if constexpr (MM > 32) {
+        warp_knn<T, T, MM>(G, a.cell_start, a.sorted, q, thrM, lane, not_self, mk);
+      } else {
+        Key one[1];
+        warp_knn<T, T, MM>(G, a.cell_start, a.sorted, q, thrM, lane, not_self, one);
+        mk[0] = one[0];
+        mk[1] = O::empty();
+      }
+    }
 #pragma unroll
-    for (int r = 0; r < RM; ++r)
+    for (int r = 0; r < 2; ++r)
       if (32 * r + lane < MM) a.cand[(size_t)g * MM + 32 * r + lane] = O::idx(mk[r]);
     const Key mth = shfl_key(mk[(MM - 1) / 32], (MM - 1) % 32);
     if (lane == 0) {
@@ -497,13 +520,13 @@ __device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, i
     }
     key = mk[0];
   } else {
+    (void)tb; (void)buf;
     // candidates beyond 1.1x the last K-th squared distance are skipped; sites
     // move little between iterations, and a bound that proves too tight
     // restarts the search without it (swept 1.02-1.5: 1.05-1.1 fastest)
     const T thr0 = kp >= 0.f ? (T)kp * (T)1.1 : (T)sd.kth_est;
     Key kl[1];
-    warp_knn<T, T, KK>(a.geom[s], a.cell_start, a.sorted, q, thr0, lane, [self](uint32_t id) { return id != self; },
-                       kl);
+    warp_knn<T, T, KK>(a.geom[s], a.cell_start, a.sorted, q, thr0, lane, not_self, kl);
     key = kl[0];
   }
   knn_store<T, KK>(a, g, sd, key, lane);
@@ -520,10 +543,12 @@ __device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, i
 // KK-th is closer than rho - D.  `valid`: this half has a site.  Every lane
 // runs every warp-wide step; true when the half's K-list came from the list
 // (and is stored: row entries that changed, kth, same, the list's new
-// order, D).
+// order, D).  bound: for a site whose complete list was re-keyed, the
+// largest re-keyed squared distance rounded up (its MM list sites are MM
+// other sites, so the MM nearest lie within it); else -1.
 template <class T, int KK, int MM>
 __device__ __forceinline__ bool knn_verify_half(const EngineArgs<T>& a, int parity, int w, bool valid, int lane,
-                                                int& seg) {
+                                                int& seg, float& bound) {
   static_assert(KK <= 32 && MM > KK && MM <= 48, "candidate list of KK < MM <= 48 entries");
   using O = KeyOps<T>;
   using Key = typename O::Key;
@@ -540,7 +565,8 @@ __device__ __forceinline__ bool knn_verify_half(const EngineArgs<T>& a, int pari
     q = {me.x, me.y, me.z};
   }
   seg = s;
-  bool ok = valid && rho >= 0.f;
+  const bool have = valid && rho >= 0.f;
+  bool ok = have;
   // motion bound: lanes hl and hl + 16 < 27 read blocks
   unsigned mbits = 0u;
   float D = 0.f, lim = 0.f;
@@ -575,7 +601,7 @@ __device__ __forceinline__ bool knn_verify_half(const EngineArgs<T>& a, int pari
   for (int r = 0; r < 3; ++r) {
     const int e = 3 * hl + r;
     k[r] = O::empty();
-    if (ok && e < MM) {
+    if (have && e < MM) {
       const uint32_t id = __ldg(a.cand + (size_t)g * MM + e);
       if (id != 0xffffffffu) k[r] = O::make(dist2(ld3(a.S[parity], (long)id), q), id);
     }
@@ -584,6 +610,20 @@ __device__ __forceinline__ bool knn_verify_half(const EngineArgs<T>& a, int pari
   half_select3<T, KK>(k, hl, half, moved);
   constexpr int KL = (KK - 1) / 3, KR = (KK - 1) % 3;
   const Key kth = shfl16_key(k[KR], KL);
+  {
+    T dm = (T)0;
+    int nv = 0;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+      if (!O::is_empty(k[r])) { const T d = O::dist(k[r]); dm = d > dm ? d : dm; ++nv; }
+#pragma unroll
+    for (int o = 8; o >= 1; o >>= 1) {
+      const T od = __shfl_xor_sync(0xffffffffu, dm, o, 16);
+      dm = od > dm ? od : dm;
+      nv += __shfl_xor_sync(0xffffffffu, nv, o, 16);
+    }
+    bound = have && nv == MM ? f32_ru(dm) : -1.f;
+  }
   ok = ok && !O::is_empty(kth) && (isinf(rho) || f32_ru(O::dist(kth)) * 1.0003f < lim * lim);
   // store (per half: entries e < KK of this lane, the flags by lane hl 0)
   bool diff = false;
@@ -643,6 +683,7 @@ __global__ void __launch_bounds__(BS, kKnnVerifyWarpsPerSM * 32 / BS) k_knn_veri
   const int nw = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
   const int n = __ldg(a.act_count);
   int* mine = a.srch + (size_t)wi * a.srch_cap;
+  float* mine_thr = a.srch_thr + (size_t)wi * a.srch_cap;
   int cnt = 0;
   SegCounter<T> reused;  // per half, kept by lanes 0 and 16
   const int hl = lane & 15, half = lane >> 4;
@@ -650,12 +691,17 @@ __global__ void __launch_bounds__(BS, kKnnVerifyWarpsPerSM * 32 / BS) k_knn_veri
   for (int w0 = 2 * wi; w0 < n; w0 += 2 * nw) {
     const int w = w0 + half;
     int seg;
-    const bool ok = knn_verify_half<T, KK, MM>(a, parity, w, w < n, lane, seg);
+    float bound;
+    const bool ok = knn_verify_half<T, KK, MM>(a, parity, w, w < n, lane, seg, bound);
     const bool need = w < n && !ok;
     if (ok) reused.add(a, seg, 6, hl);
     // the warp's list: half 0's site first, then half 1's
     const unsigned b = __ballot_sync(0xffffffffu, need && hl == 0);
-    if (need && hl == 0) mine[cnt + (half ? (int)(b & 1u) : 0)] = a.act[w];
+    if (need && hl == 0) {
+      const int slot = cnt + (half ? (int)(b & 1u) : 0);
+      mine[slot] = a.act[w];
+      mine_thr[slot] = bound;
+    }
     cnt += __popc(b);
   }
   reused.flush(a, 6, hl);
@@ -671,12 +717,15 @@ __global__ void __launch_bounds__(BS, kKnnSearchWarpsPerSM * 32 / BS) k_knn_sear
   const int nw = (int)((gridDim.x * (unsigned)blockDim.x) >> 5);
   SegCounter<T> searched;
   if constexpr (MM > 0) {
+    __shared__ typename KeyOps<T>::Key buf[BS / 32][64];  // per warp: the radius query's keys
+    auto* mybuf = buf[threadIdx.x >> 5];
     for (int l = wi; l < n_lists; l += nw) {
       const int* list = a.srch + (size_t)l * a.srch_cap;
+      const float* thr = a.srch_thr + (size_t)l * a.srch_cap;
       const int n = a.srch_n[l];
       for (int k = 0; k < n; ++k) {
         int seg;
-        knn_search_site<T, KK, MM>(a, list[k], lane, seg);
+        knn_search_site<T, KK, MM>(a, list[k], thr[k], lane, seg, mybuf);
         searched.add(a, seg, 7, lane);
       }
     }
@@ -684,7 +733,7 @@ __global__ void __launch_bounds__(BS, kKnnSearchWarpsPerSM * 32 / BS) k_knn_sear
     const int n = __ldg(a.act_count);
     for (int w = wi; w < n; w += nw) {
       int seg;
-      knn_search_site<T, KK, MM>(a, a.act[w], lane, seg);
+      knn_search_site<T, KK, MM>(a, a.act[w], -1.f, lane, seg, nullptr);
       searched.add(a, seg, 7, lane);
     }
   }

@@ -315,6 +315,129 @@ __device__ __forceinline__ void warp_knn(const GridGeom& g, const int* __restric
 }
 
 // ---------------------------------------------------------------------------
+// Radius query + sort: one warp per query point
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long shfl_xor_key(unsigned long long k, int m) {
+  return __shfl_xor_sync(0xffffffffu, k, m);
+}
+__device__ __forceinline__ DKey shfl_xor_key(DKey k, int m) {
+  return {__shfl_xor_sync(0xffffffffu, k.d, m), __shfl_xor_sync(0xffffffffu, k.i, m)};
+}
+
+// Bitonic sort of 64 keys held two per lane (element 32 r + lane in k[r]),
+// ascending: 21 compare-exchange steps, all but one across lanes.
+template <class T>
+__device__ __forceinline__ void warp_bitonic64(typename KeyOps<T>::Key (&k)[2], int lane) {
+  using O = KeyOps<T>;
+#pragma unroll
+  for (int kk = 2; kk <= 64; kk <<= 1) {
+#pragma unroll
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      if (j == 32) {  // kk == 64: the partner is the lane's other register, ascending
+        const auto lo = O::kmin(k[0], k[1]), hi = O::kmax(k[0], k[1]);
+        k[0] = lo; k[1] = hi;
+      } else {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const bool up = ((32 * r + lane) & kk) == 0;
+          const auto o = shfl_xor_key(k[r], j);
+          k[r] = (((lane & j) == 0) == up) ? O::kmin(k[r], o) : O::kmax(k[r], o);
+        }
+      }
+    }
+  }
+}
+
+// Exact MM nearest points of q (uniform across the warp) from one radius
+// query: every accepted point whose squared distance is <= thr is gathered
+// into buf (the warp's CAP = 64 keys of shared memory) and the gathered
+// keys are sorted.  When at least MM and at most 64 points pass, the first
+// MM of list (element 32 r + lane in list[r], the layout of warp_knn) are
+// the MM nearest in (squared distance, index) order: every point left out
+// is farther than thr, so farther than the MM-th gathered one.  The cells
+// visited are those of the box q +- rad, which the caller sizes so that it
+// holds every point within sqrt(thr) (rad rounded up with margin; cell
+// coordinates are monotone in the position).  Returns false when the count
+// is outside [MM, 64] (the caller then runs warp_knn); it stops scanning as
+// soon as more than 64 points have passed.
+template <class T, class PT, int MM, class Accept>
+__device__ __forceinline__ bool warp_radius_knn(const GridGeom& g, const int* __restrict__ cell_start,
+                                                const Pt4<PT>* __restrict__ pts, V3<T> q, T thr, float rad,
+                                                int lane, Accept accept, typename KeyOps<T>::Key* buf,
+                                                typename KeyOps<T>::Key (&list)[2]) {
+  static_assert(MM >= 1 && MM <= 64, "at most 64 neighbours");
+  constexpr int CAP = 64;
+  using O = KeyOps<T>;
+  using Key = typename O::Key;
+  if (!finite3(q) || !(rad < INFINITY) || !(thr >= (T)0)) return false;
+  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
+  int lo[3], hi[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    lo[ax] = grid_coord(g, __fsub_rd(qf[ax], rad), ax);
+    hi[ax] = grid_coord(g, __fadd_ru(qf[ax], rad), ax);
+  }
+  const int ny = hi[1] - lo[1] + 1;
+  const int nrows = ny * (hi[2] - lo[2] + 1);
+  const unsigned below = (1u << lane) - 1u;
+  int cnt = 0;
+  for (int base = 0; base < nrows; base += 32) {
+    // one (z, y) row of the box per lane: a contiguous range of sorted points
+    const int rowi = base + lane;
+    int b = 0, e = 0;
+    if (rowi < nrows) {
+      const int z = lo[2] + rowi / ny, y = lo[1] + rowi % ny;
+      const int row = g.cell_base + (z * g.dim[1] + y) * g.dim[0];
+      b = __ldg(cell_start + row + lo[0]);
+      e = __ldg(cell_start + row + hi[0] + 1);
+    }
+    const int len = e - b;
+    int incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int excl = incl - len;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    for (int c = 0; c < total; c += 32) {
+      const int i = c + lane;
+      int src = 0;
+#pragma unroll
+      for (int step = 16; step >= 1; step >>= 1) {
+        const int probe = src + step;
+        const int ex = __shfl_sync(0xffffffffu, excl, probe & 31);
+        if (probe < 32 && ex <= i) src = probe;
+      }
+      const int rb = __shfl_sync(0xffffffffu, b, src);
+      const int rex = __shfl_sync(0xffffffffu, excl, src);
+      bool pass = false;
+      Key key = O::empty();
+      if (i < total) {
+        const Pt4<PT> p = pts[rb + (i - rex)];
+        if (accept(p.id)) {
+          const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
+          key = O::make(d, p.id);
+          pass = d <= thr;
+        }
+      }
+      const unsigned m = __ballot_sync(0xffffffffu, pass);
+      const int slot = cnt + __popc(m & below);
+      if (pass && slot < CAP) buf[slot] = key;
+      cnt += __popc(m);
+      if (cnt > CAP) return false;
+    }
+  }
+  if (cnt < MM) return false;
+  __syncwarp();
+  list[0] = lane < cnt ? buf[lane] : O::empty();
+  list[1] = lane + 32 < cnt ? buf[lane + 32] : O::empty();
+  __syncwarp();  // every lane has read buf before the next query writes it
+  warp_bitonic64<T>(list, lane);
+  return true;
+}
+
+// ---------------------------------------------------------------------------
 // Warp-wide selection of the KK smallest keys of short lists, in order,
 // one list per half warp (16 lanes) with three keys per lane (element
 // e = 3 hl + r, hl = lane within the half): odd-even transposition passes
