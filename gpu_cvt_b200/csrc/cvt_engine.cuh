@@ -493,8 +493,11 @@ __device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, f
     Key mk[2];
     const float rho = a.cand_rho[g];
     const GridGeom G = a.geom[s];
-    const T base = kp >= 0.f ? (T)kp : (T)sd.kth_est;
-    const T thr_r = tb >= 0.f ? (T)tb : base * (T)((MM + 64) / 2.0 / (KK + 1));
+    // kth holds the site's last K-th squared distance (K sites within it);
+    // kth_est, from the segment's density, is expected to hold 2 (K + 1)
+    constexpr double kTarget = (MM + 64) / 2.0;
+    const T thr_r = tb >= 0.f ? (T)tb
+                    : kp >= 0.f ? (T)kp * (T)(kTarget / KK) : (T)sd.kth_est * (T)(kTarget / (2.0 * (KK + 1)));
     const float qm = fmaxf(fabsf((float)q.x), fmaxf(fabsf((float)q.y), fabsf((float)q.z)));
     const float rad = __fsqrt_ru(f32_ru(thr_r)) * 1.0001f + 1e-3f * G.h + 4e-7f * qm;
     if (!warp_radius_knn<T, T, MM>(G, a.cell_start, a.sorted, q, thr_r, rad, lane, not_self, buf, mk)) {
