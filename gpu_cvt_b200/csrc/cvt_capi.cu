@@ -1515,6 +1515,10 @@ static cvt_status_t enqueue_iteration_t(cvt_engine* e, int parity, cudaStream_t 
   launch_site_clip<PROF>(a, parity, ns, e->p.clip_block, e->p.frame_mode, e->num_sms, st);
   L += 2;
   if (ev) CK(cudaEventRecord(ev[3], st));
+  if (e->p.proj_mode == CVT_PROJ_ONERING) {
+    k_site_vsearch<PROF, 128><<<cdiv(ns, 128), 128, 0, st>>>(a, parity);
+    L++;
+  }
   launch_site_proj<PROF>(a, parity, ns, e->p.proj_block, e->p.proj_mode, st);
   k_site_far<PROF><<<e->num_sms, 128, 0, st>>>(a, parity, e->d_segs, e->d_active, e->max_seg, e->d_tickets + 1);
   L += 2;

@@ -897,38 +897,55 @@ __device__ __forceinline__ void site_finish(const EngineArgs<typename PT<PROF>::
 // that the neighbours leave almost unbounded in the first iteration).
 constexpr int kVertexRingLimit = 4;
 
-// Everything after the centroid; false when the 5-NN search was deferred
-// (the site is then listed in a.far and finished by k_site_far).
+// Centroid -> its kKProj nearest mesh vertices, for every gridded site that
+// is not frozen (one thread per site), into a.knnv.  A site whose search
+// would pass kVertexRingLimit rings is listed in a.far and its list marked
+// kVertexDeferred; k_site_far finishes it.  A kernel of its own: the search
+// needs a fraction of the projection's registers, so it runs at twice the
+// projection's resident warps.
+constexpr int kVertexDeferred = -2;
+
+template <int PROF, int BS>
+__global__ void __launch_bounds__(BS) k_site_vsearch(EngineArgs<typename PT<PROF>::T> a, int parity) {
+  using T = typename PT<PROF>::T;
+  (void)parity;
+  const int t = blockIdx.x * BS + threadIdx.x;
+  const int n_grid = __ldg(a.cell_start + a.total_cells);
+  if (t >= n_grid) return;
+  const int g = (int)a.sorted[t].id;
+  const int s = __ldg(a.site_seg + g);
+  const SegDev& sd = a.segs[s];
+  if (sd.mode != 0 && a.frozen[g]) return;  // frozen sites keep their vertices
+  const MeshDev& md = a.meshes[sd.mesh];
+  int* kv = a.knnv + (size_t)g * kKProj;
+  const int skip = (sd.mode == 0 && sd.ex_quirk) ? g - sd.site_base : -1;
+  TopK<T, kKProj> top;
+  if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, ld3((const T*)a.cent, g), top,
+                                  [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
+    const int k = atomicAdd(a.far, 1);
+    a.far[1 + k] = g;
+    kv[0] = kVertexDeferred;
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < kKProj; ++k) kv[k] = (int)KeyOps<T>::idx(top.k[k]);
+}
+
+// Everything after the centroid and (PROJ 0) the vertex search of
+// k_site_vsearch; false when that search was deferred (the site is then
+// listed in a.far and finished by k_site_far).
 template <int PROF, int PROJ>
 __device__ __forceinline__ bool site_proj(const EngineArgs<typename PT<PROF>::T>& a, int parity, int g, SiteOut& o) {
-  using T = typename PT<PROF>::T;
   if (PROJ == 1) {
     const int none[kKProj] = {-1, -1, -1, -1, -1};
     site_finish<PROF, 1>(a, parity, g, none, o);
     return true;
   }
-  const int s = __ldg(a.site_seg + g);
-  const SegDev& sd = a.segs[s];
-  const MeshDev& md = a.meshes[sd.mesh];
-  const bool fz = sd.mode != 0 && a.frozen[g];
-  // centroid -> nearest mesh vertices (frozen sites keep theirs)
-  int* kv = a.knnv + (size_t)g * kKProj;
+  const int* kv = a.knnv + (size_t)g * kKProj;
   int knnv[kKProj];
-  if (!fz) {
-    const int skip = (sd.mode == 0 && sd.ex_quirk) ? g - sd.site_base : -1;
-    TopK<T, kKProj> top;
-    if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, ld3((const T*)a.cent, g), top,
-                                    [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
-      const int k = atomicAdd(a.far, 1);
-      a.far[1 + k] = g;
-      return false;
-    }
 #pragma unroll
-    for (int k = 0; k < kKProj; ++k) { knnv[k] = (int)KeyOps<T>::idx(top.k[k]); kv[k] = knnv[k]; }
-  } else {
-#pragma unroll
-    for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];
-  }
+  for (int k = 0; k < kKProj; ++k) knnv[k] = kv[k];
+  if (knnv[0] == kVertexDeferred) return false;
   site_finish<PROF, 0>(a, parity, g, knnv, o);
   return true;
 }
@@ -1018,8 +1035,11 @@ __device__ __forceinline__ void motion_to_block(const EngineArgs<T>& a, int pari
     atomicMax(a.blockmax + blk, ((unsigned long long)stamp << 32) | mb);
 }
 
+// One-ring projection: 24 resident warps per SM (80 registers), the
+// fastest budget of a register sweep (64 or 51: spills; 96 or 128: too few
+// warps).  The BVH projection keeps the compiler's choice.
 template <int PROF, int BS, int PROJ>
-__global__ void __launch_bounds__(BS) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
+__global__ void __launch_bounds__(BS, PROJ == 0 ? 768 / BS : 1) k_site_proj(EngineArgs<typename PT<PROF>::T> a, int parity) {
   __shared__ StatsStage stage;
   stats_stage_init(stage);
   __syncthreads();
