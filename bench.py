@@ -193,6 +193,7 @@ def _recorded(name):
 
 
 KNN_GROUP = "site_knn (k_knn_verify + k_knn_search)"
+PROJ_GROUP = "projection (k_site_vsearch + k_site_proj)"
 
 
 def _recorded_workload(name, workload):
@@ -495,7 +496,7 @@ def run_ours_batched(args):
     reuse["over"] = "the 8 meshes with the most sites, one whole remesh"
     groups = {KNN_GROUP: (prof["knn"], n_mine * knn_bytes_per_site(K)),
               "k_site_clip": (prof["clip"], n_mine * clip_bytes_per_site(K)),
-              "k_site_proj": (prof["proj"], n_mine * proj_bytes_per_site(K))}
+              PROJ_GROUP: (prof["proj"], n_mine * proj_bytes_per_site(K))}
     dom = max(groups, key=lambda g: groups[g][0])
     ms, alg_bytes = groups[dom]
     peak, peak_kind = measured_peaks()
@@ -718,7 +719,7 @@ def run_ours_torus(args):
     active_mean = float(np.mean(n - np.concatenate([[0.0], np.cumsum(newly)[:-1]])))
     groups = {KNN_GROUP: (prof["knn"], active_mean * knn_bytes_per_site(K)),
               "k_site_clip": (prof["clip"], n * clip_bytes_per_site(K)),
-              "k_site_proj": (prof["proj"], n * proj_bytes_per_site(K))}
+              PROJ_GROUP: (prof["proj"], n * proj_bytes_per_site(K))}
     dom = max(groups, key=lambda g: groups[g][0])
     ms, alg_bytes = groups[dom]
     peak, peak_kind = measured_peaks()

@@ -55,7 +55,7 @@ def test_issue_roofline_arithmetic():
     out = bench.issue_roofline("batched_256_meshes", prof, 100, 1965.0, sites, sms=148)
     assert out["bound"] == "issue" and out["peak"] == 148 * 4 * 1965e6
     assert "recorded" in out["counts"]
-    assert set(out["kernels"]) == {"k_knn_verify + k_knn_search", "k_site_clip", "k_site_proj"}
+    assert set(out["kernels"]) == {" + ".join(ks) for ks in rec["groups"].values()}
     for group, kernels in rec["groups"].items():
         k = out["kernels"][" + ".join(kernels)]
         want = 3 * sum(counts[x] for x in kernels) / (prof[group] * 1e-3 * 100)
