@@ -538,10 +538,12 @@ __device__ __forceinline__ void knn_search_site(const EngineArgs<T>& a, int t, f
 // Candidate-list check of active site w by a half warp (16 lanes, one site
 // each half, three list entries per lane: element e = 3 hl + r), so a warp
 // checks two sites at once.  The motion bound D grows by the largest last
-// motion M in the 27 coarse blocks around the site's old position (lanes
-// hl and hl + 16 < 27 read one block each) plus the site's own motion; the
-// step condition asks that the segment's largest motion plus the site's own
-// stay below B - rho.  The list is re-keyed at the current positions and its
+// motion M in the 8 coarse blocks nearest the site's old position (lanes
+// hl < 8 read one block each), which hold every site that started the step
+// within B/2 of it, plus the site's own motion; the step condition asks
+// that the segment's largest motion plus the site's own stay below
+// B/2 - rho (B/2 shrunk by 1e-3 for the rounding of cell coordinates), so a
+// site that started the step outside those blocks ends it beyond rho.  The list is re-keyed at the current positions and its
 // KK smallest selected in order (half_select3); it is accepted when the
 // KK-th is closer than rho - D.  `valid`: this half has a site.  Every lane
 // runs every warp-wide step; true when the half's K-list came from the list
@@ -576,25 +578,27 @@ __device__ __forceinline__ bool knn_verify_half(const EngineArgs<T>& a, int pari
   if (ok) {
     const SegDev& sd = a.segs[s];
     const GridGeom G = a.geom[s];
-    int bx, by, bz;
-    motion_block(G, ld3(a.S[parity ^ 1], g), bx, by, bz);
-    const int dx = block_dim(G, 0), dy = block_dim(G, 1), dz = block_dim(G, 2);
+    // the 2 x 2 x 2 blocks nearest the old position: per axis the block of
+    // its cell and the neighbour on the side of the nearer block face, which
+    // reach at least kBlockCells / 2 cells beyond the cell on either side
+    const V3<T> po = ld3(a.S[parity ^ 1], g);
+    const int c0[3] = {grid_coord(G, po.x, 0), grid_coord(G, po.y, 1), grid_coord(G, po.z, 2)};
+    int b0[3];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int b = hl + 16 * k;
-      if (b < 27) {
-        const int x = bx + b % 3 - 1, y = by + (b / 3) % 3 - 1, z = bz + b / 9 - 1;
-        if (x >= 0 && x < dx && y >= 0 && y < dy && z >= 0 && z < dz) {
-          const unsigned long long v = a.blockmax[G.cell_base + (z * dy + y) * dx + x];
-          if ((unsigned)(v >> 32) == (unsigned)(sd.iter - 1)) mbits = max(mbits, (unsigned)v);
-        }
+    for (int ax = 0; ax < 3; ++ax) b0[ax] = c0[ax] / kBlockCells - (c0[ax] % kBlockCells < kBlockCells / 2 ? 1 : 0);
+    const int dx = block_dim(G, 0), dy = block_dim(G, 1), dz = block_dim(G, 2);
+    if (hl < 8) {
+      const int x = b0[0] + (hl & 1), y = b0[1] + ((hl >> 1) & 1), z = b0[2] + (hl >> 2);
+      if (x >= 0 && x < dx && y >= 0 && y < dy && z >= 0 && z < dz) {
+        const unsigned long long v = a.blockmax[G.cell_base + (z * dy + y) * dx + x];
+        if ((unsigned)(v >> 32) == (unsigned)(sd.iter - 1)) mbits = (unsigned)v;
       }
     }
     mbits = __reduce_max_sync(hmask, mbits);
     // this site's own motion (also inside M, but usually far below it)
     const float mu = __fsqrt_rn(f32_ru(dist2(q, ld3(a.S[parity ^ 1], g)))) * 1.000001f;
     D = __fadd_ru(a.cand_D[g], __fadd_ru(__uint_as_float(mbits), mu));
-    const bool step_ok = __fadd_ru(sd.step_motion, mu) * 1.0001f < ((float)kBlockCells * G.h - rho) * 0.9999f;
+    const bool step_ok = __fadd_ru(sd.step_motion, mu) * 1.0001f < (0.4995f * (float)kBlockCells * G.h - rho) * 0.9999f;
     lim = rho * 0.9999f - D * 1.0001f;
     ok = isinf(rho) || (step_ok && lim > 0.f);
   }
