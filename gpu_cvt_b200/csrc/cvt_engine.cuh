@@ -906,11 +906,14 @@ constexpr int kVertexRingLimit = 4;
 // would pass kVertexRingLimit rings is listed in a.far and its list marked
 // kVertexDeferred; k_site_far finishes it.  A kernel of its own: the search
 // needs a fraction of the projection's registers, so it runs at twice the
-// projection's resident warps.
+// projection's resident warps (FP32 positions: 48 per SM, measured 3 %
+// faster for the projection group than the compiler's 56 registers and no
+// faster at 64; FP64 positions keep the compiler's choice, which spills
+// less).
 constexpr int kVertexDeferred = -2;
 
 template <int PROF, int BS>
-__global__ void __launch_bounds__(BS) k_site_vsearch(EngineArgs<typename PT<PROF>::T> a, int parity) {
+__global__ void __launch_bounds__(BS, PROF == PROF_FP64 ? 1 : 1536 / BS) k_site_vsearch(EngineArgs<typename PT<PROF>::T> a, int parity) {
   using T = typename PT<PROF>::T;
   (void)parity;
   const int t = blockIdx.x * BS + threadIdx.x;
