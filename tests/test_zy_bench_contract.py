@@ -38,5 +38,10 @@ def test_main_arm_prints_contract_line():
     assert line["batched_over_plain"] > 0
     rf = line["roofline"]
     assert rf["bound"] == "hbm" and rf["unit"] == "GB/s" and abs(rf["frac"] - rf["achieved"] / rf["peak"]) < 1e-9
+    assert rf["traffic"] is not None and "recorded" in rf["traffic_source"], rf
+    ir = line["issue_roofline"]
+    assert ir is not None, f"issue_roofline missing although a clock is known: clocks={clk}"
+    assert "recorded" in ir["counts"] and len(ir["kernels"]) == 3, ir
+    assert all(0.0 < k["frac"] < 1.5 for k in ir["kernels"].values()), ir
     assert set(line["tiles"]) == {"knn_block", "clip_block", "proj_block"}
     assert 0 < line["hausdorff_rel"]["max"] < 1e-2
