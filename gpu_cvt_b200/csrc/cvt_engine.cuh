@@ -9,16 +9,18 @@
 //   k_knn_verify per active site (one warp): the K-list from the site's
 //                candidate list where its motion bound proves it exact
 //   k_knn_search the other active sites (one warp each): exact (K+1)-NN in
-//                the segment, drop self (site_knn.cuh:79); frozen sites
-//                keep the previous list (main.cu:678)
+//                the segment, drop self (site_knn.cuh:79), by one radius
+//                query where a bound is known, else ring by ring; frozen
+//                sites keep the previous list (main.cu:678)
 //   k_site_clip  per site (one thread): frame (site_normals.cuh:69; or,
 //                as an option, from the PCA normal of the neighbours),
 //                tangent-plane clip and centroid (2dClip.cuh:82)
 //   k_clip_overflow  the same for the rare cells whose polygon outgrows
 //                the shared-memory buffer (exact 64-vertex cap)
-//   k_site_proj  per site (one thread): centroid -> 5 nearest
-//                vertices (main.cu:719-735, frozen sites keep theirs),
-//                one-ring projection (near_project.cuh:149; or, as an
+//   k_site_vsearch per site (one thread): centroid -> 5 nearest vertices
+//                (main.cu:719-735, frozen sites keep theirs)
+//   k_site_proj  per site (one thread): one-ring projection over those
+//                vertices (near_project.cuh:149; or, as an
 //                option, the exact closest point through the BVH), freeze test
 //                and apply (freezetest.cuh:155-212, 270-327, 451-466),
 //                tier assignment on the segment's first iteration
