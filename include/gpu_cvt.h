@@ -386,7 +386,10 @@ cvt_status_t cvt_remesh(const float* V, int nV, const int* F, int nF, const floa
  * floats); every mesh is a segment of one engine, so each Lloyd iteration
  * of all meshes is one pass of the iteration's kernels.  sites_out[i]
  * receives mesh i's sites after `iters` iterations -- the same values
- * cvt_remesh returns for that mesh alone.  Synchronous. */
+ * cvt_remesh returns for that mesh alone.  The meshes are ingested by up to
+ * 8 host threads, each on its own non-blocking stream (the call creates and
+ * joins them); a mesh that fails ingest fails the call with its error.
+ * Synchronous. */
 cvt_status_t cvt_remesh_batch(int n_meshes, const float* const* V, const int* nV, const int* const* F, const int* nF,
                               const float* const* sites_in, const int* n_sites, const cvt_params_t* p, int iters,
                               float* const* sites_out);

@@ -488,3 +488,31 @@ def test_knn_candidate_lists_match_full_search(eng, oracle, small_torus, mode, k
     assert out[True][2] == out[False][2]
     r = oracle.lloyd_run(m.V, m.F, S0, k, mode, 40, profile=oracle.P_MIXED)
     assert np.array_equal(out[True][0], r["S"])
+
+
+@pytest.mark.parametrize("profile", ["mixed", "fp64"])
+def test_remesh_batch_matches_single_remeshes(eng, profile):
+    """cvt_remesh_batch (meshes ingested by several host threads on their own
+    streams, every segment read back with one wait) returns, per mesh, the
+    sites of a one-mesh cvt_remesh with the same parameters."""
+    meshes = [mg.icosphere(3), mg.torus(1.0, 0.3, 60, 30, noise_sigma=0.002, seed=2),
+              mg.superquadric(4.0, 6000, seed=3), mg.icosphere(4, radius=2.0),
+              mg.torus(2.0, 0.5, 40, 20, noise_sigma=0.0, seed=4)]
+    meshes = meshes + meshes[:4]   # more meshes than ingest threads
+    S = [mg.sample_sites(m.V, m.F, 600 + 150 * i, seed=20 + i) for i, m in enumerate(meshes)]
+    prm = eng.params(k=24, mode=1, profile=profile)
+    outs = eng.remesh_batch([m.V for m in meshes], [m.F for m in meshes], S, prm, 15)
+    for m, s, o in zip(meshes, S, outs):
+        one = eng.remesh(m.V, m.F, s, iters=15, prm=prm)
+        assert np.array_equal(o, one)
+
+
+def test_remesh_batch_reports_a_bad_mesh(eng):
+    """A face index out of range in one mesh of the batch fails the call with
+    that mesh's ingest error (raised on the calling thread)."""
+    good = mg.icosphere(3)
+    bad_F = good.F.copy()
+    bad_F[5, 1] = len(good.V) + 7
+    S = [mg.sample_sites(good.V, good.F, 300, seed=1)] * 3
+    with pytest.raises(Exception, match="face index out of range"):
+        eng.remesh_batch([good.V] * 3, [good.F, bad_F, good.F], S, eng.params(k=24, mode=0, profile="mixed"), 3)
