@@ -1282,10 +1282,14 @@ extern "C" cvt_status_t cvt_engine_destroy(cvt_engine_t e) {
   return CVT_OK;
 }
 
-extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, const float* sites, int n,
-                                               int sites_on_device, int* seg_id, void* stream) {
+// defer_tables: leave the segment's entries of the device tables (segment,
+// grid geometry, mesh view, active flag) and the final wait to the caller,
+// which uploads the tables of many segments at once (each small copy from
+// pageable host memory waits for the stream); the sites buffer must then
+// stay valid until the stream has passed this segment's copy.
+static cvt_status_t add_segment_impl(cvt_engine* e, cvt_mesh_t mesh, const float* sites, int n, int sites_on_device,
+                                     int* seg_id, cudaStream_t st, bool defer_tables) {
   if (!e || !mesh || !sites || n < 1 || !seg_id) return fail(CVT_ERR_INVALID, "cvt_engine_add_segment: bad arguments");
-  cudaStream_t st = S_(stream);
   int s = -1;
   for (int k = 0; k < e->max_seg; ++k) if (!e->active[k] && !e->seg_mesh[k]) { s = k; break; }
   if (s < 0) return fail(CVT_ERR_CAPACITY, "cvt_engine_add_segment: no free segment slot");
@@ -1327,9 +1331,11 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
   e->host_iters[s] = 0;
   e->seg_p0[s] = e->parity;
   const size_t tsz = e->f64 ? sizeof(double) : sizeof(float);
-  CK(cudaMemcpyAsync(e->d_segs + s, &e->segs[s], sizeof(SegDev), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(e->d_geom + s, &e->geom[s], sizeof(GridGeom), cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(e->d_meshes + s, &md, sizeof(MeshDev), cudaMemcpyHostToDevice, st));
+  if (!defer_tables) {
+    CK(cudaMemcpyAsync(e->d_segs + s, &e->segs[s], sizeof(SegDev), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(e->d_geom + s, &e->geom[s], sizeof(GridGeom), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(e->d_meshes + s, &md, sizeof(MeshDev), cudaMemcpyHostToDevice, st));
+  }
   char* Sdst = (char*)e->d_S[e->parity] + tsz * 3 * (size_t)base;
   if (!e->f64) {
     CK(cudaMemcpyAsync(Sdst, sites, sizeof(float) * 3 * (size_t)n,
@@ -1363,10 +1369,30 @@ extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, 
     CK(cudaMemsetAsync(e->d_blockmax + cbase, 0, sizeof(unsigned long long) * (size_t)cells, st));
   }
   CK(cudaMemsetAsync(e->d_stats + (size_t)s * kStatsRing * kStatsWords, 0, sizeof(int) * kStatsRing * kStatsWords, st));
+  *seg_id = s;
+  if (defer_tables) return CVT_OK;
   CK(cudaMemcpyAsync(e->d_active + s, &e->active[s], sizeof(int), cudaMemcpyHostToDevice, st));
   // the host mirrors above are read by the async copies; keep them stable
   CK(cudaStreamSynchronize(st));
-  *seg_id = s;
+  return CVT_OK;
+}
+
+extern "C" cvt_status_t cvt_engine_add_segment(cvt_engine_t e, cvt_mesh_t mesh, const float* sites, int n,
+                                               int sites_on_device, int* seg_id, void* stream) {
+  return add_segment_impl(e, mesh, sites, n, sites_on_device, seg_id, S_(stream), false);
+}
+
+// The device tables of every segment slot from the host mirrors, in four
+// copies, then a wait (after add_segment_impl with defer_tables).
+static cvt_status_t upload_segment_tables(cvt_engine* e, cudaStream_t st) {
+  std::vector<MeshDev> md(e->max_seg);
+  for (int k = 0; k < e->max_seg; ++k)
+    if (e->seg_mesh[k]) md[k] = e->seg_mesh[k]->dev();
+  CK(cudaMemcpyAsync(e->d_segs, e->segs.data(), sizeof(SegDev) * e->max_seg, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(e->d_geom, e->geom.data(), sizeof(GridGeom) * e->max_seg, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(e->d_meshes, md.data(), sizeof(MeshDev) * e->max_seg, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(e->d_active, e->active.data(), sizeof(int) * e->max_seg, cudaMemcpyHostToDevice, st));
+  CK(cudaStreamSynchronize(st));
   return CVT_OK;
 }
 
@@ -1901,8 +1927,13 @@ extern "C" cvt_status_t cvt_remesh_batch(int n_meshes, const float* const* V, co
   cvt_engine_t e = nullptr;
   if (s == CVT_OK) s = cvt_engine_create(p, n_meshes, (int)total_sites, (int)total_cells, &e);
   std::vector<int> seg(n_meshes, -1);
+  // segments added with their tables uploaded once for all
   for (int i = 0; i < n_meshes && s == CVT_OK; ++i)
-    s = cvt_engine_add_segment(e, meshes[i], sites_in[i], n_sites[i], 0, &seg[i], nullptr);
+    s = add_segment_impl(e, meshes[i], sites_in[i], n_sites[i], 0, &seg[i], S_(nullptr), true);
+  if (e) {
+    const cvt_status_t u = upload_segment_tables(e, S_(nullptr));
+    if (s == CVT_OK) s = u;
+  }
   if (s == CVT_OK) s = cvt_engine_run(e, iters, nullptr);
   if (s == CVT_OK) s = engine_get_sites_all(e, seg.data(), n_meshes, sites_out);
   if (e) cvt_engine_destroy(e);
