@@ -401,10 +401,16 @@ __global__ void __launch_bounds__(kActiveListThreads) k_active_list(EngineArgs<T
 
 // ---------------------------------------------------------------------------
 // k_frame_vertex: each listed site's nearest mesh vertex (the frame vertex,
-// main.cu:685-700), one thread per site: the same exact grid search and key
-// order as any other, so the same vertex.  Runs on a second stream while
-// site KNN runs; k_site_clip is the first kernel to read a.nnv.
+// main.cu:685-700), one thread per site, in the same key order as any other
+// search, so the same vertex.  The site's vertex of the last iteration is
+// at the squared distance thr from its new position, so the nearest vertex
+// lies in the box of cells within sqrt(thr): a few cells, against the 27 of
+// the ring search, which runs when there is no such vertex or the box is
+// larger.  Runs on a second stream while the site KNN runs; k_site_clip is
+// the first kernel to read a.nnv.
 // ---------------------------------------------------------------------------
+constexpr int kFrameBoxCells = 27;
+
 template <class T>
 __global__ void k_frame_vertex(EngineArgs<T> a) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -412,9 +418,20 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
   const Pt4<T> me = a.sorted[a.act[w]];
   const int g = (int)me.id;
   const MeshDev& md = a.meshes[a.segs[__ldg(a.site_seg + g)].mesh];
+  const V3<T> q{me.x, me.y, me.z};
+  auto all = [](uint32_t) { return true; };
   TopK<T, 1> nv;
-  grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, V3<T>{me.x, me.y, me.z}, nv,
-                        [](uint32_t) { return true; });
+  const int old = a.nnv[g];
+  bool done = false;
+  if ((unsigned)old < (unsigned)md.nV) {
+    const V3<T> pv{(T)__ldg(md.V + 3 * old), (T)__ldg(md.V + 3 * old + 1), (T)__ldg(md.V + 3 * old + 2)};
+    const T thr = dist2(pv, q);
+    const float qm = fmaxf(fabsf((float)q.x), fmaxf(fabsf((float)q.y), fabsf((float)q.z)));
+    const float rad = __fsqrt_ru(f32_ru(thr)) * 1.0001f + 1e-3f * md.vg.h + 4e-7f * qm;
+    done = grid_knn_box<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, thr, rad, nv, all, kFrameBoxCells);
+    if (!done) nv = TopK<T, 1>();
+  }
+  if (!done) grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, nv, all);
   a.nnv[g] = (int)KeyOps<T>::idx(nv.k[0]);
 }
 
@@ -429,12 +446,13 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
 // nearest other sites of its last full search (ids and the MM-th squared
 // distance r2b = rho^2) and a bound D on how much closer any other site can
 // have come since.  Every iteration adds to D the site's own last motion and
-// the largest last motion of any site in the 27 coarse blocks (3 x 3 x 3
-// cells, edge B = 3h) around the site's old position.  A site j outside the
-// list started at distance >= rho; while it is within B of site i its steps
-// are among those counted, and it cannot jump from beyond B to within rho in
-// one step as long as (largest motion of the step in the segment) + (i's
-// motion) < B - rho, which every iteration checks.  So when the K-th nearest
+// the largest last motion of any site in the 8 coarse blocks (kBlockCells^3
+// cells each, edge B = kBlockCells h) nearest the site's old position, which
+// reach at least B/2 beyond it on every side.  A site j outside the list
+// started at distance >= rho; while it starts a step within B/2 of site i
+// its step is among those counted, and from farther it cannot end the step
+// within rho as long as (largest motion of the step in the segment) + (i's
+// motion) < B/2 - rho, which every iteration checks.  So when the K-th nearest
 // of the re-keyed list is closer than rho - D, no site outside the list is
 // closer: the list's first K are exactly the K nearest of all, the keys a
 // full search returns, at a fraction of its work.  Otherwise (and in a

@@ -149,6 +149,43 @@ __device__ __forceinline__ bool grid_knn(const GridGeom& g, const int* __restric
   return true;
 }
 
+// The KK nearest points of q from one box query (one thread): every
+// accepted point of the cells in q +- rad with squared distance <= thr is
+// offered to top.  When top fills, it holds the KK nearest in (squared
+// distance, index) order, the keys grid_knn returns: a point left out is
+// farther than thr, so farther than every key kept.  rad must cover
+// sqrt(thr) with margin (cell coordinates are monotone in the position).
+// Returns false, top partly filled, when fewer than KK points pass or the
+// box spans more than max_cells cells; the caller then resets top and runs
+// grid_knn.
+template <class T, class PT, int KK, class Accept>
+__device__ __forceinline__ bool grid_knn_box(const GridGeom& g, const int* __restrict__ cell_start,
+                                             const Pt4<PT>* __restrict__ pts, V3<T> q, T thr, float rad,
+                                             TopK<T, KK>& top, Accept accept, int max_cells) {
+  if (!finite3(q) || !(rad < INFINITY) || !(thr >= (T)0)) return false;
+  const float qf[3] = {(float)q.x, (float)q.y, (float)q.z};
+  int lo[3], hi[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = grid_coord(g, __fsub_rd(qf[a], rad), a);
+    hi[a] = grid_coord(g, __fadd_ru(qf[a], rad), a);
+  }
+  if ((hi[0] - lo[0] + 1) * (hi[1] - lo[1] + 1) * (hi[2] - lo[2] + 1) > max_cells) return false;
+  for (int z = lo[2]; z <= hi[2]; ++z) {
+    for (int y = lo[1]; y <= hi[1]; ++y) {
+      const int row = g.cell_base + (z * g.dim[1] + y) * g.dim[0];
+      const int e = __ldg(cell_start + row + hi[0] + 1);
+      for (int k = __ldg(cell_start + row + lo[0]); k < e; ++k) {
+        const Pt4<PT> p = pts[k];
+        if (!accept(p.id)) continue;
+        const T d = dist2(V3<T>{(T)p.x, (T)p.y, (T)p.z}, q);
+        if (d <= thr && d <= top.worst_d()) top.insert(KeyOps<T>::make(d, p.id));
+      }
+    }
+  }
+  return top.full();
+}
+
 // ---------------------------------------------------------------------------
 // warp-cooperative search: one warp per query point
 // ---------------------------------------------------------------------------
