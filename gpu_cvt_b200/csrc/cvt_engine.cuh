@@ -946,9 +946,34 @@ __global__ void __launch_bounds__(BS, PROF == PROF_FP64 ? 1 : 1536 / BS) k_site_
   const MeshDev& md = a.meshes[sd.mesh];
   int* kv = a.knnv + (size_t)g * kKProj;
   const int skip = (sd.mode == 0 && sd.ex_quirk) ? g - sd.site_base : -1;
+  auto accept = [skip](uint32_t id) { return (int)id != skip; };
+  const V3<T> c = ld3((const T*)a.cent, g);
   TopK<T, kKProj> top;
-  if (!grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, ld3((const T*)a.cent, g), top,
-                                  [skip](uint32_t id) { return (int)id != skip; }, kVertexRingLimit)) {
+  // the site's 5 vertices of the last iteration lie within the largest of
+  // their squared distances to the new centroid, so the 5 nearest do: one
+  // box query of the cells within it (exact when it finds 5 vertices)
+  bool done = false;
+  {
+    T thr = (T)0;
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < kKProj; ++k) {
+      const int v = kv[k];
+      ok = ok && (unsigned)v < (unsigned)md.nV && v != skip;
+      if (ok) {
+        const V3<T> pv{(T)__ldg(md.V + 3 * v), (T)__ldg(md.V + 3 * v + 1), (T)__ldg(md.V + 3 * v + 2)};
+        const T d = dist2(pv, c);
+        thr = d > thr ? d : thr;
+      }
+    }
+    if (ok) {
+      const float qm = fmaxf(fabsf((float)c.x), fmaxf(fabsf((float)c.y), fabsf((float)c.z)));
+      const float rad = __fsqrt_ru(f32_ru(thr)) * 1.0001f + 1e-3f * md.vg.h + 4e-7f * qm;
+      done = grid_knn_box<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, c, thr, rad, top, accept, 27);
+      if (!done) top = TopK<T, kKProj>();
+    }
+  }
+  if (!done && !grid_knn<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, c, top, accept, kVertexRingLimit)) {
     const int k = atomicAdd(a.far, 1);
     a.far[1 + k] = g;
     kv[0] = kVertexDeferred;
