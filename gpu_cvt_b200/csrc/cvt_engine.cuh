@@ -40,6 +40,9 @@ namespace cvt {
 constexpr int kStatsRing = 256;   // iterations of per-segment statistics kept
 constexpr int kStatsWords = 8;    // same, low, both, newly, maxdisp2 bits, iter, KNN lists reused, searched
 constexpr int kKProj = 5;         // KPROJ (main.cu:394)
+// Largest box (in vertex-grid cells) a bounded vertex query visits before it
+// leaves the site to the ring search: ring 1's 27 cells.
+constexpr int kVertexBoxCells = 27;
 constexpr int kFallbackCap = 66;  // 64-vertex reference cap + room for the overshoot
 // threads per SM that k_site_clip's launch bounds ask to keep resident: it
 // caps registers near 80 (6 blocks of 128 with 32 KB of polygon buffers each
@@ -409,8 +412,6 @@ __global__ void __launch_bounds__(kActiveListThreads) k_active_list(EngineArgs<T
 // larger.  Runs on a second stream while the site KNN runs; k_site_clip is
 // the first kernel to read a.nnv.
 // ---------------------------------------------------------------------------
-constexpr int kFrameBoxCells = 27;
-
 template <class T>
 __global__ void k_frame_vertex(EngineArgs<T> a) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
@@ -428,7 +429,7 @@ __global__ void k_frame_vertex(EngineArgs<T> a) {
     const T thr = dist2(pv, q);
     const float qm = fmaxf(fabsf((float)q.x), fmaxf(fabsf((float)q.y), fabsf((float)q.z)));
     const float rad = __fsqrt_ru(f32_ru(thr)) * 1.0001f + 1e-3f * md.vg.h + 4e-7f * qm;
-    done = grid_knn_box<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, thr, rad, nv, all, kFrameBoxCells);
+    done = grid_knn_box<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, thr, rad, nv, all, kVertexBoxCells);
     if (!done) nv = TopK<T, 1>();
   }
   if (!done) grid_knn<T, float, 1>(md.vg, md.vcell_start, md.vsorted, q, nv, all);
@@ -969,7 +970,8 @@ __global__ void __launch_bounds__(BS, PROF == PROF_FP64 ? 1 : 1536 / BS) k_site_
     if (ok) {
       const float qm = fmaxf(fabsf((float)c.x), fmaxf(fabsf((float)c.y), fabsf((float)c.z)));
       const float rad = __fsqrt_ru(f32_ru(thr)) * 1.0001f + 1e-3f * md.vg.h + 4e-7f * qm;
-      done = grid_knn_box<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, c, thr, rad, top, accept, 27);
+      done = grid_knn_box<T, float, kKProj>(md.vg, md.vcell_start, md.vsorted, c, thr, rad, top, accept,
+                                            kVertexBoxCells);
       if (!done) top = TopK<T, kKProj>();
     }
   }
